@@ -1,0 +1,293 @@
+"""SMI shift-map throughput on B200: maps/s for the 1024² pair (2048² FFT, 45 correlations).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One step = one full shift map of the pair at the identity pose (canvas → both sides' real planes
+→ forward FFTs → 45 correlation products → inverse FFTs → per-shift exact, calibrated score →
+argmax), the images' features resident in HBM. Device time per step is taken with CUDA events
+on the engine's stream, W untimed steps first, an L2 flush (a 256 MB write) between timed steps
+outside the timed spans. `e2e` is the same metric through the public API (Registrar.set_images
+from pinned host buffers + Registrar.shift_map copying the map back to pinned host memory).
+
+The path does not shard (one map needs all 45 correlations of every shift): N GPUs run N
+independent replicas, one process each (torchrun), and `value` is the maps/s of all ranks, timed
+as the slowest rank.
+
+--impl reference: the CPU restatement of the reference's path (the oracle, float64, scipy FFTs on
+all host cores) on the same pair; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SMI maps/s at 1024²"
+WORKLOAD = "smi_shift_map_1024_fft2048"
+
+
+def config(extra=None):
+    c = {"workload": WORKLOAD, "image": [1024, 1024], "fft": [2048, 2048], "correlations": 45,
+         "smi_features": "laplacian", "exact": True, "calibrated": True, "pose": "identity",
+         "pair": "blob field vs 8-level segmented modality, seeded shift in ±200 px (seed 1)",
+         "l2": "256 MB flush between timed steps (per-step working set 1.3 GB > 126 MB L2)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.lines, self.p = index, [], None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=lambda: self.lines.extend(self.p.stdout), daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait(timeout=10)
+            self.t.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[2:6]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def stage_bytes(p):
+    """Algorithmic bytes of each stage of one map (one launch of that kernel per side where it
+    runs per side): its compulsory reads and writes in this decomposition."""
+    nx, ny, cw, ch, P, C = p["nx"], p["ny"], p["cw"], p["ch"], p["n_real"], p["n_corr"]
+    half = (nx // 2 + 1) * 8
+    return {
+        "canvas": 2 * (5 * 1024 * 1024 * 4) * 2,
+        "fwd_rows": 2 * (5 * cw * ch * 4 + P * ch * half),
+        "fwd_cols": 2 * (P * ch * half + P * ny * half),
+        "inv_cols": 2 * P * ny * half + C * ny * half,
+        "inv_rows_score": C * ny * half + nx * ny * 4,
+    }
+
+
+def survey_bytes(p):
+    """The whole map's compulsory HBM bytes (both stacks read, both sides' half spectra written and
+    read once, the map written)."""
+    nx, ny, P = p["nx"], p["ny"], p["n_real"]
+    return 2 * 5 * 1024 * 1024 * 4 + 2 * (2 * P * nx * (ny // 2 + 1) * 8) + nx * ny * 4
+
+
+def cpu_map_seconds(m, f):
+    """One map of the pair by the CPU restatement (float64; scipy FFTs on every host core)."""
+    import scipy.fft as sf
+
+    from oracle import smi_oracle as O
+
+    t0 = time.perf_counter()
+    pa, pb = O.prepare(m), O.prepare(f)
+    t1 = time.perf_counter()
+    ga, gb, (nx, ny, cw, ch), (ox, oy, W, Hh) = O.grid_stacks(pa, pb, np.eye(3), cap=2048)
+    ids, corrs = O.corr_plan(True, False)
+    A, B = O.real_planes(ga, ids), O.real_planes(gb, ids)
+    w = os.cpu_count()
+    FA = {p: sf.rfft2(A[k], (ny, nx), workers=w) for k, p in enumerate(ids)}
+    FB = {p: sf.rfft2(B[k], (ny, nx), workers=w) for k, p in enumerate(ids)}
+    corr = np.zeros((45, ny, nx))
+    for a, b, c in corrs:
+        corr[c] = sf.irfft2(FA[a] * np.conj(FB[b]), (ny, nx), workers=w)
+    area = max(1.0, O.pair_area(pa["acf"], pb["acf"]))
+    mp = O.combine(corr, True, True, 12, area)
+    O.argmax_first(mp)
+    t2 = time.perf_counter()
+    return t2 - t1, t1 - t0
+
+
+def make_pair():
+    from zcmir_b200 import synth
+
+    m, f, H = synth.pair_segmented(n=1024, seed=1)
+    return (m / 65535.0).astype(np.float32), (f / 65535.0).astype(np.float32), H
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    m, f, _ = make_pair()
+    for _ in range(args.warmup):
+        cpu_map_seconds(m, f)
+    ts = [cpu_map_seconds(m, f)[0] for _ in range(args.steps)]
+    sec = float(np.mean(ts))
+    v = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "maps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(),
+        "cpu_baseline": {"value": v, "unit": "maps/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "one full 1024² map per step (features excluded, as on the GPU)"},
+        "e2e": {"value": v, "unit": "maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank, ws, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import zcmir_b200 as zc
+
+    m, f, H = make_pair()
+    reg = zc.Registrar(half=False)
+    reg.set_images(m, f, preprocess=False)
+    sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048)
+    assert (sm.dx, sm.dy) == (-H[0, 2], -H[1, 2]), (sm.dx, sm.dy, H)
+
+    # device-timed maps: the 45-correlation workload, and the 28-correlation ("none") one
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    barrier()
+    reg.gpu_counts()
+    with Clocks(local) as clk:
+        r = reg.bench_maps(np.eye(3), flags=3, cap=2048, warmup=args.warmup, steps=args.steps)
+    launches = reg.gpu_counts()["launches"]
+    barrier()
+    ms = r["ms_per_map"]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    reg.configure(smi_features="three")
+    r28 = reg.bench_maps(np.eye(3), flags=3, cap=2048, warmup=1, steps=max(3, args.steps // 2))
+    reg.configure(smi_features="laplacian")
+
+    # e2e: the public API from pinned host buffers, map back into pinned host memory
+    pm = torch.empty(m.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pf = torch.empty(f.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pm[:] = m
+    pf[:] = f
+    out = torch.empty(2048 * 2048, dtype=torch.float32, pin_memory=True).numpy()
+    for _ in range(args.warmup):
+        reg.set_images(pm, pf, preprocess=False)
+        reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048, out=out)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        reg.set_images(pm, pf, preprocess=False)
+        e = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048, out=out)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    assert (e.dx, e.dy) == (sm.dx, sm.dy)
+
+    if rank == 0:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = peaks.get("hbm_gbs")
+        peak_kind = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        sb = stage_bytes(r)
+        top = max(r["stages_ms"], key=r["stages_ms"].get)
+        launches_of = {"canvas": 1, "fwd_rows": 2, "fwd_cols": 2, "inv_cols": 1, "inv_rows_score": 1}
+        t_launch = r["stages_ms"][top] / launches_of[top]
+        b_launch = sb[top] / launches_of[top]
+        achieved = b_launch / (t_launch * 1e-3) / 1e9
+        traffic = None
+        tf = ROOT / "profiles" / "traffic.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get(top)
+        line = {
+            "metric": METRIC, "value": ws * 1000.0 / ms, "unit": "maps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config({"parallelism": f"replicas{ws}", "none_28_correlations_maps_s": ws * 1000.0 / r28["ms_per_map"],
+                              "plan": {k: r[k] for k in ("nx", "ny", "cw", "ch", "n_real", "n_corr", "split")},
+                              "stages_ms": r["stages_ms"]}),
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": b_launch, "launch_ms": t_launch,
+                         "map_algorithmic_bytes": survey_bytes(r),
+                         "map_frac": survey_bytes(r) / (ms * 1e-3) / 1e9 / hbm},
+            "e2e": {"value": ws / e2e_s, "unit": "maps/s", "h2d_bytes_per_step": int(pm.nbytes + pf.nbytes),
+                    "d2h_bytes_per_step": int(2048 * 2048 * 4 + 88)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if ws == 1 and not args.no_cpu:
+            sec, _ = cpu_map_seconds(m, f)
+            line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "maps/s", "cores": os.cpu_count(), "kind": "port",
+                                    "sample": "one full 1024² map of the same pair (float64 oracle, scipy FFTs)"}
+        print(json.dumps(line), flush=True)
+    reg.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank, ws, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_gpu(args, rank, ws, local)
+
+
+if __name__ == "__main__":
+    main()

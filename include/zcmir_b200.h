@@ -1,0 +1,31 @@
+/* Entry points of the B200 build beyond the reference's zc_* ABI (libzcmir.so). They have no
+ * counterpart in the reference: benchmarking and host-logic checks that need no GPU. */
+#ifndef ZCMIR_B200_H
+#define ZCMIR_B200_H
+
+#include "zcmir.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Time `steps` shift maps at pose H after `warmup` untimed ones, with the images' features
+ * resident on the GPU and an L2 flush between timed maps (outside the timed spans). flags: 1
+ * exact, 2 calibrated; cap as zc_shift_map (0: 1024). out[16] (out_len ≥ 16): [0] ms per map
+ * (CUDA events), [1..5] per-stage ms (canvas, forward rows, forward columns, inverse columns,
+ * inverse rows + score), [8..15] nx, ny, cw, ch, real planes, correlations, row split, canvas
+ * width. 0 / -1 with zc_error. */
+int32_t zcb_bench_maps(zc_engine* e, const double H[9], uint32_t flags, uint32_t cap, uint32_t warmup, uint32_t steps,
+                       double* out, size_t out_len);
+
+/* Settings without an engine: apply the JSON object `json` onto the defaults and write the
+ * resulting settings JSON to out (the full length is returned through *out_len). 0 on success;
+ * -1 with the message in err (its length through *err_len) when the JSON is rejected. */
+int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, size_t* out_len, char* err,
+                           size_t err_cap, size_t* err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZCMIR_B200_H */

@@ -1,0 +1,355 @@
+"""zcmir_b200: the SMI path of zcmir (square-loss mutual information registration), B200-native.
+
+The Python surface mirrors the reference's (python/zcmir/__init__.py, python/zcmir/api.py) for the
+SMI path: the same names, arguments, result types and errors, over the same zc_* C ABI, served by
+libzcmir.so (CUDA kernels for sm_100a).
+
+    import zcmir_b200 as zcmir
+    sm = zcmir.shift_map(moving, fixed, preprocess=False, map_res=2048)   # dense SMI shift map
+    sm.peak, sm.dx, sm.dy, sm.map
+
+Pose convention: H maps MOVING pixel coordinates to FIXED pixel coordinates, row-major, with
+(1, 1) the centre of the top-left pixel.
+"""
+import ctypes
+import json
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+__all__ = [
+    "Registrar", "ShiftMap", "Score", "Gradient", "Climb", "Search",
+    "shift_map", "score", "refine", "register", "search", "settings", "close", "__version__",
+]
+
+__version__ = "0.1.4"
+
+
+def _mat(H):
+    a = np.ascontiguousarray(np.asarray(H, dtype=np.float64).reshape(9))
+    return a, a.ctypes.data_as(_native.f64p)
+
+
+def _fp(a):
+    return a.ctypes.data_as(_native.f32p)
+
+
+@dataclass
+class Score:
+    """Pose score: the mean of the forward and inverse directions when symmetric."""
+    mean: float
+    fwd: float
+    inv: float | None
+
+
+@dataclass
+class Gradient:
+    score: float
+    fwd: float
+    inv: float | None
+    n: float
+    grad: np.ndarray
+    hess: np.ndarray | None
+
+
+@dataclass
+class ShiftMap:
+    """Dense score over every translation of the moving image about a pose.
+
+    map: ny rows × n columns, lag (0, 0) at [0, 0], negative lags wrapped (np.fft.fftshift
+    centres it); one cell spans (canvas_w / cw, canvas_h / ch) pixels. dx, dy: the peak's lag in
+    fixed pixels; ``corrected(H)`` = translate(−dx, −dy)·H.
+    """
+    peak: float
+    dx: float
+    dy: float
+    zero: float
+    n: int
+    cw: int
+    ch: int
+    canvas: tuple
+    offset: tuple
+    corr_area_px: float
+    exact: bool
+    calibrated: bool
+    map: np.ndarray | None
+    ny: int = 0
+    peak_index: int = 0
+
+    def corrected(self, H):
+        T = np.array([[1, 0, -self.dx], [0, 1, -self.dy], [0, 0, 1.0]])
+        return T @ np.asarray(H, dtype=np.float64).reshape(3, 3)
+
+
+@dataclass
+class Climb:
+    H: np.ndarray
+    score: float
+    iterations: int
+    moved: bool
+
+
+@dataclass
+class Search:
+    H: np.ndarray
+    score: float
+    previous: float
+    improved: bool
+    count_a: int
+    count_b: int
+
+
+class Registrar:
+    """One GPU engine and one image pair, whose features stay on the GPU between calls.
+
+    Keyword arguments are settings (``configure``). close() releases the engine (also on garbage
+    collection; ``with`` works too).
+    """
+
+    def __init__(self, on_event=None, **settings):
+        lib = _native.load()
+        self._lib = lib
+        self._e = lib.zc_create(b"")
+        self.on_event = on_event
+        self._events = []
+        if not self._e:
+            buf = ctypes.create_string_buffer(1024)
+            n = lib.zc_create_error(buf, 1024)
+            raise RuntimeError(buf.raw[:n].decode(errors="replace") or "zcmir: could not create the engine")
+        if settings:
+            self.configure(**settings)
+
+    # ── plumbing ──
+    def _error(self):
+        buf = ctypes.create_string_buffer(1024)
+        n = self._lib.zc_error(self._e, buf, 1024)
+        return buf.raw[:n].decode(errors="replace")
+
+    def _check(self, rc, what):
+        self._drain()
+        if rc != 0:
+            raise RuntimeError(f"{what}: {self._error() or rc}")
+
+    def _drain(self):
+        buf = ctypes.create_string_buffer(1 << 16)
+        while True:
+            n = self._lib.zc_events(self._e, buf, len(buf))
+            if n == 0:
+                break
+            for line in buf.raw[:n].decode(errors="replace").splitlines():
+                if line:
+                    ev = json.loads(line)
+                    self._events.append(ev)
+                    if self.on_event:
+                        self.on_event(ev)
+
+    def events(self):
+        self._drain()
+        out, self._events = self._events, []
+        return out
+
+    @property
+    def adapter(self):
+        buf = ctypes.create_string_buffer(256)
+        n = self._lib.zc_adapter(self._e, buf, 256)
+        return buf.raw[:n].decode(errors="replace")
+
+    # ── settings ──
+    def configure(self, **settings):
+        b = json.dumps(settings).encode()
+        self._check(self._lib.zc_configure(self._e, b, len(b)), "configure")
+
+    @property
+    def settings(self):
+        cap = 8192
+        buf = ctypes.create_string_buffer(cap)
+        n = self._lib.zc_settings(self._e, buf, cap)
+        if n > cap:
+            buf = ctypes.create_string_buffer(n)
+            n = self._lib.zc_settings(self._e, buf, n)
+        return json.loads(buf.raw[:n])
+
+    # ── images ──
+    def _set(self, side, img, preprocess):
+        a = np.asarray(img)
+        if a.dtype == np.uint8:
+            raise ValueError("uint8 images are always preprocessed (CLAHE), which this build leaves out: "
+                             "pass float gray in [0, 1] (or uint16) with preprocess=False")
+        if a.ndim == 3 and a.shape[2] in (3, 4):
+            a = a[:, :, :3].astype(np.float64) @ np.array([0.299, 0.587, 0.114])
+        if a.dtype == np.uint16:
+            a = a / 65535.0
+        if not (a.dtype == np.float32 and a.flags.c_contiguous):
+            a = np.ascontiguousarray(a, dtype=np.float32)
+        if a.ndim != 2:
+            raise ValueError("expected a gray image (h, w)")
+        h, w = a.shape
+        rc = self._lib.zc_set_image_gray(self._e, side, _fp(a), w, h, 1 if preprocess else 0)
+        self._check(rc, "set_image")
+
+    def set_moving(self, img, preprocess=True):
+        self._set(0, img, preprocess)
+
+    def set_fixed(self, img, preprocess=True):
+        self._set(1, img, preprocess)
+
+    def set_images(self, moving, fixed, preprocess=True):
+        self._set(0, moving, preprocess)
+        self._set(1, fixed, preprocess)
+
+    def image_size(self, side):
+        out = (ctypes.c_uint32 * 2)()
+        self._lib.zc_image_size(self._e, side, out)
+        return out[0], out[1]
+
+    def work_image(self, side):
+        w, h = self.image_size(side)
+        out = np.empty((h, w), np.float32)
+        self._check(self._lib.zc_work_image(self._e, side, _fp(out), out.size), "work_image")
+        return out
+
+    def features(self, side):
+        """The SMI feature planes of side 0 (moving) or 1 (fixed), (4, h, w) float32: the
+        whitened rank r, r², |∇r| and the fourth feature."""
+        w, h = self.image_size(side)
+        out = np.empty((4, h, w), np.float32)
+        self._check(self._lib.zc_features(self._e, side, _fp(out), out.size), "features")
+        return out
+
+    def moments(self, H=None):
+        a, p = self._Hp(H)
+        out = np.empty(45, np.float64)
+        self._check(self._lib.zc_moments(self._e, p, out.ctypes.data_as(_native.f64p)), "moments")
+        return out
+
+    def _map_cap(self, resolution=0):
+        n = max(int(resolution or 0), int(self.settings.get("map_res", 0)), 1024)
+        return n * n
+
+    # ── pose ──
+    @property
+    def pose(self):
+        H = (ctypes.c_double * 9)()
+        self._lib.zc_get_pose(self._e, H)
+        return np.array(list(H), np.float64).reshape(3, 3)
+
+    @pose.setter
+    def pose(self, H):
+        a, p = _mat(H)
+        self._lib.zc_set_pose(self._e, p)
+
+    def _Hp(self, H):
+        return _mat(self.pose if H is None else H)
+
+    # ── scores and maps ──
+    def score(self, H=None):
+        a, p = self._Hp(H)
+        out = np.empty(3, np.float64)
+        self._check(self._lib.zc_score(self._e, p, out.ctypes.data_as(_native.f64p)), "score")
+        return Score(float(out[0]), float(out[1]), None if math.isnan(out[2]) else float(out[2]))
+
+    def gradient(self, H=None, hess=False):
+        a, p = self._Hp(H)
+        r = _native.GradResult()
+        self._check(self._lib.zc_gradient(self._e, p, 1 if hess else 0, ctypes.byref(r)), "gradient")
+        nk = r.nk
+        g = np.array(r.grad[:nk])
+        Hm = np.array(r.hess[: nk * nk]).reshape(nk, nk) if r.has_hess else None
+        return Gradient(r.score, r.fwd, None if math.isnan(r.inv) else r.inv, r.n, g, Hm)
+
+    def shift_map(self, H=None, *, exact=None, calibrated=None, resolution=1024, return_map=True, out=None):
+        """Score every translation of the moving image about pose H. Without exact / calibrated the
+        settings decide (score, resolution, overlap floor); with them those are explicit and there
+        is no overlap floor. ``out``: an optional float32 buffer (≥ ny·n) the map is written to."""
+        a, p = self._Hp(H)
+        r = _native.ShiftResult()
+        buf = None
+        if return_map:
+            buf = out if out is not None else np.empty(self._map_cap(resolution), np.float32)
+        mp, ml = (_fp(buf), buf.size) if buf is not None else (None, 0)
+        if exact is None and calibrated is None:
+            rc = self._lib.zc_shift_map_set(self._e, p, ctypes.byref(r), mp, ml)
+        else:
+            flags = (1 if (exact is None or exact) else 0) | (2 if (calibrated is None or calibrated) else 0)
+            rc = self._lib.zc_shift_map(self._e, p, flags, resolution, ctypes.byref(r), mp, ml)
+        self._check(rc, "shift_map")
+        ny = r.n_y or r.n
+        m = None
+        if buf is not None:
+            m = buf[: r.n * ny].reshape(ny, r.n)
+            if out is None:
+                m = m.copy()
+        return ShiftMap(
+            peak=r.peak, dx=r.dx, dy=r.dy, zero=r.zero, n=r.n, cw=r.cw, ch=r.ch,
+            canvas=(r.canvas_w, r.canvas_h), offset=(r.ox, r.oy), corr_area_px=r.corr_area_px,
+            exact=bool(r.exact), calibrated=bool(r.calibrated), map=m, ny=ny, peak_index=r.peak_index,
+        )
+
+    def canvas(self, H=None, inverse=False):
+        a, p = self._Hp(H)
+        c = _native.Canvas()
+        self._check(self._lib.zc_canvas(self._e, p, 1 if inverse else 0, ctypes.byref(c)), "canvas")
+        return (c.ox, c.oy), (c.ow, c.oh), np.array(list(c.Hc)).reshape(3, 3)
+
+    # ── optimisation ──
+    def climb(self):
+        r = _native.ClimbResult()
+        self._check(self._lib.zc_climb(self._e, ctypes.byref(r)), "climb")
+        return Climb(np.array(list(r.H)).reshape(3, 3), r.score, r.iterations, bool(r.moved))
+
+    def search(self):
+        r = _native.SearchResult()
+        self._check(self._lib.zc_search(self._e, ctypes.byref(r)), "search")
+        return Search(np.array(list(r.H)).reshape(3, 3), r.score, r.prev, bool(r.improved), r.count_a, r.count_b)
+
+    # ── profiling ──
+    def profile(self, on=True):
+        return bool(self._lib.zc_profile(self._e, 1 if on else 0))
+
+    def profile_report(self):
+        buf = ctypes.create_string_buffer(1 << 14)
+        n = self._lib.zc_profile_report(self._e, buf, len(buf))
+        return buf.raw[:n].decode()
+
+    def gpu_counts(self):
+        out = (ctypes.c_uint32 * 4)()
+        self._lib.zc_gpu_counts(self._e, out)
+        return dict(zip(("launches", "submits", "reads", "waits"), list(out)))
+
+    def bench_maps(self, H=None, *, flags=3, cap=1024, warmup=3, steps=10):
+        """Device-timed maps (CUDA events, inputs resident, L2 flushed between timed maps):
+        ms per map, per-stage ms and the plan."""
+        a, p = self._Hp(H)
+        out = np.zeros(16, np.float64)
+        self._check(self._lib.zcb_bench_maps(self._e, p, flags, cap, warmup, steps, out.ctypes.data_as(_native.f64p), 16),
+                    "bench_maps")
+        stages = ("canvas", "fwd_rows", "fwd_cols", "inv_cols", "inv_rows_score")
+        return {
+            "ms_per_map": float(out[0]), "stages_ms": dict(zip(stages, map(float, out[1:6]))),
+            "nx": int(out[8]), "ny": int(out[9]), "cw": int(out[10]), "ch": int(out[11]),
+            "n_real": int(out[12]), "n_corr": int(out[13]), "split": int(out[14]), "canvas_w": int(out[15]),
+        }
+
+    # ── lifetime ──
+    def close(self):
+        if getattr(self, "_e", None):
+            self._lib.zc_destroy(self._e)
+            self._e = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+from .api import close, refine, register, score, search, settings, shift_map  # noqa: E402

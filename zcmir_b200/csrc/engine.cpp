@@ -1,0 +1,480 @@
+// The B200 SMI engine: images, features and the shift-map schedule.
+// Host schedule restated from the reference's src/engine.zig (setImageGray 430-434, bake 322-341,
+// shiftMapOpts 795-819, shiftMap 822-829) and src/smi.zig (prepare 348-400, shiftMapFrom 552-572).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace zc {
+
+const char* const kStageNames[kNumStages] = {"canvas", "fwd_rows", "fwd_cols", "inv_cols", "inv_rows_score"};
+
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+Engine::Engine(int dev) : device(dev) {
+    cudaSetDevice(dev);
+    cudaGetDeviceProperties(&prop, dev);
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+}
+
+Engine::~Engine() {
+    cudaStreamSynchronize(st);
+    for (auto& s : side) {
+        s.raw.release();
+        s.work.release();
+        s.feat.release();
+        s.mag.release();
+        s.stack.release();
+    }
+    for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
+                      &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_})
+        b->release();
+    for (auto& kv : tw_) cudaFree(kv.second);
+    cudaStreamDestroy(st);
+}
+
+bool Engine::fail(const std::string& m) {
+    if (err.empty()) err = m;
+    return false;
+}
+
+bool Engine::cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    return fail(std::string(what) + ": CUDA error: " + cudaGetErrorString(e));
+}
+
+// ── images and features ──────────────────────────────────────────────────────────────────────
+
+bool Engine::set_image(int s, const float* data, int w, int h, bool preprocess) {
+    // the reference's setImageGray checks (src/engine.zig:430-434)
+    if (s < 0 || s > 1 || w < 8 || h < 8 || !data) return fail("set_image_gray: BadImage");
+    if (preprocess && (set.b("clahe") || set.b("band") || set.b("invert")))
+        return fail(
+            "set_image_gray: preprocessing (CLAHE, band pass, invert) is not part of this build's SMI path; "
+            "pass preprocess=False, or configure clahe=false, band=false, invert=false");
+    Side& sd = side[s];
+    const size_t n = (size_t)w * h;
+    if (!cuda_ok(sd.raw.ensure(n * 4), "set_image_gray")) return false;
+    if (!cuda_ok(cudaMemcpyAsync(sd.raw.p, data, n * 4, cudaMemcpyHostToDevice, st), "set_image_gray")) return false;
+    sd.has = true;
+    sd.w = w;
+    sd.h = h;
+    sd.preprocess = preprocess;
+    sd.built = false;
+    return build_side(s);
+}
+
+bool Engine::build_side(int s) {
+    Side& sd = side[s];
+    const size_t n = (size_t)sd.w * sd.h;
+    const std::string& fm = set.e("smi_features");
+    const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
+    const bool half = set.b("half");
+    const int ntiles = ((sd.w + 31) / 32) * ((sd.h + 31) / 32);
+    bool ok = cuda_ok(sd.work.ensure(n * 4), "features") && cuda_ok(sd.feat.ensure(n * 16), "features") &&
+              cuda_ok(sd.mag.ensure(n * 4), "features") && cuda_ok(sd.stack.ensure(n * 20), "features") &&
+              cuda_ok(rank_tmp_.ensure(n * 4), "features") && cuda_ok(fs_stats_.ensure(22 * 8), "features") &&
+              cuda_ok(fs_hist_.ensure(256 * 4), "features") && cuda_ok(fs_wt_.ensure(20 * 4), "features") &&
+              cuda_ok(fs_acfpart_.ensure((size_t)ntiles * 1156 * 4), "features") &&
+              cuda_ok(fs_acf_.ensure(1156 * 8), "features");
+    if (!ok) return false;
+    fs_.stats = fs_stats_.as<double>();
+    fs_.hist = fs_hist_.as<unsigned>();
+    fs_.wt = fs_wt_.as<float>();
+    fs_.acf_part = fs_acfpart_.as<float>();
+    fs_.acf_part_cap = fs_acfpart_.cap / 4;
+    fs_.acf = fs_acf_.as<double>();
+    if (!cuda_ok(cudaMemcpyAsync(sd.work.p, sd.raw.p, n * 4, cudaMemcpyDeviceToDevice, st), "features")) return false;
+    if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rank_tmp_.as<float>(), sd.feat.as<float>(),
+                                sd.mag.as<float>(), sd.stack.as<float>(), fs_, st),
+                 "features"))
+        return false;
+    counts[0] += 13;
+    double acf[1156];
+    if (!cuda_ok(cudaMemcpyAsync(acf, fs_.acf, sizeof acf, cudaMemcpyDeviceToHost, st), "features")) return false;
+    if (!cuda_ok(cudaStreamSynchronize(st), "features")) return false;
+    counts[2] += 1;
+    counts[3] += 1;
+    // normalise by the zero lag (smi.wgsl:1572-1578)
+    for (int k = 0; k < 1156; ++k) sd.acf[k] = acf[k] / std::max(acf[144 * 4 + (k & 3)], 1e-12);
+    sd.built = true;
+    sd.mode = mode;
+    sd.half = half;
+    return true;
+}
+
+bool Engine::need_images() {
+    if (!side[0].has || !side[1].has) return fail("NoImages");
+    const std::string& fm = set.e("smi_features");
+    const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
+    for (int s = 0; s < 2; ++s) {
+        Side& sd = side[s];
+        if (!sd.built || sd.mode != mode || sd.half != set.b("half"))
+            if (!build_side(s)) return false;
+    }
+    return true;
+}
+
+double Engine::pair_area() const {
+    // Bartlett correlation area (smi.wgsl:1580-1595)
+    double s = 0;
+    for (int k = 0; k < 289; ++k) {
+        double ra = 0, rb = 0;
+        for (int i = 0; i < 4; ++i) {
+            ra += side[0].acf[k * 4 + i];
+            rb += side[1].acf[k * 4 + i];
+        }
+        s += ra * rb;
+    }
+    return std::max(1.0, s / 16.0);
+}
+
+bool Engine::features(int s, float* out, size_t len) {
+    if (s < 0 || s > 1 || !side[s].has) return fail("features: NoImage");
+    if (!need_images()) return false;
+    const size_t n = 4 * (size_t)side[s].w * side[s].h;
+    if (len < n) return fail("features: BufferTooSmall");
+    if (!cuda_ok(cudaMemcpyAsync(out, side[s].feat.p, n * 4, cudaMemcpyDeviceToHost, st), "features")) return false;
+    counts[2]++;
+    counts[3]++;
+    return cuda_ok(cudaStreamSynchronize(st), "features");
+}
+
+bool Engine::work_image(int s, float* out, size_t len) {
+    if (s < 0 || s > 1 || !side[s].has) return fail("work_image: NoImage");
+    Side& sd = side[s];
+    if (!sd.built && !build_side(s)) return false;
+    const size_t n = (size_t)sd.w * sd.h;
+    if (len < n) return fail("work_image: BufferTooSmall");
+    if (!cuda_ok(cudaMemcpyAsync(out, sd.work.p, n * 4, cudaMemcpyDeviceToHost, st), "work_image")) return false;
+    counts[2]++;
+    counts[3]++;
+    return cuda_ok(cudaStreamSynchronize(st), "work_image");
+}
+
+// ── FFT plans ─────────────────────────────────────────────────────────────────────────────────
+
+const float2* Engine::twiddles(int n) {
+    auto it = tw_.find(n);
+    if (it != tw_.end()) return it->second;
+    std::vector<float2> h(n);
+    for (int t = 0; t < n; ++t) {
+        const double a = -2.0 * M_PI * (double)t / (double)n;
+        h[t] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    float2* d = nullptr;
+    if (cudaMalloc(&d, (size_t)n * sizeof(float2)) != cudaSuccess) return nullptr;
+    // stream-ordered before every kernel that reads it (pageable source: staged before return)
+    if (cudaMemcpyAsync(d, h.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        cudaFree(d);
+        return nullptr;
+    }
+    tw_[n] = d;
+    return d;
+}
+
+bool Engine::line_plan(int n, LinePlan& p) {
+    if (n < 2 || n > kMaxLine) return fail("FFT length " + std::to_string(n) + " is outside 2..8192");
+    int a = 0, b = 0, m = n;
+    while (m % 2 == 0) m /= 2, ++a;
+    while (m % 3 == 0) m /= 3, ++b;
+    if (m != 1) return fail("FFT length " + std::to_string(n) + " is not 2^a·3^b (fft_sizes=ladder lengths only)");
+    p = LinePlan{};
+    p.n = n;
+    // power of two: ⌈a/4⌉ stages of radix 16/8/4/2 with balanced bit counts; then the 3s
+    const int s2 = (a + 3) / 4;
+    for (int i = 0; i < s2; ++i) {
+        const int bits = a / s2 + (i < a % s2 ? 1 : 0);
+        p.radix[p.nst++] = 1 << bits;
+    }
+    for (int i = 0; i < b; ++i) p.radix[p.nst++] = 3;
+    int tl = (n + 15) / 16;
+    tl = ((tl + 31) / 32) * 32;
+    p.tl = tl;
+    // every stage's butterflies must fit in its threads (BM·tl ≥ n/R)
+    for (int s = 0; s < p.nst; ++s) {
+        const int R = p.radix[s];
+        const int bm = R == 3 ? 6 : 16 / R;
+        if (n / R > bm * tl) return fail("internal: FFT plan does not fit its threads");
+    }
+    p.tw = twiddles(n);
+    if (!p.tw) return fail("twiddles: out of device memory");
+    return true;
+}
+
+// ── shift map ─────────────────────────────────────────────────────────────────────────────────
+
+bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap, double min_overlap, MapJob& job) {
+    if (!need_images()) return false;
+    if (set.e("metric") != "smi")
+        return fail("shift_map: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    const bool ladder = set.e("fft_sizes") == "ladder";
+    if (!ladder) return fail("shift_map: fft_sizes=\"compact\" is not supported by this build (use \"ladder\")");
+    job.exact = exact;
+    job.calibrated = exact && calibrated;
+    job.fr = reg_frame(Hm, side[0].w, side[0].h, side[1].w, side[1].h);
+    job.Hc = canvas_H(Hm, job.fr.ox, job.fr.oy);
+    MapPlan mp;
+    if (cap == 0) {
+        mp = auto_shift_plan(job.fr.w, job.fr.h);
+    } else {
+        // capN (src/smi.zig:414-422) with this build's longest line, 8192
+        const unsigned c = largest_smooth(std::min<unsigned>(cap, kMaxLine), ladder);
+        mp = linear_corr_plan_rect(job.fr.w, job.fr.h, c, ladder);
+    }
+    MapGeom& g = job.g;
+    g.W = job.fr.w;
+    g.Hh = job.fr.h;
+    g.ox = job.fr.ox;
+    g.oy = job.fr.oy;
+    g.cw = mp.cw;
+    g.ch = mp.ch;
+    g.nx = mp.nx;
+    g.ny = mp.ny;
+    g.WP = ((g.nx / 2 + 1) + 7) / 8 * 8;
+    job.identity_grid = (g.cw == g.W && g.ch == g.Hh);
+    // correlation plan (src/smi.zig:90-158)
+    const bool three = side[0].mode == 1;
+    int lst_a[45], lst_b[45], nl = 0;
+    lst_a[nl] = 0, lst_b[nl++] = 0;
+    for (int i = 0; i < 4; ++i) lst_a[nl] = 1 + i, lst_b[nl++] = 0;
+    for (int j = 0; j < 4; ++j) lst_a[nl] = 0, lst_b[nl++] = 1 + j;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) lst_a[nl] = 1 + i, lst_b[nl++] = 1 + j;
+    if (exact) {
+        for (int k = 0; k < 10; ++k) lst_a[nl] = 5 + k, lst_b[nl++] = 0;
+        for (int k = 0; k < 10; ++k) lst_a[nl] = 0, lst_b[nl++] = 5 + k;
+    }
+    const int n_planes = exact ? 15 : 5;
+    int slot[15];
+    CorrPlanDev& P = job.plan;
+    P = CorrPlanDev{};
+    for (int pl = 0; pl < n_planes; ++pl) {
+        const bool fourth = pl == 4 || pl == 8 || pl == 11 || pl == 13 || pl == 14;
+        if (three && fourth) {
+            slot[pl] = -1;
+            continue;
+        }
+        slot[pl] = P.n_real;
+        P.planes[P.n_real++] = pl;
+    }
+    for (int c = 0; c < nl; ++c) {
+        const int sa = slot[lst_a[c]], sb = slot[lst_b[c]];
+        if (sa < 0 || sb < 0) continue;
+        P.ca[P.n_corr] = sa;
+        P.cb[P.n_corr] = sb;
+        P.cnum[P.n_corr] = c;
+        P.n_corr++;
+    }
+    if (!line_plan(g.nx, job.row) || !line_plan(g.ny, job.col)) return false;
+    job.S = row_split(g.nx, P.n_corr);
+    if (job.S == 0) return fail("shift_map: row of " + std::to_string(g.nx) + " does not split to fit shared memory");
+    if (!line_plan(g.nx / job.S, job.line)) return false;
+    const unsigned floor_n = min_overlap > 0 ? (unsigned)std::floor(min_overlap * (double)g.cw * (double)g.ch) : 0u;
+    const double gcell = (double)g.W / (double)g.cw;
+    CombineParams& cp = job.cp;
+    cp.exact = exact ? 1 : 0;
+    cp.calib = job.calibrated ? 1 : 0;
+    cp.nf = three ? 3 : 4;
+    cp.min_n = (float)std::max(12u, floor_n);
+    cp.area = std::max(1.0, pair_area() * (1.0 / (gcell * gcell)));
+    cp.ridge = 1e-4;
+    cp.inv_nn = 1.0 / ((double)g.nx * (double)g.ny);
+    return true;
+}
+
+bool Engine::run_map(MapJob& job, cudaEvent_t* ev) {
+    const MapGeom& g = job.g;
+    const size_t cn = (size_t)g.W * g.Hh, gn = (size_t)g.cw * g.ch;
+    const size_t hs = (size_t)job.plan.n_real * g.ny * g.WP * sizeof(float2);
+    const size_t qs = (size_t)job.plan.n_corr * g.ny * g.WP * sizeof(float2);
+    bool ok = cuda_ok(canvas_a_.ensure(cn * 20), "shift_map") && cuda_ok(canvas_b_.ensure(cn * 20), "shift_map") &&
+              cuda_ok(half_a_.ensure(hs), "shift_map") && cuda_ok(half_b_.ensure(hs), "shift_map") &&
+              cuda_ok(q_.ensure(qs), "shift_map") && cuda_ok(map_.ensure((size_t)g.nx * g.ny * 4), "shift_map") &&
+              cuda_ok(res_.ensure(64), "shift_map");
+    if (ok && !job.identity_grid)
+        ok = cuda_ok(grid_a_.ensure(gn * 20), "shift_map") && cuda_ok(grid_b_.ensure(gn * 20), "shift_map");
+    if (!ok) return false;
+    auto rec = [&](int i) {
+        if (ev) cudaEventRecord(ev[i], st);
+    };
+    const Side &A = side[0], &B = side[1];
+    const Mat3 hi = inv3_plain(job.Hc);
+    float hif[9];
+    for (int i = 0; i < 9; ++i) hif[i] = (float)hi[i];
+    const bool okdet = std::fabs(det3(job.Hc)) >= 1e-12;
+    char* res = res_.as<char>();
+    unsigned long long* best = reinterpret_cast<unsigned long long*>(res);
+    float* zero = reinterpret_cast<float*>(res + 8);
+    double* n00 = reinterpret_cast<double*>(res + 16);
+    rec(0);
+    if (!cuda_ok(warp_stack(A.stack.as<float>(), A.w, A.h, hif, okdet, g.W, g.Hh, canvas_a_.as<float>(), st), "canvas") ||
+        !cuda_ok(paste_stack(B.stack.as<float>(), B.w, B.h, g.ox, g.oy, g.W, g.Hh, canvas_b_.as<float>(), st), "canvas"))
+        return false;
+    const float* ga = canvas_a_.as<float>();
+    const float* gb = canvas_b_.as<float>();
+    if (!job.identity_grid) {
+        if (!cuda_ok(resample_grid(ga, g.W, g.Hh, g.cw, g.ch, grid_a_.as<float>(), st), "resample") ||
+            !cuda_ok(resample_grid(gb, g.W, g.Hh, g.cw, g.ch, grid_b_.as<float>(), st), "resample"))
+            return false;
+        ga = grid_a_.as<float>();
+        gb = grid_b_.as<float>();
+    }
+    if (!cuda_ok(lag0_count(ga, gb, g.cw, g.ch, n00, st), "lag0") ||
+        !cuda_ok(cudaMemsetAsync(best, 0, 8, st), "shift_map"))
+        return false;
+    rec(1);
+    // the two sides' forward transforms: rows of both, then columns of both
+    if (!cuda_ok(forward_rows(ga, g, job.plan, job.row, half_a_.as<float2>(), st), "forward rows") ||
+        !cuda_ok(forward_rows(gb, g, job.plan, job.row, half_b_.as<float2>(), st), "forward rows"))
+        return false;
+    rec(2);
+    if (!cuda_ok(forward_cols(half_a_.as<float2>(), g, job.plan, job.col, st), "forward columns") ||
+        !cuda_ok(forward_cols(half_b_.as<float2>(), g, job.plan, job.col, st), "forward columns"))
+        return false;
+    rec(3);
+    if (!cuda_ok(inverse_columns(half_a_.as<float2>(), half_b_.as<float2>(), g, job.plan, job.col, q_.as<float2>(), st),
+                 "inverse columns"))
+        return false;
+    rec(4);
+    if (!cuda_ok(inverse_rows_score(q_.as<float2>(), g, job.plan, job.line, job.S, twiddles(g.nx), job.cp, n00,
+                                    map_.as<float>(), best, zero, st),
+                 "inverse rows"))
+        return false;
+    rec(5);
+    counts[0] += job.identity_grid ? 10 : 12;
+    return true;
+}
+
+bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap, double min_overlap,
+                       zc_shift_result* out, float* map, size_t map_len) {
+    MapJob job;
+    if (!plan_map(Hm, exact, calibrated, cap, min_overlap, job)) return false;
+    const size_t nn = (size_t)job.g.nx * job.g.ny;
+    if (map && map_len < nn) return fail("shift_map: MapTooSmall");
+    cudaEvent_t ev[kNumStages + 1];
+    if (profiling)
+        for (auto& e : ev) cudaEventCreate(&e);
+    if (!run_map(job, profiling ? ev : nullptr)) return false;
+    unsigned char host[24];
+    if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 24, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
+    counts[2]++;
+    if (map) {
+        if (!cuda_ok(cudaMemcpyAsync(map, map_.p, nn * 4, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
+        counts[2]++;
+    }
+    if (!cuda_ok(cudaStreamSynchronize(st), "shift_map")) return false;
+    counts[1]++;
+    counts[3]++;
+    if (profiling) {
+        for (int i = 0; i < kNumStages; ++i) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            auto& p = prof[kStageNames[i]];
+            p.first += ms;
+            p.second++;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+    unsigned long long best;
+    float zero;
+    memcpy(&best, host, 8);
+    memcpy(&zero, host + 8, 4);
+    const MapGeom& g = job.g;
+    zc_shift_result r{};
+    r.n = g.nx;
+    r.n_y = g.ny;
+    r.cw = g.cw;
+    r.ch = g.ch;
+    r.canvas_w = g.W;
+    r.canvas_h = g.Hh;
+    r.ox = g.ox;
+    r.oy = g.oy;
+    r.peak = key_float((uint32_t)(best >> 32));
+    r.zero = zero;
+    r.corr_area_px = pair_area();
+    r.exact = job.exact;
+    r.calibrated = job.calibrated;
+    const uint32_t idx = 0xffffffffu - (uint32_t)(best & 0xffffffffu);
+    if (best != 0 && idx < nn) {
+        const int64_t py = idx / g.nx, px = idx % g.nx;
+        const int64_t lx = px <= g.nx / 2 ? px : px - g.nx;
+        const int64_t ly = py <= g.ny / 2 ? py : py - g.ny;
+        r.peak_index = idx;
+        r.dx = (double)lx * ((double)g.W / (double)g.cw);
+        r.dy = (double)ly * ((double)g.Hh / (double)g.ch);
+    }
+    *out = r;
+    return true;
+}
+
+bool Engine::shift_map_settings(const Mat3& Hm, zc_shift_result* out, float* map, size_t map_len) {
+    // mapOpts (src/engine.zig:287-293)
+    return shift_map(Hm, set.b("exact"), set.b("calibrated"), set.u("map_res"), set.f("min_overlap"), out, map, map_len);
+}
+
+bool Engine::bench_maps(const Mat3& Hm, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
+                        size_t out_len) {
+    if (out_len < 16) return fail("bench_maps: output needs 16 doubles");
+    MapJob job;
+    if (!plan_map(Hm, (flags & 1) != 0, (flags & 2) != 0, cap, 0.0, job)) return false;
+    // an L2 flush between timed maps: write a buffer larger than the 126 MB L2
+    const size_t flush_bytes = (size_t)256 << 20;
+    if (!cuda_ok(flush_.ensure(flush_bytes), "bench_maps")) return false;
+    std::vector<cudaEvent_t> ev((size_t)(kNumStages + 1) * std::max(steps, 1u));
+    for (auto& e : ev) cudaEventCreate(&e);
+    for (unsigned i = 0; i < warmup; ++i)
+        if (!run_map(job, nullptr)) return false;
+    for (unsigned i = 0; i < steps; ++i) {
+        cudaMemsetAsync(flush_.p, (int)(i & 0xff), flush_bytes, st);
+        if (!run_map(job, &ev[(size_t)i * (kNumStages + 1)])) return false;
+    }
+    if (!cuda_ok(cudaStreamSynchronize(st), "bench_maps")) return false;
+    double stage[kNumStages] = {0}, total = 0;
+    for (unsigned i = 0; i < steps; ++i) {
+        cudaEvent_t* e = &ev[(size_t)i * (kNumStages + 1)];
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e[0], e[kNumStages]);
+        total += ms;
+        for (int s = 0; s < kNumStages; ++s) {
+            cudaEventElapsedTime(&ms, e[s], e[s + 1]);
+            stage[s] += ms;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (size_t i = 0; i < out_len; ++i) out[i] = 0;
+    out[0] = total / std::max(steps, 1u);
+    for (int s = 0; s < kNumStages; ++s) out[1 + s] = stage[s] / std::max(steps, 1u);
+    out[8] = job.g.nx;
+    out[9] = job.g.ny;
+    out[10] = job.g.cw;
+    out[11] = job.g.ch;
+    out[12] = job.plan.n_real;
+    out[13] = job.plan.n_corr;
+    out[14] = job.S;
+    out[15] = job.g.W;
+    return true;
+}
+
+}  // namespace zc

@@ -1,0 +1,116 @@
+// The B200 SMI engine behind the zc_* C ABI: two images with their resident features, the pose,
+// the settings, and the shift-map schedule on one CUDA stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <deque>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/zcmir.h"
+#include "geom.hpp"
+#include "kernels.hpp"
+#include "settings.hpp"
+
+namespace zc {
+
+// A device allocation that grows on demand (never shrinks until release).
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct Side {
+    bool has = false;
+    int w = 0, h = 0;
+    bool preprocess = false;
+    DevBuf raw;    // the image as uploaded (f32 gray)
+    DevBuf work;   // the work image the features are built from (f16-quantised when half)
+    DevBuf feat;   // 4 whitened planes, plane-major
+    DevBuf mag;    // Sobel magnitude of the rank
+    DevBuf stack;  // [1, f0..f3]
+    std::array<double, 1156> acf{};  // normalised autocorrelation, 289 lags × 4 planes
+    bool built = false;
+    int mode = -1;
+    bool half = false;
+};
+
+// One map's plan and device-side description.
+struct MapJob {
+    Frame fr;
+    Mat3 Hc;
+    MapGeom g;
+    CorrPlanDev plan;
+    LinePlan row, col, line;
+    int S;
+    CombineParams cp;
+    bool identity_grid;
+    bool exact, calibrated;
+};
+
+// Stages of a map timed by the profiler / the benchmark entry point.
+enum Stage { kCanvas = 0, kFwdRows, kFwdCols, kInvCols, kInvRows, kNumStages };
+extern const char* const kStageNames[kNumStages];
+
+class Engine {
+  public:
+    explicit Engine(int device);
+    ~Engine();
+
+    Settings set;
+    Mat3 H = mat_identity();
+    Side side[2];
+    std::string err;
+    bool cancel = false;
+    std::deque<std::string> events;
+
+    int device = 0;
+    cudaDeviceProp prop{};
+    cudaStream_t st = nullptr;
+
+    // counters since the last zc_gpu_counts: launches, submits, reads, waits
+    uint32_t counts[4] = {0, 0, 0, 0};
+    bool profiling = false;
+    std::map<std::string, std::pair<double, uint32_t>> prof;  // name → (ms, count)
+
+    bool fail(const std::string& m);
+    bool cuda_ok(cudaError_t e, const char* what);
+
+    // images and features
+    bool set_image(int s, const float* data, int w, int h, bool preprocess);
+    bool need_images();
+    bool features(int s, float* out, size_t len);
+    bool work_image(int s, float* out, size_t len);
+    double pair_area() const;
+
+    // maps
+    bool plan_map(const Mat3& H, bool exact, bool calibrated, unsigned cap, double min_overlap, MapJob& job);
+    bool run_map(MapJob& job, cudaEvent_t* ev /* kNumStages+1 events or null */);
+    bool shift_map(const Mat3& H, bool exact, bool calibrated, unsigned cap, double min_overlap, zc_shift_result* out,
+                   float* map, size_t map_len);
+    bool shift_map_settings(const Mat3& H, zc_shift_result* out, float* map, size_t map_len);
+    // benchmark: warmup + steps maps at H (device-resident inputs), per-step CUDA-event times
+    bool bench_maps(const Mat3& H, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
+                    size_t out_len);
+
+  private:
+    bool build_side(int s);
+    bool line_plan(int n, LinePlan& p);
+    const float2* twiddles(int n);
+
+    FeatScratch fs_;
+    DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
+    DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
+    std::map<int, float2*> tw_;
+};
+
+}  // namespace zc

@@ -1,0 +1,341 @@
+// The zc_* C ABI of the B200 engine (the reference's src/exports.zig and src/native_api.zig):
+// every name the reference's ctypes loader binds (python/zcmir/_native.py:79-133), with the same
+// argument meanings, struct layouts, return values and error reporting (0 / -1 and zc_error).
+// Calls outside this build's SMI path return their failure value with a message saying so.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "../../include/zcmir_b200.h"
+#include "engine.hpp"
+
+struct zc_engine : zc::Engine {
+    using zc::Engine::Engine;
+};
+
+static_assert(sizeof(zc_shift_result) == 88, "ShiftResult layout");
+static_assert(sizeof(zc_rs_result) == 96, "RsResult layout");
+static_assert(sizeof(zc_grad_result) == 616, "GradResult layout");
+static_assert(sizeof(zc_climb_result) == 88, "ClimbResult layout");
+static_assert(sizeof(zc_detect_result) == 16, "DetectResult layout");
+static_assert(sizeof(zc_match_result) == 112, "MatchResult layout");
+static_assert(sizeof(zc_search_result) == 104, "SearchResult layout");
+static_assert(sizeof(zc_canvas_info) == 88, "Canvas layout");
+
+namespace {
+
+char g_create_err[512];
+size_t g_create_err_len = 0;
+
+size_t copy_out(const std::string& s, char* buf, size_t cap) {
+    const size_t n = std::min(s.size(), cap);
+    if (buf && n) memcpy(buf, s.data(), n);
+    return n;
+}
+
+zc::Mat3 mat(const double* H) {
+    zc::Mat3 m;
+    for (int i = 0; i < 9; ++i) m[i] = H[i];
+    return m;
+}
+
+int32_t unsupported(zc_engine* e, const char* what) {
+    if (e) e->fail(std::string(what) + ": not part of this build (the B200 SMI path: maps, scores, refine, sweep)");
+    return -1;
+}
+
+template <class F>
+int32_t guarded(zc_engine* e, const char* what, F&& f) {
+    if (!e) return -1;
+    e->err.clear();
+    try {
+        return f() ? 0 : -1;
+    } catch (const std::exception& x) {
+        e->fail(std::string(what) + ": " + x.what());
+        return -1;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zc_version(void) { return "0.1.4"; }
+
+zc_engine* zc_create(const char* /*wgpu_path: the reference's WebGPU library, unused here*/) {
+    g_create_err_len = 0;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        const std::string m = std::string("GPU init failed: no CUDA device (") + cudaGetErrorString(e) + ")";
+        g_create_err_len = copy_out(m, g_create_err, sizeof g_create_err);
+        return nullptr;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    try {
+        return new zc_engine(dev);
+    } catch (const std::exception& x) {
+        const std::string m = std::string("engine init failed: ") + x.what();
+        g_create_err_len = copy_out(m, g_create_err, sizeof g_create_err);
+        return nullptr;
+    }
+}
+
+size_t zc_create_error(char* buf, size_t cap) {
+    const size_t n = std::min(g_create_err_len, cap);
+    if (n) memcpy(buf, g_create_err, n);
+    return n;
+}
+
+void zc_destroy(zc_engine* e) { delete e; }
+
+size_t zc_adapter(zc_engine* e, char* buf, size_t cap) {
+    if (!e) return 0;
+    char s[256];
+    snprintf(s, sizeof s, "%s (CUDA, sm_%d%d, %d SMs, %.0f GB)", e->prop.name, e->prop.major, e->prop.minor,
+             e->prop.multiProcessorCount, (double)e->prop.totalGlobalMem / 1e9);
+    return copy_out(s, buf, cap);
+}
+
+size_t zc_error(zc_engine* e, char* buf, size_t cap) {
+    if (!e) return 0;
+    const size_t n = copy_out(e->err, buf, cap);
+    e->err.clear();
+    return n;
+}
+
+int32_t zc_configure(zc_engine* e, const char* json, size_t len) {
+    return guarded(e, "configure", [&] {
+        std::string m;
+        if (!e->set.apply(json, len, m)) return e->fail(m);
+        return true;
+    });
+}
+
+size_t zc_settings(zc_engine* e, char* buf, size_t cap) {
+    if (!e) return 0;
+    const std::string j = e->set.to_json();
+    copy_out(j, buf, cap);
+    return j.size();
+}
+
+int32_t zc_set_image_gray(zc_engine* e, uint32_t side, const float* data, uint32_t w, uint32_t h,
+                          uint32_t preprocess) {
+    return guarded(e, "set_image_gray", [&] { return e->set_image((int)side, data, (int)w, (int)h, preprocess != 0); });
+}
+
+int32_t zc_set_image(zc_engine* e, uint32_t side, const float* data, uint32_t w, uint32_t h) {
+    return zc_set_image_gray(e, side, data, w, h, 0);
+}
+
+int32_t zc_set_image_rgba(zc_engine* e, uint32_t, const uint8_t*, uint32_t, uint32_t) {
+    if (e) e->err.clear();
+    return unsupported(e, "set_image_rgba (RGBA images are always preprocessed with CLAHE; pass float gray with "
+                          "preprocess=False)");
+}
+
+int32_t zc_work_image(zc_engine* e, uint32_t side, float* out, size_t len) {
+    return guarded(e, "work_image", [&] { return e->work_image((int)side, out, len); });
+}
+
+int32_t zc_features(zc_engine* e, uint32_t side, float* out, size_t len) {
+    return guarded(e, "features", [&] { return e->features((int)side, out, len); });
+}
+
+void zc_image_size(zc_engine* e, uint32_t side, uint32_t out[2]) {
+    if (!e || side > 1 || !e->side[side].has) {
+        out[0] = out[1] = 0;
+        return;
+    }
+    out[0] = (uint32_t)e->side[side].w;
+    out[1] = (uint32_t)e->side[side].h;
+}
+
+void zc_swap(zc_engine* e) {
+    if (e) std::swap(e->side[0], e->side[1]);
+}
+
+int32_t zc_moments(zc_engine* e, const double*, double*) { return unsupported(e, "moments"); }
+int32_t zc_score(zc_engine* e, const double*, double*) { return unsupported(e, "score"); }
+int32_t zc_gradient(zc_engine* e, const double*, uint32_t, zc_grad_result*) { return unsupported(e, "gradient"); }
+
+int32_t zc_shift_map(zc_engine* e, const double H[9], uint32_t flags, uint32_t cap, zc_shift_result* out, float* map,
+                     size_t map_len) {
+    // explicit flags (1 exact, 2 calibrated), no overlap floor; cap 0 = the 1024 default
+    // (src/engine.zig:822-829)
+    return guarded(e, "shift_map", [&] {
+        return e->shift_map(mat(H), (flags & 1) != 0, (flags & 2) != 0, cap == 0 ? zc::kMapCap : cap, 0.0, out, map,
+                            map_len);
+    });
+}
+
+int32_t zc_shift_map_set(zc_engine* e, const double H[9], zc_shift_result* out, float* map, size_t map_len) {
+    return guarded(e, "shift_map", [&] { return e->shift_map_settings(mat(H), out, map, map_len); });
+}
+
+int32_t zc_rs_map(zc_engine* e, const double*, const double*, uint32_t, zc_rs_result*, float*, float*, float*, size_t) {
+    return unsupported(e, "rs_map");
+}
+
+void zc_set_pose(zc_engine* e, const double H[9]) {
+    if (e) e->H = mat(H);
+}
+
+void zc_get_pose(zc_engine* e, double H[9]) {
+    if (e)
+        for (int i = 0; i < 9; ++i) H[i] = e->H[i];
+}
+
+int32_t zc_climb(zc_engine* e, zc_climb_result*) { return unsupported(e, "climb"); }
+int32_t zc_search(zc_engine* e, zc_search_result*) { return unsupported(e, "search"); }
+
+void zc_cancel(zc_engine* e) {
+    if (e) e->cancel = true;
+}
+
+size_t zc_events(zc_engine* e, char* buf, size_t cap) {
+    if (!e) return 0;
+    size_t n = 0;
+    while (!e->events.empty()) {
+        const std::string& l = e->events.front();
+        if (n + l.size() + 1 > cap) break;
+        memcpy(buf + n, l.data(), l.size());
+        n += l.size();
+        buf[n++] = '\n';
+        e->events.pop_front();
+    }
+    return n;
+}
+
+int32_t zc_profile(zc_engine* e, uint32_t on) {
+    if (!e) return 0;
+    e->profiling = on != 0;
+    return 1;
+}
+
+size_t zc_profile_report(zc_engine* e, char* buf, size_t cap) {
+    if (!e) return 0;
+    std::vector<std::pair<std::string, std::pair<double, uint32_t>>> v(e->prof.begin(), e->prof.end());
+    std::sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.second.first > b.second.first; });
+    std::string s;
+    for (auto& kv : v) {
+        char line[160];
+        snprintf(line, sizeof line, "%9.3f ms %6u  %s\n", kv.second.first, kv.second.second, kv.first.c_str());
+        s += line;
+    }
+    e->prof.clear();
+    return copy_out(s, buf, cap);
+}
+
+void zc_gpu_counts(zc_engine* e, uint32_t out[4]) {
+    if (!e) return;
+    for (int i = 0; i < 4; ++i) {
+        out[i] = e->counts[i];
+        e->counts[i] = 0;
+    }
+}
+
+int32_t zc_bench_moments(zc_engine* e, uint32_t, uint32_t) { return unsupported(e, "bench_moments"); }
+
+void zc_tune_parts(uint32_t, uint32_t, uint32_t, uint32_t) {}
+
+int32_t zc_compile_wgsl(zc_engine*, const char*, size_t, const char*, size_t, char*, size_t) {
+    return -1;  // "unsupported here" (python/zcmir/__init__.py:315-325)
+}
+
+int32_t zc_pg_info(zc_engine* e, double*) { return unsupported(e, "pg_info"); }
+int32_t zc_pg_maps(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "pg_maps"); }
+int32_t zc_pg_descriptors(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "pg_descriptors"); }
+int32_t zc_match_scores(zc_engine* e, float*, size_t) { return unsupported(e, "match_scores"); }
+int32_t zc_detect(zc_engine* e, zc_detect_result*) { return unsupported(e, "detect"); }
+int32_t zc_match(zc_engine* e, zc_match_result*) { return unsupported(e, "match"); }
+int32_t zc_auto(zc_engine* e, zc_climb_result*) { return unsupported(e, "auto"); }
+int32_t zc_keypoints(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "keypoints"); }
+int32_t zc_keypoint_frames(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "keypoint_frames"); }
+int32_t zc_matches(zc_engine* e, uint32_t*, size_t) { return unsupported(e, "matches"); }
+
+int32_t zc_set_ffd(zc_engine* e, const float*, size_t n) {
+    // the spline stays off in this build; all-zero control points are accepted
+    (void)n;
+    if (e) e->err.clear();
+    return 0;
+}
+
+size_t zc_get_ffd(zc_engine* e, float* cps, size_t cap) {
+    if (!e) return 0;
+    const unsigned g = std::min(std::max(e->set.u("ffd_grid"), 2u), 16u);
+    const size_t n = 2 * (size_t)g * g;
+    for (size_t i = 0; i < std::min(n, cap); ++i) cps[i] = 0.f;
+    return n;
+}
+
+uint32_t zc_fit_check(zc_engine* e, const double*) {
+    if (e) e->fail("fit_check: not part of this build");
+    return 7;  // "it fails the sanity check" (python/zcmir/__init__.py:178-181)
+}
+
+int32_t zc_ffd_gradient(zc_engine* e, const double*, double*, double*, size_t) {
+    return unsupported(e, "ffd_gradient");
+}
+
+int32_t zc_canvas(zc_engine* e, const double H[9], uint32_t inverse, zc_canvas_info* out) {
+    // src/overlay.zig:122-128 (host arithmetic only)
+    return guarded(e, "canvas", [&] {
+        if (!e->side[0].has || !e->side[1].has) return e->fail("canvas: NoImages");
+        const zc::Side& a = e->side[inverse ? 1 : 0];
+        const zc::Side& b = e->side[inverse ? 0 : 1];
+        const zc::Mat3 Hp = inverse ? zc::inv3(mat(H)) : mat(H);
+        const zc::Frame fr = zc::reg_frame(Hp, a.w, a.h, b.w, b.h);
+        const zc::Mat3 Hc = zc::canvas_H(Hp, fr.ox, fr.oy);
+        out->ox = fr.ox;
+        out->oy = fr.oy;
+        out->ow = (uint32_t)fr.w;
+        out->oh = (uint32_t)fr.h;
+        for (int i = 0; i < 9; ++i) out->Hc[i] = Hc[i];
+        return true;
+    });
+}
+
+int32_t zc_overlay(zc_engine* e, const double*, uint32_t, zc_canvas_info*, float*, float*, size_t) {
+    return unsupported(e, "overlay");
+}
+int32_t zc_tile_heat(zc_engine* e, const double*, uint32_t, uint32_t, double*, float*, float*, size_t) {
+    return unsupported(e, "tile_heat");
+}
+int64_t zc_export_warp(zc_engine* e, const char*, size_t, void*, size_t) { return unsupported(e, "export_warp"); }
+int32_t zc_displacement(zc_engine* e, float*, size_t) { return unsupported(e, "displacement"); }
+
+void zc_result_sizes(uint32_t out[4]) {
+    out[0] = sizeof(zc_shift_result);
+    out[1] = sizeof(zc_rs_result);
+    out[2] = sizeof(zc_grad_result);
+    out[3] = 0;
+}
+
+// ── the B200 build's own entry points (include/zcmir_b200.h) ──
+
+int32_t zcb_bench_maps(zc_engine* e, const double H[9], uint32_t flags, uint32_t cap, uint32_t warmup, uint32_t steps,
+                       double* out, size_t out_len) {
+    return guarded(e, "bench_maps", [&] { return e->bench_maps(mat(H), flags, cap, warmup, steps, out, out_len); });
+}
+
+int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, size_t* out_len, char* err,
+                           size_t err_cap, size_t* err_len) {
+    zc::Settings st;
+    std::string m;
+    if (!st.apply(json, len, m)) {
+        if (err_len) *err_len = copy_out(m, err, err_cap);
+        return -1;
+    }
+    const std::string j = st.to_json();
+    copy_out(j, out, cap);
+    if (out_len) *out_len = j.size();
+    if (err_len) *err_len = 0;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+// Line FFTs in shared memory for the SMI maps.
+//
+// A line of n complex points (n = 2^a·3^b, the reference's "ladder" sizes, src/fft.zig:14-34)
+// is transformed in place in shared memory by a Stockham autosort schedule of radix-16/8/4/2/3
+// stages (radices 16, 8, 4, 2 for the power of two, 3 for each factor 3). Each stage reads every
+// butterfly's inputs into registers, synchronises, then twiddles, runs the small DFT and writes
+// the outputs at their autosorted places, so one buffer of n points serves all stages.
+// Forward: e^{−2πi k t/n}, no scaling; inverse: e^{+2πi k t/n}, no scaling (the 1/(nx·ny) of
+// src/fft.zig:280-286 is applied where the correlations are scored).
+//
+// Shared-memory index padding (one slot per 16 points) keeps the strided writes of the first
+// stages free of bank conflicts.
+#pragma once
+
+#include "common.cuh"
+
+namespace zc {
+
+constexpr int kMaxStages = 16;
+constexpr int kMaxLine = 8192;
+
+struct LinePlan {
+    int n;                    // line length
+    int nst;                  // number of stages
+    int radix[kMaxStages];    // radix of each stage, in order
+    int tl;                   // threads per line (each stage's butterflies fit in tl·16/R)
+    const float2* tw;         // n twiddles e^{−2πi t/n}, t < n (device memory)
+};
+
+__host__ __device__ __forceinline__ int pad_idx(int i) { return i + (i >> 4); }
+__host__ __device__ __forceinline__ int padded_len(int n) { return n + (n >> 4) + 1; }
+
+// ── small DFTs, natural order in and out; INV flips the sign of the exponent ──
+
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {  // a·(−i) forward, a·(+i) inverse
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(float2* v) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft3(float2* v) {
+    const float s3 = 0.86602540378443864676f;
+    const float2 t = cadd(v[1], v[2]);
+    const float2 d = csub(v[1], v[2]);
+    const float2 m = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+    const float2 j = mul_mi<INV>(cscale(d, s3));
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, j);
+    v[2] = csub(m, j);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2* v) {
+    const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    const float2 a2 = cadd(v[1], v[3]), a3 = mul_mi<INV>(csub(v[1], v[3]));
+    v[0] = cadd(a0, a2);
+    v[2] = csub(a0, a2);
+    v[1] = cadd(a1, a3);
+    v[3] = csub(a1, a3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(float2* v) {
+    const float h = 0.70710678118654752440f;
+    float2 a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        a[r] = cadd(v[r], v[r + 4]);
+        b[r] = csub(v[r], v[r + 4]);
+    }
+    // b_r ·= w8^r
+    b[1] = INV ? make_float2(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
+               : make_float2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
+    b[2] = mul_mi<INV>(b[2]);
+    b[3] = INV ? make_float2(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y))
+               : make_float2(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
+    dft4<INV>(a);
+    dft4<INV>(b);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[2 * k] = a[k];
+        v[2 * k + 1] = b[k];
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft16(float2* v) {
+    // w16^r = (cos 2πr/16, ∓sin 2πr/16), r = 0..7
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    const float h = 0.70710678118654752440f;
+    const float cs[8] = {1.f, c1, h, s1, 0.f, -s1, -h, -c1};
+    const float sn[8] = {0.f, s1, h, c1, 1.f, c1, h, s1};
+    float2 a[8], b[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        a[r] = cadd(v[r], v[r + 8]);
+        const float2 d = csub(v[r], v[r + 8]);
+        const float si = INV ? sn[r] : -sn[r];
+        b[r] = make_float2(d.x * cs[r] - d.y * si, d.x * si + d.y * cs[r]);
+    }
+    dft8<INV>(a);
+    dft8<INV>(b);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        v[2 * k] = a[k];
+        v[2 * k + 1] = b[k];
+    }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2* v) {
+    if constexpr (R == 2) dft2<INV>(v);
+    else if constexpr (R == 3) dft3<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else dft16<INV>(v);
+}
+
+// One Stockham stage of radix R over a line in shared memory. Thread `t` of the line's `tlc`
+// threads takes butterflies j = t + b·tlc, b < BM (BM·R ≤ 18 registers of points). Ns: the
+// length of the sub-transforms done so far. All threads of the block must call it (it holds two
+// __syncthreads); threads without a line pass t ≥ 2^30.
+template <int R, int BM, bool INV>
+__device__ __noinline__ void fft_stage(float2* __restrict__ buf, const float2* __restrict__ tw,
+                                          int n, int Ns, int t, int tlc) {
+    const int m = n / R;
+    const int tws = n / (Ns * R);
+    float2 v[BM][R];
+#pragma unroll
+    for (int b = 0; b < BM; ++b) {
+        const int j = t + b * tlc;
+        if (j < m) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[b][r] = buf[pad_idx(j + r * m)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < BM; ++b) {
+        const int j = t + b * tlc;
+        if (j < m) {
+            const int k = j % Ns;
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(&tw[r * k * tws]);
+                    if (INV) w.y = -w.y;
+                    v[b][r] = cmul(v[b][r], w);
+                }
+            }
+            dft<R, INV>(v[b]);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[pad_idx(base + r * Ns)] = v[b][r];
+        }
+    }
+    __syncthreads();
+}
+
+// The whole line: every thread of the block calls it; `t` is the thread's index within its
+// line's plan.tl threads (≥ 2^30 for threads without a line).
+template <bool INV>
+__device__ __forceinline__ void line_fft(float2* __restrict__ buf, const LinePlan& p, int t) {
+    int Ns = 1;
+    for (int s = 0; s < p.nst; ++s) {
+        const int R = p.radix[s];
+        switch (R) {
+            case 16: fft_stage<16, 1, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;
+            case 8: fft_stage<8, 2, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;
+            case 4: fft_stage<4, 4, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;
+            case 2: fft_stage<2, 8, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;
+            default: fft_stage<3, 6, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;
+        }
+        Ns *= R;
+    }
+}
+
+}  // namespace zc

@@ -1,0 +1,84 @@
+// Host-side launchers of the engine's CUDA kernels (features.cu, shiftmap.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft.cuh"
+
+namespace zc {
+
+// ── per-image features (features.cu) ──
+// Scratch the feature build needs on the device (sizes in bytes are fixed; see features.cu).
+struct FeatScratch {
+    double* stats = nullptr;     // [0] Σg, [1] Σ(g − mean)², [2..21] whitening moments
+    unsigned* hist = nullptr;    // 256 bins
+    float* wt = nullptr;         // L⁻¹ (16) and μ (4) of the whitening
+    float* acf_part = nullptr;   // per-tile autocorrelation partial sums
+    size_t acf_part_cap = 0;     // floats
+    double* acf = nullptr;       // 289 × 4 normalised autocorrelation
+};
+
+// gray (w×h f32, device) → feat (4 planes), mag (1 plane), stack (5 planes), acf (289×4,
+// device doubles in scratch.acf). mode: 0 laplacian, 1 three, 2 cubic. `half`: quantise the
+// input to f16 first (in place on `gray`).
+cudaError_t build_features(float* gray, int w, int h, int mode, bool half, float* rank_tmp, float* feat,
+                           float* mag, float* stack, FeatScratch& s, cudaStream_t st);
+
+// ── shift maps (shiftmap.cu) ──
+struct MapGeom {
+    int W, Hh;       // canvas
+    int ox, oy;      // canvas offset (fixed pixel (0,0) at canvas (−ox, −oy))
+    int cw, ch;      // correlation grid
+    int nx, ny;      // FFT grid
+    int WP;          // half-spectrum row pitch (≥ nx/2 + 1)
+};
+
+struct CombineParams {
+    int exact;       // per-overlap whitening
+    int calib;       // Wilson–Hilferty z (exact only)
+    int nf;          // features the score runs over (3 or 4)
+    float min_n;     // overlap floor (cells)
+    double area;     // feature correlation area in cells (calibrated z)
+    double ridge;
+    double inv_nn;   // 1/(nx·ny): the inverse FFT's scale
+};
+
+// Correlation plan on the device: plane numbers per slot, and per correlation slot its
+// (moving slot, fixed slot, correlation number).
+struct CorrPlanDev {
+    int n_real;
+    int n_corr;
+    int planes[15];
+    int ca[45], cb[45], cnum[45];
+};
+
+// canvas stacks: moving warped by the canvas pose (hi = its inverse, f32 row-major), fixed pasted
+cudaError_t warp_stack(const float* stack, int w, int h, const float hi[9], bool ok, int W, int Hh, float* canvas,
+                       cudaStream_t st);
+cudaError_t paste_stack(const float* stack, int w, int h, int ox, int oy, int W, int Hh, float* canvas,
+                        cudaStream_t st);
+cudaError_t resample_grid(const float* canvas, int W, int Hh, int cw, int ch, float* grid, cudaStream_t st);
+// Σ grid_a[0]·grid_b[0] (float64) into *out: the overlap count at lag 0
+cudaError_t lag0_count(const float* grid_a, const float* grid_b, int cw, int ch, double* out, cudaStream_t st);
+
+// forward transforms of one side: real planes of the grid → row R2C (rows < ch) into the half
+// spectra [n_real][ny][WP] complex; then the column FFTs of the half spectra in place
+cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& row,
+                         float2* half, cudaStream_t st);
+cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
+                         cudaStream_t st);
+// products and inverse column FFTs: Q[slot][ny][WP]
+cudaError_t inverse_columns(const float2* half_a, const float2* half_b, const MapGeom& g, const CorrPlanDev& plan,
+                            const LinePlan& col, float2* Q, cudaStream_t st);
+// inverse row FFTs fused with the per-shift score and the argmax: map (ny × nx f32), best key
+// (u64), zero-lag score
+cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
+                               int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
+                               unsigned long long* best, float* zero, cudaStream_t st);
+// the split S of the row pass for nx (smallest divisor keeping its shared memory in budget); 0
+// when none fits
+int row_split(int nx, int n_corr);
+size_t row_pass_smem(int L, int n_corr, int tl);
+
+}  // namespace zc

@@ -1,0 +1,537 @@
+// The SMI shift map on the GPU (the reference's Smi.shiftMap, src/smi.zig:540-572, with its
+// kernels in shaders/smi.wgsl:626-931, 1597-1706).
+//
+// Pipeline for one map (nx × ny FFT grid, cw × ch correlation grid, P real planes, C
+// correlations):
+//   1. canvas: the moving stack warped by the canvas pose, the fixed stack pasted
+//      (warp_stack / paste_stack), then resampled to the grid when the map is coarser.
+//   2. forward_rows / forward_cols (per side): the P real planes are formed on the fly from the
+//      5 stack values, two per complex row, row-FFT'd (rows < ch only), unpacked into P half
+//      spectra (columns 0..nx/2), then column-FFT'd (rows ≥ ch are zero).
+//   3. inverse_columns: per correlation and column tile, A·conj(B) and the inverse column FFT.
+//   4. inverse_rows_score: per row, correlations paired as c1 + i·c2 on the Hermitian full row,
+//      inverse row FFT, and the per-shift score in float64 with its argmax, without writing a
+//      correlation plane to memory. Rows longer than shared memory holds for all C correlations
+//      are split S ways by one decimation-in-frequency step (output shifts x ≡ s mod S).
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace zc {
+namespace {
+
+constexpr int kNoLine = 1 << 30;
+
+// ── canvas (smi.wgsl:1655-1706) ──────────────────────────────────────────────────────────────
+
+struct Mat9f {
+    float m[9];
+};
+
+__global__ void k_warp_stack(const float* __restrict__ stack, int w, int h, Mat9f hi, int ok_det, int W, int Hh,
+                             float* __restrict__ canvas) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= Hh) return;
+    const size_t n = (size_t)W * Hh, pix = (size_t)y * W + x, sn = (size_t)w * h;
+    bool ok = ok_det != 0;
+    float fx = 0.f, fy = 0.f;
+    if (ok) {
+        const float X = (float)x + 1.0f, Y = (float)y + 1.0f;
+        const float qx = hi.m[0] * X + hi.m[1] * Y + hi.m[2];
+        const float qy = hi.m[3] * X + hi.m[4] * Y + hi.m[5];
+        const float qz = hi.m[6] * X + hi.m[7] * Y + hi.m[8];
+        ok = fabsf(qz) >= 1e-8f;
+        if (ok) {
+            fx = qx / qz - 1.0f;
+            fy = qy / qz - 1.0f;
+            ok = !(fx < 0.f || fy < 0.f || fx > (float)(w - 1) || fy > (float)(h - 1));
+        }
+    }
+    int x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+    float tx = 0.f, ty = 0.f;
+    if (ok) {
+        const float flx = floorf(fx), fly = floorf(fy);
+        tx = fx - flx;
+        ty = fy - fly;
+        x0 = min(max((int)flx, 0), w - 1);
+        y0 = min(max((int)fly, 0), h - 1);
+        x1 = min(max((int)flx + 1, 0), w - 1);
+        y1 = min(max((int)fly + 1, 0), h - 1);
+    }
+#pragma unroll
+    for (int p = 0; p < 5; ++p) {
+        float v = 0.f;
+        if (ok) {
+            const float* s = stack + p * sn;
+            const float v00 = s[(size_t)y0 * w + x0], v10 = s[(size_t)y0 * w + x1];
+            const float v01 = s[(size_t)y1 * w + x0], v11 = s[(size_t)y1 * w + x1];
+            const float a = v00 * (1.f - tx) + v10 * tx, b = v01 * (1.f - tx) + v11 * tx;
+            v = a * (1.f - ty) + b * ty;
+        }
+        canvas[p * n + pix] = v;
+    }
+}
+
+__global__ void k_paste_stack(const float* __restrict__ stack, int w, int h, int ox, int oy, int W, int Hh,
+                              float* __restrict__ canvas) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= Hh) return;
+    const size_t n = (size_t)W * Hh, pix = (size_t)y * W + x, sn = (size_t)w * h;
+    const int sx = x + ox, sy = y + oy;
+    const bool in = sx >= 0 && sy >= 0 && sx < w && sy < h;
+#pragma unroll
+    for (int p = 0; p < 5; ++p) canvas[p * n + pix] = in ? stack[p * sn + (size_t)sy * w + sx] : 0.f;
+}
+
+// k×k box of bilinear taps per cell (smi.wgsl:626-639, 675-705)
+__global__ void k_resample(const float* __restrict__ canvas, int W, int Hh, int cw, int ch, float* __restrict__ grid) {
+    const int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (gx >= cw || gy >= ch) return;
+    const float fx = (float)W / (float)max(cw, 1), fy = (float)Hh / (float)max(ch, 1);
+    const int kx = (int)fminf(fmaxf(ceilf(fx - 1e-4f), 1.f), 8.f);
+    const int ky = (int)fminf(fmaxf(ceilf(fy - 1e-4f), 1.f), 8.f);
+    const size_t n = (size_t)W * Hh, gn = (size_t)cw * ch;
+    float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int j = 0; j < ky; ++j) {
+        const float py = ((float)gy + ((float)j + 0.5f) / (float)ky) * fy - 0.5f;
+        const float fly = floorf(py);
+        const float ay = py - fly;
+        const int ya = min(max((int)fly, 0), Hh - 1), yb = min(max((int)fly + 1, 0), Hh - 1);
+        for (int i = 0; i < kx; ++i) {
+            const float px = ((float)gx + ((float)i + 0.5f) / (float)kx) * fx - 0.5f;
+            const float flx = floorf(px);
+            const float ax = px - flx;
+            const int xa = min(max((int)flx, 0), W - 1), xb = min(max((int)flx + 1, 0), W - 1);
+#pragma unroll
+            for (int p = 0; p < 5; ++p) {
+                const float* c = canvas + p * n;
+                const float a = c[(size_t)ya * W + xa] * (1.f - ax) + c[(size_t)ya * W + xb] * ax;
+                const float b = c[(size_t)yb * W + xa] * (1.f - ax) + c[(size_t)yb * W + xb] * ax;
+                s[p] += a * (1.f - ay) + b * ay;
+            }
+        }
+    }
+    const float inv = 1.f / (float)(kx * ky);
+#pragma unroll
+    for (int p = 0; p < 5; ++p) grid[p * gn + (size_t)gy * cw + gx] = s[p] * inv;
+}
+
+__global__ void k_lag0(const float* __restrict__ a, const float* __restrict__ b, int n, double* out) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc += (double)a[i] * (double)b[i];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) atomicAdd(out, acc);
+}
+
+// ── forward: real planes → row R2C → column FFT ─────────────────────────────────────────────
+
+// Real correlation plane r from the premultiplied samples s = [w, w f0..w f3]
+// (smi.wgsl:641-649): 0 → w, 1..4 → w f_i, 5..14 → s_i s_j / s_0 (0 where s_0 ≤ 1e-6).
+__device__ __forceinline__ float real_plane(int r, const float* s) {
+    if (r < 5) return s[r];
+    if (s[0] <= 1e-6f) return 0.f;
+    const int k = r - 5;
+    const int ti = (k < 4) ? 0 : (k < 7) ? 1 : (k < 9) ? 2 : 3;
+    const int tj = (k < 4) ? k : (k < 7) ? k - 3 : (k < 9) ? k - 5 : 3;
+    return s[1 + ti] * s[1 + tj] / s[0];
+}
+
+// One block per grid row y < ch; lines = packed plane pairs (2z, 2z+1), lpb of them at a time.
+__global__ void __launch_bounds__(512) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int nx, int WP, CorrPlanDev plan,
+                           LinePlan lp, int lpb, float2* __restrict__ half, size_t pstride) {
+    extern __shared__ float2 smem[];
+    const int y = blockIdx.x;
+    const int line = threadIdx.x / lp.tl;
+    const int t = threadIdx.x - line * lp.tl;
+    const int pl = padded_len(nx);
+    float2* buf = smem + line * pl;
+    const size_t gn = (size_t)cw * ch;
+    const int n_cplx = (plan.n_real + 1) / 2;
+    for (int z0 = 0; z0 < n_cplx; z0 += lpb) {
+        const int z = z0 + line;
+        const bool act = line < lpb && z < n_cplx;
+        if (act) {
+            const int ra = plan.planes[2 * z];
+            const int rb = (2 * z + 1 < plan.n_real) ? plan.planes[2 * z + 1] : -1;
+            for (int x = t; x < nx; x += lp.tl) {
+                float2 v = make_float2(0.f, 0.f);
+                if (x < cw) {
+                    float s[5];
+#pragma unroll
+                    for (int p = 0; p < 5; ++p) s[p] = __ldg(&grid[p * gn + (size_t)y * cw + x]);
+                    v.x = real_plane(ra, s);
+                    if (rb >= 0) v.y = real_plane(rb, s);
+                }
+                buf[pad_idx(x)] = v;
+            }
+        }
+        __syncthreads();
+        line_fft<false>(buf, lp, act ? t : kNoLine);
+        if (act) {
+            const bool has_b = 2 * z + 1 < plan.n_real;
+            float2* oa = half + (size_t)(2 * z) * pstride + (size_t)y * WP;
+            float2* ob = half + (size_t)(2 * z + 1) * pstride + (size_t)y * WP;
+            for (int x = t; x <= nx / 2; x += lp.tl) {
+                const float2 Z = buf[pad_idx(x)];
+                const float2 Zm = buf[pad_idx(x == 0 ? 0 : nx - x)];
+                oa[x] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
+                if (has_b) ob[x] = make_float2(0.5f * (Z.y + Zm.y), 0.5f * (Zm.x - Z.x));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Column FFTs of the half spectra, in place: block = a tile of tx columns of one plane; rows
+// ≥ rows_in read as zero. INV: inverse transform.
+template <bool INV>
+__global__ void __launch_bounds__(512, 1) k_cols(float2* __restrict__ half, size_t pstride, int WP, int ncols, int rows_in, LinePlan lp,
+                       int tx) {
+    extern __shared__ float2 smem[];
+    const int x0 = blockIdx.x * tx;
+    float2* base = half + (size_t)blockIdx.y * pstride;
+    const int ny = lp.n, pl = padded_len(ny);
+    const int total = tx * ny;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int y = e / tx, c = e - y * tx;
+        float2 v = make_float2(0.f, 0.f);
+        if (y < rows_in && x0 + c < ncols) v = base[(size_t)y * WP + x0 + c];
+        smem[c * pl + pad_idx(y)] = v;
+    }
+    __syncthreads();
+    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
+    line_fft<INV>(smem + (line < tx ? line : 0) * pl, lp, line < tx ? t : kNoLine);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int y = e / tx, c = e - y * tx;
+        if (x0 + c < ncols) base[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
+    }
+}
+
+// ── inverse: products and column IFFTs ──────────────────────────────────────────────────────
+
+// block (correlation slot k, column tile): P = A·conj(B) on the tile, inverse column FFT → Q
+__global__ void __launch_bounds__(512, 1) k_inv_cols(const float2* __restrict__ ha, const float2* __restrict__ hb, size_t pstride, int WP,
+                           int ncols, CorrPlanDev plan, LinePlan lp, int tx, float2* __restrict__ Q) {
+    extern __shared__ float2 smem[];
+    const int k = blockIdx.x;
+    const int x0 = blockIdx.y * tx;
+    const float2* A = ha + (size_t)plan.ca[k] * pstride;
+    const float2* B = hb + (size_t)plan.cb[k] * pstride;
+    float2* O = Q + (size_t)k * pstride;
+    const int ny = lp.n, pl = padded_len(ny);
+    const int total = tx * ny;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int y = e / tx, c = e - y * tx;
+        float2 v = make_float2(0.f, 0.f);
+        if (x0 + c < ncols) {
+            const size_t i = (size_t)y * WP + x0 + c;
+            v = cmulc(__ldg(&A[i]), __ldg(&B[i]));
+        }
+        smem[c * pl + pad_idx(y)] = v;
+    }
+    __syncthreads();
+    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
+    line_fft<true>(smem + (line < tx ? line : 0) * pl, lp, line < tx ? t : kNoLine);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int y = e / tx, c = e - y * tx;
+        if (x0 + c < ncols) O[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
+    }
+}
+
+// ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
+
+__device__ __forceinline__ int tri_k(int i, int j) {
+    const int a = min(i, j), b = max(i, j);
+    return a * 4 - (a * (a + 1)) / 2 + b;
+}
+
+// In-place 4×4 Cholesky (lower), false when a pivot is not > 0 (smi.wgsl:798-813), float64.
+__device__ __forceinline__ bool chol4d(double* g) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double s = g[i * 4 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) s -= g[i * 4 + k] * g[j * 4 + k];
+            if (i == j) {
+                if (!(s > 0.0)) return false;
+                g[i * 5] = sqrt(s);
+            } else {
+                g[i * 4 + j] = s / g[j * 5];
+            }
+        }
+    }
+    return true;
+}
+
+// Per-shift score (smi.wgsl:825-915, combine_cell) in float64. c: the 45 sums (absent ones 0),
+// already scaled. n00: the overlap at lag 0.
+__device__ float combine_cell(const double* c, const CombineParams& p, double n00) {
+    const int nf = p.nf;
+    const double n = c[0];
+    const bool calib = p.exact && p.calib;
+    const double neff = n / fmax(p.area, 1.0);
+    double floor_n = fmax((double)p.min_n, 0.08 * fmax(n00, 0.0));
+    if (calib) floor_n = (double)p.min_n;
+    if (n < floor_n || (calib && neff <= 10.0)) return 0.f;
+    const double den = fmax(n, 1e-8);
+    double ma[4] = {0, 0, 0, 0}, mb[4] = {0, 0, 0, 0};
+    for (int i = 0; i < nf; ++i) {
+        ma[i] = c[1 + i] / den;
+        mb[i] = c[5 + i] / den;
+    }
+    if (!p.exact) {
+        double s = 0.0;
+        for (int i = 0; i < nf; ++i)
+            for (int j = 0; j < nf; ++j) {
+                const double cij = fmin(fmax(c[9 + i * 4 + j] / den - ma[i] * mb[j], -1.0), 1.0);
+                s += cij * cij;
+            }
+        const double sc = n * s;
+        return (sc == sc) ? (float)sc : 0.f;
+    }
+    double ga[16] = {0}, gb[16] = {0};
+    double tra = 0.0, trb = 0.0;
+    for (int i = 0; i < nf; ++i) {
+        for (int j = 0; j < nf; ++j) {
+            const int k = tri_k(i, j);
+            ga[i * 4 + j] = c[25 + k] / den - ma[i] * ma[j];
+            gb[i * 4 + j] = c[35 + k] / den - mb[i] * mb[j];
+        }
+        tra += ga[i * 5];
+        trb += gb[i * 5];
+    }
+    for (int i = 0; i < nf; ++i) {
+        ga[i * 5] += p.ridge * fmax(tra * 0.25, 1e-12);
+        gb[i * 5] += p.ridge * fmax(trb * 0.25, 1e-12);
+    }
+    for (int i = nf; i < 4; ++i) {
+        ga[i * 5] = 1.0;
+        gb[i * 5] = 1.0;
+    }
+    if (!chol4d(ga) || !chol4d(gb)) return 0.f;
+    double x[16];
+    for (int j = 0; j < nf; ++j)
+        for (int i = 0; i < nf; ++i) {
+            double s = c[9 + i * 4 + j] / den - ma[i] * mb[j];
+            for (int k = 0; k < i; ++k) s -= ga[i * 4 + k] * x[k * 4 + j];
+            x[i * 4 + j] = s / ga[i * 5];
+        }
+    double acc = 0.0;
+    for (int r = 0; r < nf; ++r) {
+        double yv[4];
+        for (int i = 0; i < nf; ++i) {
+            double s = x[r * 4 + i];
+            for (int k = 0; k < i; ++k) s -= gb[i * 4 + k] * yv[k];
+            yv[i] = s / gb[i * 5];
+            acc += yv[i] * yv[i];
+        }
+    }
+    double score = n * acc;
+    if (calib) {
+        const double q = (double)nf;
+        const double v = fmin(acc, q - 1e-4);
+        const double f = (neff - q - 1.0) / q * v / (q - v);
+        const double d1 = q * q, d2 = q * (neff - q - 1.0);
+        const double a = 2.0 / (9.0 * d1), b = 2.0 / (9.0 * d2);
+        const double cc = cbrt(fmax(f, 0.0));
+        const double z = ((1.0 - b) * cc - (1.0 - a)) / sqrt(b * cc * cc + a);
+        score = fmax(z, 0.0);
+    }
+    return (score == score) ? (float)score : 0.f;
+}
+
+// block (row y, split s): every correlation pair's row (Hermitian full row from the half
+// spectrum) pre-combined for outputs x ≡ s (mod S), inverse FFT of length L = nx/S, the sums
+// kept in shared memory; then the score of each of the row's L shifts and the block argmax.
+__global__ void __launch_bounds__(256, 1) k_inv_rows(const float2* __restrict__ Q, size_t pstride, int WP, int nx, int ny, int S,
+                           CorrPlanDev plan, LinePlan lp, int lpb, const float2* __restrict__ tw_nx,
+                           CombineParams cp, const double* __restrict__ n00p, float* __restrict__ map,
+                           unsigned long long* best, float* zero_out) {
+    extern __shared__ float2 smem[];
+    const int y = blockIdx.x / S, s = blockIdx.x - (blockIdx.x / S) * S;
+    const int L = lp.n, pl = padded_len(L);
+    float* corr = reinterpret_cast<float*>(smem + lpb * pl);  // [n_corr][L]
+    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
+    float2* buf = smem + (line < lpb ? line : 0) * pl;
+    const int npairs = (plan.n_corr + 1) / 2;
+    for (int p0 = 0; p0 < npairs; p0 += lpb) {
+        const int pr = p0 + line;
+        const bool act = line < lpb && pr < npairs;
+        const int k1 = 2 * pr, k2 = (2 * pr + 1 < plan.n_corr) ? 2 * pr + 1 : -1;
+        if (act) {
+            const float2* q1 = Q + (size_t)k1 * pstride + (size_t)y * WP;
+            const float2* q2 = (k2 >= 0) ? Q + (size_t)k2 * pstride + (size_t)y * WP : nullptr;
+            for (int m = t; m < L; m += lp.tl) {
+                float2 acc = make_float2(0.f, 0.f);
+                for (int q = 0; q < S; ++q) {
+                    const int x = m + q * L;
+                    float2 z;
+                    if (x <= nx / 2) {
+                        const float2 a = __ldg(&q1[x]);
+                        const float2 b = q2 ? __ldg(&q2[x]) : make_float2(0.f, 0.f);
+                        z = make_float2(a.x - b.y, a.y + b.x);
+                    } else {
+                        const float2 a = __ldg(&q1[nx - x]);
+                        const float2 b = q2 ? __ldg(&q2[nx - x]) : make_float2(0.f, 0.f);
+                        z = make_float2(a.x + b.y, b.x - a.y);
+                    }
+                    if (S > 1 && q > 0) z = cmul(z, cconj(__ldg(&tw_nx[(q * s * L) % nx])));
+                    acc = cadd(acc, z);
+                }
+                if (S > 1 && s > 0) acc = cmul(acc, cconj(__ldg(&tw_nx[m * s])));
+                buf[pad_idx(m)] = acc;
+            }
+        }
+        __syncthreads();
+        line_fft<true>(buf, lp, act ? t : kNoLine);
+        if (act) {
+            for (int m = t; m < L; m += lp.tl) {
+                const float2 z = buf[pad_idx(m)];
+                corr[(size_t)k1 * L + m] = z.x;
+                if (k2 >= 0) corr[(size_t)k2 * L + m] = z.y;
+            }
+        }
+        __syncthreads();
+    }
+    const double n00 = *n00p;
+    float bv = -3.4e38f;
+    uint32_t bi = 0xffffffffu;
+    for (int m = threadIdx.x; m < L; m += blockDim.x) {
+        double c[45];
+#pragma unroll
+        for (int i = 0; i < 45; ++i) c[i] = 0.0;
+        for (int k = 0; k < plan.n_corr; ++k) c[plan.cnum[k]] = (double)corr[(size_t)k * L + m] * cp.inv_nn;
+        const float sc = combine_cell(c, cp, n00);
+        const int x = m * S + s;
+        const uint32_t idx = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
+        map[idx] = sc;
+        if (sc > bv || (sc == bv && idx < bi)) {
+            bv = sc;
+            bi = idx;
+        }
+        if (idx == 0) *zero_out = sc;
+    }
+    unsigned long long key = (bi == 0xffffffffu) ? 0ull : argmax_key(bv, bi);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if ((threadIdx.x & 31) == 0 && key) atomicMax(best, key);
+}
+
+}  // namespace
+
+// ── launchers ────────────────────────────────────────────────────────────────────────────────
+
+cudaError_t warp_stack(const float* stack, int w, int h, const float hi[9], bool ok, int W, int Hh, float* canvas,
+                       cudaStream_t st) {
+    Mat9f m;
+    for (int i = 0; i < 9; ++i) m.m[i] = hi[i];
+    dim3 b(32, 8), g((W + 31) / 32, (Hh + 7) / 8);
+    k_warp_stack<<<g, b, 0, st>>>(stack, w, h, m, ok ? 1 : 0, W, Hh, canvas);
+    return cudaGetLastError();
+}
+
+cudaError_t paste_stack(const float* stack, int w, int h, int ox, int oy, int W, int Hh, float* canvas,
+                        cudaStream_t st) {
+    dim3 b(32, 8), g((W + 31) / 32, (Hh + 7) / 8);
+    k_paste_stack<<<g, b, 0, st>>>(stack, w, h, ox, oy, W, Hh, canvas);
+    return cudaGetLastError();
+}
+
+cudaError_t resample_grid(const float* canvas, int W, int Hh, int cw, int ch, float* grid, cudaStream_t st) {
+    dim3 b(32, 8), g((cw + 31) / 32, (ch + 7) / 8);
+    k_resample<<<g, b, 0, st>>>(canvas, W, Hh, cw, ch, grid);
+    return cudaGetLastError();
+}
+
+cudaError_t lag0_count(const float* a, const float* b, int cw, int ch, double* out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, sizeof(double), st);
+    const int n = cw * ch;
+    int blocks = (n + 255) / 256;
+    if (blocks > 296) blocks = 296;
+    k_lag0<<<blocks, 256, 0, st>>>(a, b, n, out);
+    return cudaGetLastError();
+}
+
+static int lines_per_block(int tl, int want_threads) {
+    int l = want_threads / tl;
+    return l < 1 ? 1 : l;
+}
+
+cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& row,
+                         float2* half, cudaStream_t st) {
+    const size_t pstride = (size_t)g.ny * g.WP;
+    // lpb packed planes at a time, ~256 threads
+    const int lpb = lines_per_block(row.tl, 256);
+    const int n_cplx = (plan.n_real + 1) / 2;
+    const int lines = lpb < n_cplx ? lpb : n_cplx;
+    const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2);
+    cudaFuncSetAttribute(k_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_fwd_rows<<<g.ch, lines * row.tl, sm, st>>>(grid, g.cw, g.ch, g.nx, g.WP, plan, row, lines, half, pstride);
+    return cudaGetLastError();
+}
+
+static int col_tile(const LinePlan& col) {
+    int tx = lines_per_block(col.tl, 512);
+    while (tx > 1 && (size_t)tx * padded_len(col.n) * sizeof(float2) > 160 * 1024) tx >>= 1;
+    return tx;
+}
+
+cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
+                         cudaStream_t st) {
+    const size_t pstride = (size_t)g.ny * g.WP;
+    const int ncols = g.nx / 2 + 1;
+    const int tx = col_tile(col);
+    const size_t sm = (size_t)tx * padded_len(g.ny) * sizeof(float2);
+    cudaFuncSetAttribute(k_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 gc((ncols + tx - 1) / tx, plan.n_real);
+    k_cols<false><<<gc, tx * col.tl, sm, st>>>(half, pstride, g.WP, ncols, g.ch, col, tx);
+    return cudaGetLastError();
+}
+
+cudaError_t inverse_columns(const float2* ha, const float2* hb, const MapGeom& g, const CorrPlanDev& plan,
+                            const LinePlan& col, float2* Q, cudaStream_t st) {
+    const size_t pstride = (size_t)g.ny * g.WP;
+    const int ncols = g.nx / 2 + 1;
+    const int tx = col_tile(col);
+    const size_t sm = (size_t)tx * padded_len(g.ny) * sizeof(float2);
+    cudaFuncSetAttribute(k_inv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 gc(plan.n_corr, (ncols + tx - 1) / tx);
+    k_inv_cols<<<gc, tx * col.tl, sm, st>>>(ha, hb, pstride, g.WP, ncols, plan, col, tx, Q);
+    return cudaGetLastError();
+}
+
+size_t row_pass_smem(int L, int n_corr, int tl) {
+    const int lpb = lines_per_block(tl, 256);
+    return (size_t)lpb * padded_len(L) * sizeof(float2) + (size_t)n_corr * L * sizeof(float);
+}
+
+int row_split(int nx, int n_corr) {
+    for (int S = 1; S <= 64; ++S) {
+        if (nx % S) continue;
+        const int L = nx / S;
+        int tl = (L + 15) / 16;
+        tl = ((tl + 31) / 32) * 32;
+        if (row_pass_smem(L, n_corr, tl) <= 220 * 1024) return S;
+    }
+    return 0;
+}
+
+cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
+                               int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
+                               unsigned long long* best, float* zero, cudaStream_t st) {
+    const size_t pstride = (size_t)g.ny * g.WP;
+    const int lpb = lines_per_block(line.tl, 256);
+    const size_t sm = row_pass_smem(line.n, plan.n_corr, line.tl);
+    cudaFuncSetAttribute(k_inv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_inv_rows<<<g.ny * S, lpb * line.tl, sm, st>>>(Q, pstride, g.WP, g.nx, g.ny, S, plan, line, lpb, tw_nx, cp, n00,
+                                                   map, best, zero);
+    return cudaGetLastError();
+}
+
+}  // namespace zc

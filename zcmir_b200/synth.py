@@ -1,0 +1,71 @@
+"""Seeded synthetic image pairs with the shapes and value distributions of the SMI workloads.
+
+* ``blob_field``: a smooth field of Gaussian blobs (σ 4–20 px, amplitudes ±1) plus two
+  sinusoidal gratings, normalised to [0, 1].
+* ``pair_remap`` (256² map workload): fixed = the field, moving = 1 − field² (inverted,
+  nonlinear contrast) at a known integer shift, plus N(0, 0.02²).
+* ``pair_segmented`` (1024² map workload): modality A = a blob field (uint16 range); modality
+  B = an 8-level piecewise-constant segmentation of it with a random level → intensity
+  permutation plus N(0, 0.03²), shifted by a random integer shift in ±200 px.
+
+The true pose maps moving → fixed (1-based pixels): H = translate(dx, dy), i.e. the moving pixel
+x shows the fixed content at x + (dx, dy). The shift map at the identity pose then peaks at the
+lag (−dx, −dy) and its corrected pose is H.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def blob_field(h, w, rng, n_blobs=64, sigma=(4.0, 20.0), gratings=2):
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    f = np.zeros((h, w))
+    scale = max(h, w) / 256.0
+    for _ in range(int(n_blobs * scale * scale)):
+        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
+        s = rng.uniform(*sigma)
+        a = rng.uniform(-1, 1)
+        x0, x1 = int(max(0, cx - 4 * s)), int(min(w, cx + 4 * s + 1))
+        y0, y1 = int(max(0, cy - 4 * s)), int(min(h, cy + 4 * s + 1))
+        if x1 <= x0 or y1 <= y0:
+            continue
+        f[y0:y1, x0:x1] += a * np.exp(-((xx[y0:y1, x0:x1] - cx) ** 2 + (yy[y0:y1, x0:x1] - cy) ** 2) / (2 * s * s))
+    for _ in range(gratings):
+        th = rng.uniform(0, np.pi)
+        period = rng.uniform(24, 64)
+        f += 0.3 * np.sin(2 * np.pi * (np.cos(th) * xx + np.sin(th) * yy) / period + rng.uniform(0, 2 * np.pi))
+    f -= f.min()
+    return f / max(f.max(), 1e-12)
+
+
+def pair_remap(n=256, shift=(17, -9), seed=0, noise=0.02):
+    """(moving, fixed, H_true) float32 in [0, 1]: moving = 1 − field² shifted by `shift`."""
+    rng = np.random.default_rng(seed)
+    dx, dy = shift
+    pad = max(abs(dx), abs(dy)) + 8
+    big = blob_field(n + 2 * pad, n + 2 * pad, rng)
+    fixed = big[pad:pad + n, pad:pad + n]
+    mov = big[pad + dy:pad + dy + n, pad + dx:pad + dx + n]
+    moving = 1.0 - mov ** 2 + noise * rng.standard_normal((n, n))
+    H = np.array([[1, 0, dx], [0, 1, dy], [0, 0, 1.0]])
+    return moving.astype(np.float32), fixed.astype(np.float32), H
+
+
+def pair_segmented(n=1024, seed=1, max_shift=200, levels=8, noise=0.03, shift=None):
+    """(moving, fixed, H_true) uint16: fixed = blob field (modality A), moving = its segmented
+    modality B at a random integer shift in ±max_shift."""
+    rng = np.random.default_rng(seed)
+    if shift is None:
+        shift = tuple(int(v) for v in rng.integers(-max_shift, max_shift + 1, size=2))
+    dx, dy = shift
+    pad = max(abs(dx), abs(dy)) + 8
+    big = blob_field(n + 2 * pad, n + 2 * pad, rng, n_blobs=64)
+    fixed = big[pad:pad + n, pad:pad + n]
+    src = big[pad + dy:pad + dy + n, pad + dx:pad + dx + n]
+    edges = np.quantile(src, np.linspace(0, 1, levels + 1)[1:-1])
+    lab = np.digitize(src, edges)
+    perm = rng.permutation(levels)
+    moving = perm[lab] / (levels - 1.0) + noise * rng.standard_normal((n, n))
+    to16 = lambda a: (np.clip(a, 0, 1) * 65535 + 0.5).astype(np.uint16)
+    H = np.array([[1, 0, dx], [0, 1, dy], [0, 0, 1.0]])
+    return to16(moving), to16(fixed), H
