@@ -29,6 +29,12 @@ struct LinePlan {
 
 __host__ __device__ __forceinline__ int pad_idx(int i) { return i + (i >> 4); }
 __host__ __device__ __forceinline__ int padded_len(int n) { return n + (n >> 4) + 1; }
+// pitch between lines stored side by side (column tiles): ≡ 4 (mod 16) points, so a half-warp
+// touching 4 lines × 4 consecutive points hits 16 distinct bank pairs
+__host__ __device__ __forceinline__ int line_pitch(int n) {
+    const int p = padded_len(n);
+    return p + ((4 - (p & 15)) & 15);
+}
 
 // ── small DFTs, natural order in and out; INV flips the sign of the exponent ──
 
@@ -181,5 +187,91 @@ __device__ __forceinline__ void line_fft(float2* __restrict__ buf, const LinePla
         Ns *= R;
     }
 }
+
+// ── power-of-two lines with the whole schedule known at compile time ──
+// N = 2^a points, N/16 threads per line (one radix-16 butterfly, or 16/R of radix R, per thread
+// per stage), ⌈a/4⌉ stages with balanced radices; strides, twiddle steps and index arithmetic
+// fold to constants.
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+template <int N>
+struct Pow2 {
+    static constexpr int kLog = ilog2(N);
+    static constexpr int kStages = (kLog + 3) / 4;
+    static constexpr int kThreads = N / 16;
+    static constexpr int bits(int s) { return kLog / kStages + (s < kLog % kStages ? 1 : 0); }
+};
+
+template <int R, int NS, int N, int TL, bool INV>
+__device__ __forceinline__ void p2_stage(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
+    constexpr int M = N / R, BM = (M + TL - 1) / TL, TWS = N / (NS * R);
+    float2 v[BM][R];
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BM; ++b) {
+            const int j = t + b * TL;
+            if (M % TL == 0 || j < M) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[b][r] = buf[pad_idx(j + r * M)];
+            }
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BM; ++b) {
+            const int j = t + b * TL;
+            if (M % TL == 0 || j < M) {
+                const int k = j & (NS - 1);
+                if (NS > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        float2 w = __ldg(&tw[r * k * TWS]);
+                        if (INV) w.y = -w.y;
+                        v[b][r] = cmul(v[b][r], w);
+                    }
+                }
+                dft<R, INV>(v[b]);
+                const int base = (j - k) * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) buf[pad_idx(base + r * NS)] = v[b][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, int TL, bool INV, int S = 0, int NS = 1>
+__device__ __forceinline__ void p2_fft(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
+    if constexpr (S < Pow2<N>::kStages) {
+        constexpr int R = 1 << Pow2<N>::bits(S);
+        p2_stage<R, NS, N, TL, INV>(buf, tw, t, act);
+        p2_fft<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
+    }
+}
+
+// Line-FFT policies the map kernels are written against: n(), threads per line, run<INV>().
+struct GenericLine {
+    LinePlan p;
+    __device__ __forceinline__ int n() const { return p.n; }
+    __device__ __forceinline__ int tl() const { return p.tl; }
+    template <bool INV>
+    __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
+        line_fft<INV>(buf, p, act ? t : (1 << 30));
+    }
+};
+
+// TPL: threads per line (N/16 by default: one radix-16 butterfly each; N/8 gives every thread
+// 8 points of the loads and stores around the transform, half of them idle in radix-16 stages)
+template <int N, int TPL = N / 16>
+struct Pow2Line {
+    const float2* tw;
+    __device__ __forceinline__ static constexpr int n() { return N; }
+    __device__ __forceinline__ static constexpr int tl() { return TPL; }
+    template <bool INV>
+    __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
+        p2_fft<N, TPL, INV>(buf, tw, t, act && t < TPL);
+    }
+};
 
 }  // namespace zc

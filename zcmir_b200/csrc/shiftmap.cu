@@ -137,42 +137,62 @@ __device__ __forceinline__ float real_plane(int r, const float* s) {
     return s[1 + ti] * s[1 + tj] / s[0];
 }
 
+// real_plane on a staged row [5][cw] (indexing shared memory, not a register array)
+__device__ __forceinline__ float real_plane_row(int r, const float* row, int cw, int x) {
+    if (r < 5) return row[r * cw + x];
+    const float s0 = row[x];
+    if (s0 <= 1e-6f) return 0.f;
+    const int k = r - 5;
+    const int ti = (k < 4) ? 0 : (k < 7) ? 1 : (k < 9) ? 2 : 3;
+    const int tj = (k < 4) ? k : (k < 7) ? k - 3 : (k < 9) ? k - 5 : 3;
+    return row[(1 + ti) * cw + x] * row[(1 + tj) * cw + x] / s0;
+}
+
 // One block per grid row y < ch; lines = packed plane pairs (2z, 2z+1), lpb of them at a time.
-__global__ void __launch_bounds__(512) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int nx, int WP, CorrPlanDev plan,
-                           LinePlan lp, int lpb, float2* __restrict__ half, size_t pstride) {
+// The row's 5 stack values per cell are staged in shared memory once (after the line buffers).
+template <class F>
+__global__ void __launch_bounds__(256, 2) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int WP,
+                                                     CorrPlanDev plan, F f, int lpb, float2* __restrict__ half,
+                                                     size_t pstride) {
     extern __shared__ float2 smem[];
+    const int nx = f.n(), tl = f.tl();
     const int y = blockIdx.x;
-    const int line = threadIdx.x / lp.tl;
-    const int t = threadIdx.x - line * lp.tl;
+    const int line = threadIdx.x / tl;
+    const int t = threadIdx.x - line * tl;
     const int pl = padded_len(nx);
-    float2* buf = smem + line * pl;
+    float2* buf = smem + (line < lpb ? line : 0) * pl;
+    float* row = reinterpret_cast<float*>(smem + lpb * pl);  // [5][cw]
+    __shared__ int planes[16];
+    if (threadIdx.x < 16) planes[threadIdx.x] = threadIdx.x < plan.n_real ? plan.planes[threadIdx.x] : -1;
     const size_t gn = (size_t)cw * ch;
+    for (int i = threadIdx.x; i < 5 * cw; i += blockDim.x) {
+        const int p = i / cw, x = i - p * cw;
+        row[i] = __ldg(&grid[p * gn + (size_t)y * cw + x]);
+    }
+    __syncthreads();
     const int n_cplx = (plan.n_real + 1) / 2;
     for (int z0 = 0; z0 < n_cplx; z0 += lpb) {
         const int z = z0 + line;
         const bool act = line < lpb && z < n_cplx;
         if (act) {
-            const int ra = plan.planes[2 * z];
-            const int rb = (2 * z + 1 < plan.n_real) ? plan.planes[2 * z + 1] : -1;
-            for (int x = t; x < nx; x += lp.tl) {
+            const int ra = planes[2 * z];
+            const int rb = planes[2 * z + 1];
+            for (int x = t; x < nx; x += tl) {
                 float2 v = make_float2(0.f, 0.f);
                 if (x < cw) {
-                    float s[5];
-#pragma unroll
-                    for (int p = 0; p < 5; ++p) s[p] = __ldg(&grid[p * gn + (size_t)y * cw + x]);
-                    v.x = real_plane(ra, s);
-                    if (rb >= 0) v.y = real_plane(rb, s);
+                    v.x = real_plane_row(ra, row, cw, x);
+                    if (rb >= 0) v.y = real_plane_row(rb, row, cw, x);
                 }
                 buf[pad_idx(x)] = v;
             }
         }
         __syncthreads();
-        line_fft<false>(buf, lp, act ? t : kNoLine);
+        f.template run<false>(buf, t, act);
         if (act) {
             const bool has_b = 2 * z + 1 < plan.n_real;
             float2* oa = half + (size_t)(2 * z) * pstride + (size_t)y * WP;
             float2* ob = half + (size_t)(2 * z + 1) * pstride + (size_t)y * WP;
-            for (int x = t; x <= nx / 2; x += lp.tl) {
+            for (int x = t; x <= nx / 2; x += tl) {
                 const float2 Z = buf[pad_idx(x)];
                 const float2 Zm = buf[pad_idx(x == 0 ? 0 : nx - x)];
                 oa[x] = make_float2(0.5f * (Z.x + Zm.x), 0.5f * (Z.y - Zm.y));
@@ -184,24 +204,33 @@ __global__ void __launch_bounds__(512) k_fwd_rows(const float* __restrict__ grid
 }
 
 // Column FFTs of the half spectra, in place: block = a tile of tx columns of one plane; rows
-// ≥ rows_in read as zero. INV: inverse transform.
-template <bool INV>
-__global__ void __launch_bounds__(512, 1) k_cols(float2* __restrict__ half, size_t pstride, int WP, int ncols, int rows_in, LinePlan lp,
-                       int tx) {
+// ≥ rows_in read as zero. Loads and stores go 8 per thread at a time (all in flight together).
+template <class F, bool INV>
+__global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size_t pstride, int WP, int ncols,
+                                                 int rows_in, F f, int tx) {
     extern __shared__ float2 smem[];
     const int x0 = blockIdx.x * tx;
     float2* base = half + (size_t)blockIdx.y * pstride;
-    const int ny = lp.n, pl = padded_len(ny);
+    const int ny = f.n(), pl = line_pitch(ny), tl = f.tl();
     const int total = tx * ny;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int y = e / tx, c = e - y * tx;
-        float2 v = make_float2(0.f, 0.f);
-        if (y < rows_in && x0 + c < ncols) v = base[(size_t)y * WP + x0 + c];
-        smem[c * pl + pad_idx(y)] = v;
+    for (int e0 = 0; e0 < total; e0 += 8 * blockDim.x) {
+        float2 v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = e0 + i * blockDim.x + threadIdx.x;
+            const int y = e / tx, c = e - y * tx;
+            v[i] = (e < total && y < rows_in && x0 + c < ncols) ? base[(size_t)y * WP + x0 + c] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = e0 + i * blockDim.x + threadIdx.x;
+            const int y = e / tx, c = e - y * tx;
+            if (e < total) smem[c * pl + pad_idx(y)] = v[i];
+        }
     }
     __syncthreads();
-    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
-    line_fft<INV>(smem + (line < tx ? line : 0) * pl, lp, line < tx ? t : kNoLine);
+    const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
+    f.template run<INV>(smem + (line < tx ? line : 0) * pl, t, line < tx);
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int y = e / tx, c = e - y * tx;
         if (x0 + c < ncols) base[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
@@ -211,28 +240,39 @@ __global__ void __launch_bounds__(512, 1) k_cols(float2* __restrict__ half, size
 // ── inverse: products and column IFFTs ──────────────────────────────────────────────────────
 
 // block (correlation slot k, column tile): P = A·conj(B) on the tile, inverse column FFT → Q
-__global__ void __launch_bounds__(512, 1) k_inv_cols(const float2* __restrict__ ha, const float2* __restrict__ hb, size_t pstride, int WP,
-                           int ncols, CorrPlanDev plan, LinePlan lp, int tx, float2* __restrict__ Q) {
+template <class F>
+__global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ ha, const float2* __restrict__ hb,
+                                                     size_t pstride, int WP, int ncols, CorrPlanDev plan, F f, int tx,
+                                                     float2* __restrict__ Q) {
     extern __shared__ float2 smem[];
     const int k = blockIdx.x;
     const int x0 = blockIdx.y * tx;
     const float2* A = ha + (size_t)plan.ca[k] * pstride;
     const float2* B = hb + (size_t)plan.cb[k] * pstride;
     float2* O = Q + (size_t)k * pstride;
-    const int ny = lp.n, pl = padded_len(ny);
+    const int ny = f.n(), pl = line_pitch(ny), tl = f.tl();
     const int total = tx * ny;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int y = e / tx, c = e - y * tx;
-        float2 v = make_float2(0.f, 0.f);
-        if (x0 + c < ncols) {
-            const size_t i = (size_t)y * WP + x0 + c;
-            v = cmulc(__ldg(&A[i]), __ldg(&B[i]));
+    for (int e0 = 0; e0 < total; e0 += 4 * blockDim.x) {
+        float2 a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = e0 + i * blockDim.x + threadIdx.x;
+            const int y = e / tx, c = e - y * tx;
+            const bool ok = e < total && x0 + c < ncols;
+            const size_t ix = (size_t)y * WP + x0 + c;
+            a[i] = ok ? __ldg(&A[ix]) : make_float2(0.f, 0.f);
+            b[i] = ok ? __ldg(&B[ix]) : make_float2(0.f, 0.f);
         }
-        smem[c * pl + pad_idx(y)] = v;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = e0 + i * blockDim.x + threadIdx.x;
+            const int y = e / tx, c = e - y * tx;
+            if (e < total) smem[c * pl + pad_idx(y)] = cmulc(a[i], b[i]);
+        }
     }
     __syncthreads();
-    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
-    line_fft<true>(smem + (line < tx ? line : 0) * pl, lp, line < tx ? t : kNoLine);
+    const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
+    f.template run<true>(smem + (line < tx ? line : 0) * pl, t, line < tx);
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int y = e / tx, c = e - y * tx;
         if (x0 + c < ncols) O[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
@@ -241,102 +281,138 @@ __global__ void __launch_bounds__(512, 1) k_inv_cols(const float2* __restrict__ 
 
 // ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
 
-__device__ __forceinline__ int tri_k(int i, int j) {
-    const int a = min(i, j), b = max(i, j);
-    return a * 4 - (a * (a + 1)) / 2 + b;
+// The correlation plan as compile-time tables (src/smi.zig:90-158): the moving and fixed plane
+// of correlation c, and its slot in a plan that drops the fourth feature's planes.
+__host__ __device__ constexpr int corr_a(int c) {
+    return c == 0 ? 0 : c <= 4 ? c : c <= 8 ? 0 : c <= 24 ? 1 + (c - 9) / 4 : c <= 34 ? 5 + (c - 25) : 0;
+}
+__host__ __device__ constexpr int corr_b(int c) {
+    return c <= 4 ? 0 : c <= 8 ? c - 4 : c <= 24 ? 1 + (c - 9) % 4 : c <= 34 ? 0 : 5 + (c - 35);
+}
+__host__ __device__ constexpr bool fourth_plane(int p) { return p == 4 || p == 8 || p == 11 || p == 13 || p == 14; }
+__host__ __device__ constexpr bool corr_kept(int c, bool three) {
+    return !three || (!fourth_plane(corr_a(c)) && !fourth_plane(corr_b(c)));
+}
+__host__ __device__ constexpr int corr_slot(int c, bool three) {
+    int s = 0;
+    for (int i = 0; i < c; ++i) s += corr_kept(i, three) ? 1 : 0;
+    return s;
 }
 
-// In-place 4×4 Cholesky (lower), false when a pivot is not > 0 (smi.wgsl:798-813), float64.
-__device__ __forceinline__ bool chol4d(double* g) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-#pragma unroll
-        for (int j = 0; j <= i; ++j) {
-            double s = g[i * 4 + j];
-#pragma unroll
-            for (int k = 0; k < j; ++k) s -= g[i * 4 + k] * g[j * 4 + k];
-            if (i == j) {
-                if (!(s > 0.0)) return false;
-                g[i * 5] = sqrt(s);
-            } else {
-                g[i * 4 + j] = s / g[j * 5];
-            }
-        }
-    }
-    return true;
+__host__ __device__ constexpr int tri_kc(int i, int j) {
+    return (i < j ? i : j) * 4 - ((i < j ? i : j) * ((i < j ? i : j) + 1)) / 2 + (i < j ? j : i);
 }
 
-// Per-shift score (smi.wgsl:825-915, combine_cell) in float64. c: the 45 sums (absent ones 0),
-// already scaled. n00: the overlap at lag 0.
-__device__ float combine_cell(const double* c, const CombineParams& p, double n00) {
-    const int nf = p.nf;
-    const double n = c[0];
-    const bool calib = p.exact && p.calib;
+// Per-shift score (smi.wgsl:825-915, combine_cell) in float64 with every index known at compile
+// time (NF features, exact or global whitening, calibrated or not), so the 4×4 algebra stays in
+// registers. `col` points at this shift's entry of slot 0 in the [slot][L] sums; the slots
+// follow the plan (NF = 3 drops the fourth feature's correlations). Each Cholesky pivot is
+// inverted once (rsqrt) and the substitutions multiply by it.
+template <int NF, bool EXACT, bool CALIB>
+__device__ __forceinline__ float combine_t(const float* __restrict__ col, int L, const CombineParams& p, double n00) {
+    constexpr bool THREE = NF == 3;
+    auto S = [&](int c) -> double { return (double)col[corr_slot(c, THREE) * L] * p.inv_nn; };
+    const double n = S(0);
     const double neff = n / fmax(p.area, 1.0);
     double floor_n = fmax((double)p.min_n, 0.08 * fmax(n00, 0.0));
-    if (calib) floor_n = (double)p.min_n;
-    if (n < floor_n || (calib && neff <= 10.0)) return 0.f;
-    const double den = fmax(n, 1e-8);
-    double ma[4] = {0, 0, 0, 0}, mb[4] = {0, 0, 0, 0};
-    for (int i = 0; i < nf; ++i) {
-        ma[i] = c[1 + i] / den;
-        mb[i] = c[5 + i] / den;
+    if (CALIB) floor_n = (double)p.min_n;
+    if (n < floor_n || (CALIB && neff <= 10.0)) return 0.f;
+    const double rn = 1.0 / fmax(n, 1e-8);
+    double ma[NF], mb[NF], C[NF][NF];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
+        ma[i] = S(1 + i) * rn;
+        mb[i] = S(5 + i) * rn;
     }
-    if (!p.exact) {
+#pragma unroll
+    for (int i = 0; i < NF; ++i)
+#pragma unroll
+        for (int j = 0; j < NF; ++j) C[i][j] = S(9 + 4 * i + j) * rn - ma[i] * mb[j];
+    if (!EXACT) {
         double s = 0.0;
-        for (int i = 0; i < nf; ++i)
-            for (int j = 0; j < nf; ++j) {
-                const double cij = fmin(fmax(c[9 + i * 4 + j] / den - ma[i] * mb[j], -1.0), 1.0);
-                s += cij * cij;
+#pragma unroll
+        for (int i = 0; i < NF; ++i)
+#pragma unroll
+            for (int j = 0; j < NF; ++j) {
+                const double c = fmin(fmax(C[i][j], -1.0), 1.0);
+                s += c * c;
             }
         const double sc = n * s;
         return (sc == sc) ? (float)sc : 0.f;
     }
-    double ga[16] = {0}, gb[16] = {0};
+    double A[NF][NF], B[NF][NF];
     double tra = 0.0, trb = 0.0;
-    for (int i = 0; i < nf; ++i) {
-        for (int j = 0; j < nf; ++j) {
-            const int k = tri_k(i, j);
-            ga[i * 4 + j] = c[25 + k] / den - ma[i] * ma[j];
-            gb[i * 4 + j] = c[35 + k] / den - mb[i] * mb[j];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            A[i][j] = S(25 + tri_kc(i, j)) * rn - ma[i] * ma[j];
+            B[i][j] = S(35 + tri_kc(i, j)) * rn - mb[i] * mb[j];
         }
-        tra += ga[i * 5];
-        trb += gb[i * 5];
+        tra += A[i][i];
+        trb += B[i][i];
     }
-    for (int i = 0; i < nf; ++i) {
-        ga[i * 5] += p.ridge * fmax(tra * 0.25, 1e-12);
-        gb[i * 5] += p.ridge * fmax(trb * 0.25, 1e-12);
+    const double rga = p.ridge * fmax(tra * 0.25, 1e-12), rgb = p.ridge * fmax(trb * 0.25, 1e-12);
+    double ia[NF], ib[NF];  // 1 / L_ii
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
+        A[i][i] += rga;
+        B[i][i] += rgb;
     }
-    for (int i = nf; i < 4; ++i) {
-        ga[i * 5] = 1.0;
-        gb[i * 5] = 1.0;
-    }
-    if (!chol4d(ga) || !chol4d(gb)) return 0.f;
-    double x[16];
-    for (int j = 0; j < nf; ++j)
-        for (int i = 0; i < nf; ++i) {
-            double s = c[9 + i * 4 + j] / den - ma[i] * mb[j];
-            for (int k = 0; k < i; ++k) s -= ga[i * 4 + k] * x[k * 4 + j];
-            x[i * 4 + j] = s / ga[i * 5];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            double sa = A[i][j], sb = B[i][j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) {
+                sa -= A[i][k] * A[j][k];
+                sb -= B[i][k] * B[j][k];
+            }
+            if (i == j) {
+                if (!(sa > 0.0) || !(sb > 0.0)) return 0.f;
+                ia[i] = rsqrt(sa);
+                ib[i] = rsqrt(sb);
+                A[i][i] = sa * ia[i];
+                B[i][i] = sb * ib[i];
+            } else {
+                A[i][j] = sa * ia[j];
+                B[i][j] = sb * ib[j];
+            }
         }
+    }
+    // X = L_A⁻¹ C (forward substitution down each column), in place in C
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+        for (int i = 0; i < NF; ++i) {
+            double s = C[i][j];
+#pragma unroll
+            for (int k = 0; k < i; ++k) s -= A[i][k] * C[k][j];
+            C[i][j] = s * ia[i];
+        }
+    // Y = X L_B⁻ᵀ row by row, ‖Y‖² as it goes
     double acc = 0.0;
-    for (int r = 0; r < nf; ++r) {
-        double yv[4];
-        for (int i = 0; i < nf; ++i) {
-            double s = x[r * 4 + i];
-            for (int k = 0; k < i; ++k) s -= gb[i * 4 + k] * yv[k];
-            yv[i] = s / gb[i * 5];
+#pragma unroll
+    for (int r = 0; r < NF; ++r) {
+        double yv[NF];
+#pragma unroll
+        for (int i = 0; i < NF; ++i) {
+            double s = C[r][i];
+#pragma unroll
+            for (int k = 0; k < i; ++k) s -= B[i][k] * yv[k];
+            yv[i] = s * ib[i];
             acc += yv[i] * yv[i];
         }
     }
     double score = n * acc;
-    if (calib) {
-        const double q = (double)nf;
+    if (CALIB) {
+        constexpr double q = NF;
         const double v = fmin(acc, q - 1e-4);
-        const double f = (neff - q - 1.0) / q * v / (q - v);
+        const double fv = (neff - q - 1.0) / q * v / (q - v);
         const double d1 = q * q, d2 = q * (neff - q - 1.0);
         const double a = 2.0 / (9.0 * d1), b = 2.0 / (9.0 * d2);
-        const double cc = cbrt(fmax(f, 0.0));
+        const double cc = cbrt(fmax(fv, 0.0));
         const double z = ((1.0 - b) * cc - (1.0 - a)) / sqrt(b * cc * cc + a);
         score = fmax(z, 0.0);
     }
@@ -346,15 +422,17 @@ __device__ float combine_cell(const double* c, const CombineParams& p, double n0
 // block (row y, split s): every correlation pair's row (Hermitian full row from the half
 // spectrum) pre-combined for outputs x ≡ s (mod S), inverse FFT of length L = nx/S, the sums
 // kept in shared memory; then the score of each of the row's L shifts and the block argmax.
-__global__ void __launch_bounds__(256, 1) k_inv_rows(const float2* __restrict__ Q, size_t pstride, int WP, int nx, int ny, int S,
-                           CorrPlanDev plan, LinePlan lp, int lpb, const float2* __restrict__ tw_nx,
-                           CombineParams cp, const double* __restrict__ n00p, float* __restrict__ map,
-                           unsigned long long* best, float* zero_out) {
+template <class F, int NF, bool EXACT, bool CALIB, int SS>
+__global__ void __launch_bounds__(512, 1) k_inv_rows(const float2* __restrict__ Q, size_t pstride, int WP, int nx, int S,
+                                                     CorrPlanDev plan, F f, int lpb, const float2* __restrict__ tw_nx,
+                                                     CombineParams cp, const double* __restrict__ n00p,
+                                                     float* __restrict__ map, unsigned long long* best,
+                                                     float* zero_out) {
     extern __shared__ float2 smem[];
     const int y = blockIdx.x / S, s = blockIdx.x - (blockIdx.x / S) * S;
-    const int L = lp.n, pl = padded_len(L);
+    const int L = f.n(), pl = padded_len(L), tl = f.tl();
     float* corr = reinterpret_cast<float*>(smem + lpb * pl);  // [n_corr][L]
-    const int line = threadIdx.x / lp.tl, t = threadIdx.x - line * lp.tl;
+    const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
     float2* buf = smem + (line < lpb ? line : 0) * pl;
     const int npairs = (plan.n_corr + 1) / 2;
     for (int p0 = 0; p0 < npairs; p0 += lpb) {
@@ -363,32 +441,59 @@ __global__ void __launch_bounds__(256, 1) k_inv_rows(const float2* __restrict__ 
         const int k1 = 2 * pr, k2 = (2 * pr + 1 < plan.n_corr) ? 2 * pr + 1 : -1;
         if (act) {
             const float2* q1 = Q + (size_t)k1 * pstride + (size_t)y * WP;
-            const float2* q2 = (k2 >= 0) ? Q + (size_t)k2 * pstride + (size_t)y * WP : nullptr;
-            for (int m = t; m < L; m += lp.tl) {
-                float2 acc = make_float2(0.f, 0.f);
-                for (int q = 0; q < S; ++q) {
-                    const int x = m + q * L;
-                    float2 z;
-                    if (x <= nx / 2) {
-                        const float2 a = __ldg(&q1[x]);
-                        const float2 b = q2 ? __ldg(&q2[x]) : make_float2(0.f, 0.f);
-                        z = make_float2(a.x - b.y, a.y + b.x);
-                    } else {
-                        const float2 a = __ldg(&q1[nx - x]);
-                        const float2 b = q2 ? __ldg(&q2[nx - x]) : make_float2(0.f, 0.f);
-                        z = make_float2(a.x + b.y, b.x - a.y);
+            const float2* q2 = (k2 >= 0) ? Q + (size_t)k2 * pstride + (size_t)y * WP : q1;
+            const bool has2 = k2 >= 0;
+            // the Hermitian full row, pre-combined for x ≡ s (mod S); loads of B points per
+            // thread issued together (S·2·B in flight)
+            constexpr int B = (SS == 1) ? 8 : 4;
+            const int per = (L + tl - 1) / tl;
+            for (int b0 = 0; b0 < per; b0 += B) {
+                float2 ra[B][SS > 0 ? SS : 1], rb[B][SS > 0 ? SS : 1];
+                if constexpr (SS > 0) {
+#pragma unroll
+                    for (int i = 0; i < B; ++i) {
+                        const int m = t + (b0 + i) * tl;
+#pragma unroll
+                        for (int q = 0; q < SS; ++q) {
+                            const int x = m + q * L;
+                            const int ix = (x <= nx / 2) ? x : nx - x;
+                            const bool ok = m < L;
+                            ra[i][q] = ok ? __ldg(&q1[ix]) : make_float2(0.f, 0.f);
+                            rb[i][q] = (ok && has2) ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
+                        }
                     }
-                    if (S > 1 && q > 0) z = cmul(z, cconj(__ldg(&tw_nx[(q * s * L) % nx])));
-                    acc = cadd(acc, z);
                 }
-                if (S > 1 && s > 0) acc = cmul(acc, cconj(__ldg(&tw_nx[m * s])));
-                buf[pad_idx(m)] = acc;
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    const int m = t + (b0 + i) * tl;
+                    if (m >= L) continue;
+                    float2 acc = make_float2(0.f, 0.f);
+                    const int nq = SS > 0 ? SS : S;
+                    for (int q = 0; q < nq; ++q) {
+                        const int x = m + q * L;
+                        float2 a, bb;
+                        if constexpr (SS > 0) {
+                            a = ra[i][q];
+                            bb = rb[i][q];
+                        } else {
+                            const int ix = (x <= nx / 2) ? x : nx - x;
+                            a = __ldg(&q1[ix]);
+                            bb = has2 ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
+                        }
+                        // Z = Q1 + i·Q2 on the half row; conj(Q1) + i·conj(Q2) on the mirrored half
+                        float2 z = (x <= nx / 2) ? make_float2(a.x - bb.y, a.y + bb.x) : make_float2(a.x + bb.y, bb.x - a.y);
+                        if (q > 0 && s > 0) z = cmul(z, cconj(__ldg(&tw_nx[(q * s * L) % nx])));
+                        acc = cadd(acc, z);
+                    }
+                    if (s > 0) acc = cmul(acc, cconj(__ldg(&tw_nx[m * s])));
+                    buf[pad_idx(m)] = acc;
+                }
             }
         }
         __syncthreads();
-        line_fft<true>(buf, lp, act ? t : kNoLine);
+        f.template run<true>(buf, t, act);
         if (act) {
-            for (int m = t; m < L; m += lp.tl) {
+            for (int m = t; m < L; m += tl) {
                 const float2 z = buf[pad_idx(m)];
                 corr[(size_t)k1 * L + m] = z.x;
                 if (k2 >= 0) corr[(size_t)k2 * L + m] = z.y;
@@ -400,11 +505,7 @@ __global__ void __launch_bounds__(256, 1) k_inv_rows(const float2* __restrict__ 
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
     for (int m = threadIdx.x; m < L; m += blockDim.x) {
-        double c[45];
-#pragma unroll
-        for (int i = 0; i < 45; ++i) c[i] = 0.0;
-        for (int k = 0; k < plan.n_corr; ++k) c[plan.cnum[k]] = (double)corr[(size_t)k * L + m] * cp.inv_nn;
-        const float sc = combine_cell(c, cp, n00);
+        const float sc = combine_t<NF, EXACT, CALIB>(corr + m, L, cp, n00);
         const int x = m * S + s;
         const uint32_t idx = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
         map[idx] = sc;
@@ -421,6 +522,19 @@ __global__ void __launch_bounds__(256, 1) k_inv_rows(const float2* __restrict__ 
         key = other > key ? other : key;
     }
     if ((threadIdx.x & 31) == 0 && key) atomicMax(best, key);
+}
+
+// The line policy for a plan: compile-time power-of-two lines for the common lengths, the
+// generic mixed-radix schedule otherwise.
+template <class Fn>
+cudaError_t with_line(const LinePlan& p, Fn&& fn) {
+    switch (p.n) {
+        case 256: return fn(Pow2Line<256>{p.tw});
+        case 512: return fn(Pow2Line<512>{p.tw});
+        case 1024: return fn(Pow2Line<1024>{p.tw});
+        case 2048: return fn(Pow2Line<2048>{p.tw});
+        default: return fn(GenericLine{p});
+    }
 }
 
 }  // namespace
@@ -463,22 +577,32 @@ static int lines_per_block(int tl, int want_threads) {
     return l < 1 ? 1 : l;
 }
 
+// threads per line of the policy with_line picks for this plan
+static int line_threads(const LinePlan& p) {
+    switch (p.n) {
+        case 256: case 512: case 1024: case 2048: return p.n / 16;
+        default: return p.tl;
+    }
+}
+
 cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& row,
                          float2* half, cudaStream_t st) {
     const size_t pstride = (size_t)g.ny * g.WP;
-    // lpb packed planes at a time, ~256 threads
-    const int lpb = lines_per_block(row.tl, 256);
+    const int tl = line_threads(row);
     const int n_cplx = (plan.n_real + 1) / 2;
-    const int lines = lpb < n_cplx ? lpb : n_cplx;
-    const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2);
-    cudaFuncSetAttribute(k_fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_fwd_rows<<<g.ch, lines * row.tl, sm, st>>>(grid, g.cw, g.ch, g.nx, g.WP, plan, row, lines, half, pstride);
-    return cudaGetLastError();
+    int lines = lines_per_block(tl, 256);
+    if (lines > n_cplx) lines = n_cplx;
+    const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)5 * g.cw * sizeof(float);
+    return with_line(row, [&](auto f) {
+        cudaFuncSetAttribute(k_fwd_rows<decltype(f)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_fwd_rows<<<g.ch, lines * tl, sm, st>>>(grid, g.cw, g.ch, g.WP, plan, f, lines, half, pstride);
+        return cudaGetLastError();
+    });
 }
 
 static int col_tile(const LinePlan& col) {
-    int tx = lines_per_block(col.tl, 512);
-    while (tx > 1 && (size_t)tx * padded_len(col.n) * sizeof(float2) > 160 * 1024) tx >>= 1;
+    int tx = lines_per_block(line_threads(col), 512);
+    while (tx > 1 && (size_t)tx * line_pitch(col.n) * sizeof(float2) > 110 * 1024) tx >>= 1;
     return tx;
 }
 
@@ -486,52 +610,98 @@ cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan
                          cudaStream_t st) {
     const size_t pstride = (size_t)g.ny * g.WP;
     const int ncols = g.nx / 2 + 1;
-    const int tx = col_tile(col);
-    const size_t sm = (size_t)tx * padded_len(g.ny) * sizeof(float2);
-    cudaFuncSetAttribute(k_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int tx = col_tile(col), tl = line_threads(col);
+    const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
     dim3 gc((ncols + tx - 1) / tx, plan.n_real);
-    k_cols<false><<<gc, tx * col.tl, sm, st>>>(half, pstride, g.WP, ncols, g.ch, col, tx);
-    return cudaGetLastError();
+    return with_line(col, [&](auto f) {
+        cudaFuncSetAttribute(k_cols<decltype(f), false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_cols<decltype(f), false><<<gc, tx * tl, sm, st>>>(half, pstride, g.WP, ncols, g.ch, f, tx);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t inverse_columns(const float2* ha, const float2* hb, const MapGeom& g, const CorrPlanDev& plan,
                             const LinePlan& col, float2* Q, cudaStream_t st) {
     const size_t pstride = (size_t)g.ny * g.WP;
     const int ncols = g.nx / 2 + 1;
-    const int tx = col_tile(col);
-    const size_t sm = (size_t)tx * padded_len(g.ny) * sizeof(float2);
-    cudaFuncSetAttribute(k_inv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int tx = col_tile(col), tl = line_threads(col);
+    const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
     dim3 gc(plan.n_corr, (ncols + tx - 1) / tx);
-    k_inv_cols<<<gc, tx * col.tl, sm, st>>>(ha, hb, pstride, g.WP, ncols, plan, col, tx, Q);
-    return cudaGetLastError();
+    return with_line(col, [&](auto f) {
+        cudaFuncSetAttribute(k_inv_cols<decltype(f)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_inv_cols<<<gc, tx * tl, sm, st>>>(ha, hb, pstride, g.WP, ncols, plan, f, tx, Q);
+        return cudaGetLastError();
+    });
+}
+
+// the row pass: power-of-two lines with 8 points per thread, as many lines as fit 512 threads
+// (the score phase uses all 512)
+static int row_threads(const LinePlan& p) {
+    switch (p.n) {
+        case 256: case 512: case 1024: case 2048: return p.n / 8;
+        default: return p.tl;
+    }
+}
+static int row_lines(int tl) { return lines_per_block(tl, 512) < 4 ? lines_per_block(tl, 512) : 4; }
+
+template <class Fn>
+cudaError_t with_row_line(const LinePlan& p, Fn&& fn) {
+    switch (p.n) {
+        case 256: return fn(Pow2Line<256, 32>{p.tw});
+        case 512: return fn(Pow2Line<512, 64>{p.tw});
+        case 1024: return fn(Pow2Line<1024, 128>{p.tw});
+        case 2048: return fn(Pow2Line<2048, 256>{p.tw});
+        default: return fn(GenericLine{p});
+    }
 }
 
 size_t row_pass_smem(int L, int n_corr, int tl) {
-    const int lpb = lines_per_block(tl, 256);
-    return (size_t)lpb * padded_len(L) * sizeof(float2) + (size_t)n_corr * L * sizeof(float);
+    return (size_t)row_lines(tl) * padded_len(L) * sizeof(float2) + (size_t)n_corr * L * sizeof(float);
 }
 
 int row_split(int nx, int n_corr) {
     for (int S = 1; S <= 64; ++S) {
         if (nx % S) continue;
         const int L = nx / S;
+        if (L > kMaxLine) continue;
         int tl = (L + 15) / 16;
         tl = ((tl + 31) / 32) * 32;
+        if (L == 256 || L == 512 || L == 1024 || L == 2048) tl = L / 8;
+        if (tl > 512) continue;
         if (row_pass_smem(L, n_corr, tl) <= 220 * 1024) return S;
     }
     return 0;
 }
 
+template <class F, int NF, bool EXACT, bool CALIB>
+static cudaError_t launch_rows(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, F f, int S,
+                               const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
+                               unsigned long long* best, float* zero, int lpb, size_t sm, cudaStream_t st) {
+    auto k = S == 1 ? k_inv_rows<F, NF, EXACT, CALIB, 1> : S == 2 ? k_inv_rows<F, NF, EXACT, CALIB, 2>
+                                                                 : k_inv_rows<F, NF, EXACT, CALIB, 0>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<g.ny * S, 512, sm, st>>>(Q, (size_t)g.ny * g.WP, g.WP, g.nx, S, plan, f, lpb, tw_nx, cp, n00, map, best, zero);
+    return cudaGetLastError();
+}
+
 cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
                                int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
                                unsigned long long* best, float* zero, cudaStream_t st) {
-    const size_t pstride = (size_t)g.ny * g.WP;
-    const int lpb = lines_per_block(line.tl, 256);
-    const size_t sm = row_pass_smem(line.n, plan.n_corr, line.tl);
-    cudaFuncSetAttribute(k_inv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_inv_rows<<<g.ny * S, lpb * line.tl, sm, st>>>(Q, pstride, g.WP, g.nx, g.ny, S, plan, line, lpb, tw_nx, cp, n00,
-                                                   map, best, zero);
-    return cudaGetLastError();
+    const int tl = row_threads(line);
+    const int lpb = row_lines(tl);
+    if (lpb * tl > 512) return cudaErrorInvalidConfiguration;
+    const size_t sm = row_pass_smem(line.n, plan.n_corr, tl);
+    return with_row_line(line, [&](auto f) {
+        using Fp = decltype(f);
+        if (cp.nf == 4) {
+            if (!cp.exact) return launch_rows<Fp, 4, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+            if (cp.calib) return launch_rows<Fp, 4, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+            return launch_rows<Fp, 4, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+        }
+        if (!cp.exact) return launch_rows<Fp, 3, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+        if (cp.calib) return launch_rows<Fp, 3, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+        return launch_rows<Fp, 3, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+    });
 }
 
 }  // namespace zc
