@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace zc {
@@ -33,6 +34,7 @@ void DevBuf::release() {
 }
 
 Engine::Engine(int dev) : device(dev) {
+    if (const char* v = getenv("ZCMIR_B200_ROW_PASS")) row_pass = v;
     cudaSetDevice(dev);
     cudaGetDeviceProperties(&prop, dev);
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -358,9 +360,15 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev) {
                  "inverse columns"))
         return false;
     rec(4);
-    if (!cuda_ok(inverse_rows_score(q_.as<float2>(), g, job.plan, job.line, job.S, twiddles(g.nx), job.cp, n00,
-                                    map_.as<float>(), best, zero, st),
-                 "inverse rows"))
+    const bool tmem = row_pass != "split" && rows_tmem_supported(g.nx, job.plan.n_corr);
+    if (tmem) {
+        if (!cuda_ok(inverse_rows_score_tmem(q_.as<float2>(), g, job.plan, twiddles(g.nx), job.cp, n00, map_.as<float>(),
+                                             best, zero, st),
+                     "inverse rows (tensor memory)"))
+            return false;
+    } else if (!cuda_ok(inverse_rows_score(q_.as<float2>(), g, job.plan, job.line, job.S, twiddles(g.nx), job.cp, n00,
+                                           map_.as<float>(), best, zero, st),
+                        "inverse rows"))
         return false;
     rec(5);
     counts[0] += job.identity_grid ? 10 : 12;

@@ -80,6 +80,9 @@ class Engine {
     // counters since the last zc_gpu_counts: launches, submits, reads, waits
     uint32_t counts[4] = {0, 0, 0, 0};
     bool profiling = false;
+    // the last pass: "tmem" (sums in tensor memory, whole rows) or "split" (rows split S ways,
+    // sums in shared memory); from ZCMIR_B200_ROW_PASS at creation, "tmem" by default
+    std::string row_pass = "tmem";
     std::map<std::string, std::pair<double, uint32_t>> prof;  // name → (ms, count)
 
     bool fail(const std::string& m);

@@ -76,6 +76,11 @@ cudaError_t inverse_columns(const float2* half_a, const float2* half_b, const Ma
 cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
                                int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
                                unsigned long long* best, float* zero, cudaStream_t st);
+// the same pass with the sums in tensor memory: a whole row per block (nx ∈ {512, 1024, 2048})
+bool rows_tmem_supported(int nx, int n_corr);
+cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const float2* tw_nx,
+                                    const CombineParams& cp, const double* n00, float* map, unsigned long long* best,
+                                    float* zero, cudaStream_t st);
 // the split S of the row pass for nx (smallest divisor keeping its shared memory in budget); 0
 // when none fits
 int row_split(int nx, int n_corr);

@@ -13,13 +13,12 @@
 //      inverse row FFT, and the per-shift score in float64 with its argmax, without writing a
 //      correlation plane to memory. Rows longer than shared memory holds for all C correlations
 //      are split S ways by one decimation-in-frequency step (output shifts x ≡ s mod S).
+#include "combine.cuh"
 #include "common.cuh"
 #include "kernels.hpp"
 
 namespace zc {
 namespace {
-
-constexpr int kNoLine = 1 << 30;
 
 // ── canvas (smi.wgsl:1655-1706) ──────────────────────────────────────────────────────────────
 
@@ -126,18 +125,8 @@ __global__ void k_lag0(const float* __restrict__ a, const float* __restrict__ b,
 
 // ── forward: real planes → row R2C → column FFT ─────────────────────────────────────────────
 
-// Real correlation plane r from the premultiplied samples s = [w, w f0..w f3]
+// Real correlation plane r of a staged row [5][cw] of premultiplied samples s = [w, w f0..w f3]
 // (smi.wgsl:641-649): 0 → w, 1..4 → w f_i, 5..14 → s_i s_j / s_0 (0 where s_0 ≤ 1e-6).
-__device__ __forceinline__ float real_plane(int r, const float* s) {
-    if (r < 5) return s[r];
-    if (s[0] <= 1e-6f) return 0.f;
-    const int k = r - 5;
-    const int ti = (k < 4) ? 0 : (k < 7) ? 1 : (k < 9) ? 2 : 3;
-    const int tj = (k < 4) ? k : (k < 7) ? k - 3 : (k < 9) ? k - 5 : 3;
-    return s[1 + ti] * s[1 + tj] / s[0];
-}
-
-// real_plane on a staged row [5][cw] (indexing shared memory, not a register array)
 __device__ __forceinline__ float real_plane_row(int r, const float* row, int cw, int x) {
     if (r < 5) return row[r * cw + x];
     const float s0 = row[x];
@@ -281,144 +270,6 @@ __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ 
 
 // ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
 
-// The correlation plan as compile-time tables (src/smi.zig:90-158): the moving and fixed plane
-// of correlation c, and its slot in a plan that drops the fourth feature's planes.
-__host__ __device__ constexpr int corr_a(int c) {
-    return c == 0 ? 0 : c <= 4 ? c : c <= 8 ? 0 : c <= 24 ? 1 + (c - 9) / 4 : c <= 34 ? 5 + (c - 25) : 0;
-}
-__host__ __device__ constexpr int corr_b(int c) {
-    return c <= 4 ? 0 : c <= 8 ? c - 4 : c <= 24 ? 1 + (c - 9) % 4 : c <= 34 ? 0 : 5 + (c - 35);
-}
-__host__ __device__ constexpr bool fourth_plane(int p) { return p == 4 || p == 8 || p == 11 || p == 13 || p == 14; }
-__host__ __device__ constexpr bool corr_kept(int c, bool three) {
-    return !three || (!fourth_plane(corr_a(c)) && !fourth_plane(corr_b(c)));
-}
-__host__ __device__ constexpr int corr_slot(int c, bool three) {
-    int s = 0;
-    for (int i = 0; i < c; ++i) s += corr_kept(i, three) ? 1 : 0;
-    return s;
-}
-
-__host__ __device__ constexpr int tri_kc(int i, int j) {
-    return (i < j ? i : j) * 4 - ((i < j ? i : j) * ((i < j ? i : j) + 1)) / 2 + (i < j ? j : i);
-}
-
-// Per-shift score (smi.wgsl:825-915, combine_cell) in float64 with every index known at compile
-// time (NF features, exact or global whitening, calibrated or not), so the 4×4 algebra stays in
-// registers. `col` points at this shift's entry of slot 0 in the [slot][L] sums; the slots
-// follow the plan (NF = 3 drops the fourth feature's correlations). Each Cholesky pivot is
-// inverted once (rsqrt) and the substitutions multiply by it.
-template <int NF, bool EXACT, bool CALIB>
-__device__ __forceinline__ float combine_t(const float* __restrict__ col, int L, const CombineParams& p, double n00) {
-    constexpr bool THREE = NF == 3;
-    auto S = [&](int c) -> double { return (double)col[corr_slot(c, THREE) * L] * p.inv_nn; };
-    const double n = S(0);
-    const double neff = n / fmax(p.area, 1.0);
-    double floor_n = fmax((double)p.min_n, 0.08 * fmax(n00, 0.0));
-    if (CALIB) floor_n = (double)p.min_n;
-    if (n < floor_n || (CALIB && neff <= 10.0)) return 0.f;
-    const double rn = 1.0 / fmax(n, 1e-8);
-    double ma[NF], mb[NF], C[NF][NF];
-#pragma unroll
-    for (int i = 0; i < NF; ++i) {
-        ma[i] = S(1 + i) * rn;
-        mb[i] = S(5 + i) * rn;
-    }
-#pragma unroll
-    for (int i = 0; i < NF; ++i)
-#pragma unroll
-        for (int j = 0; j < NF; ++j) C[i][j] = S(9 + 4 * i + j) * rn - ma[i] * mb[j];
-    if (!EXACT) {
-        double s = 0.0;
-#pragma unroll
-        for (int i = 0; i < NF; ++i)
-#pragma unroll
-            for (int j = 0; j < NF; ++j) {
-                const double c = fmin(fmax(C[i][j], -1.0), 1.0);
-                s += c * c;
-            }
-        const double sc = n * s;
-        return (sc == sc) ? (float)sc : 0.f;
-    }
-    double A[NF][NF], B[NF][NF];
-    double tra = 0.0, trb = 0.0;
-#pragma unroll
-    for (int i = 0; i < NF; ++i) {
-#pragma unroll
-        for (int j = 0; j <= i; ++j) {
-            A[i][j] = S(25 + tri_kc(i, j)) * rn - ma[i] * ma[j];
-            B[i][j] = S(35 + tri_kc(i, j)) * rn - mb[i] * mb[j];
-        }
-        tra += A[i][i];
-        trb += B[i][i];
-    }
-    const double rga = p.ridge * fmax(tra * 0.25, 1e-12), rgb = p.ridge * fmax(trb * 0.25, 1e-12);
-    double ia[NF], ib[NF];  // 1 / L_ii
-#pragma unroll
-    for (int i = 0; i < NF; ++i) {
-        A[i][i] += rga;
-        B[i][i] += rgb;
-    }
-#pragma unroll
-    for (int i = 0; i < NF; ++i) {
-#pragma unroll
-        for (int j = 0; j <= i; ++j) {
-            double sa = A[i][j], sb = B[i][j];
-#pragma unroll
-            for (int k = 0; k < j; ++k) {
-                sa -= A[i][k] * A[j][k];
-                sb -= B[i][k] * B[j][k];
-            }
-            if (i == j) {
-                if (!(sa > 0.0) || !(sb > 0.0)) return 0.f;
-                ia[i] = rsqrt(sa);
-                ib[i] = rsqrt(sb);
-                A[i][i] = sa * ia[i];
-                B[i][i] = sb * ib[i];
-            } else {
-                A[i][j] = sa * ia[j];
-                B[i][j] = sb * ib[j];
-            }
-        }
-    }
-    // X = L_A⁻¹ C (forward substitution down each column), in place in C
-#pragma unroll
-    for (int j = 0; j < NF; ++j)
-#pragma unroll
-        for (int i = 0; i < NF; ++i) {
-            double s = C[i][j];
-#pragma unroll
-            for (int k = 0; k < i; ++k) s -= A[i][k] * C[k][j];
-            C[i][j] = s * ia[i];
-        }
-    // Y = X L_B⁻ᵀ row by row, ‖Y‖² as it goes
-    double acc = 0.0;
-#pragma unroll
-    for (int r = 0; r < NF; ++r) {
-        double yv[NF];
-#pragma unroll
-        for (int i = 0; i < NF; ++i) {
-            double s = C[r][i];
-#pragma unroll
-            for (int k = 0; k < i; ++k) s -= B[i][k] * yv[k];
-            yv[i] = s * ib[i];
-            acc += yv[i] * yv[i];
-        }
-    }
-    double score = n * acc;
-    if (CALIB) {
-        constexpr double q = NF;
-        const double v = fmin(acc, q - 1e-4);
-        const double fv = (neff - q - 1.0) / q * v / (q - v);
-        const double d1 = q * q, d2 = q * (neff - q - 1.0);
-        const double a = 2.0 / (9.0 * d1), b = 2.0 / (9.0 * d2);
-        const double cc = cbrt(fmax(fv, 0.0));
-        const double z = ((1.0 - b) * cc - (1.0 - a)) / sqrt(b * cc * cc + a);
-        score = fmax(z, 0.0);
-    }
-    return (score == score) ? (float)score : 0.f;
-}
-
 // block (row y, split s): every correlation pair's row (Hermitian full row from the half
 // spectrum) pre-combined for outputs x ≡ s (mod S), inverse FFT of length L = nx/S, the sums
 // kept in shared memory; then the score of each of the row's L shifts and the block argmax.
@@ -505,7 +356,7 @@ __global__ void __launch_bounds__(512, 1) k_inv_rows(const float2* __restrict__ 
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
     for (int m = threadIdx.x; m < L; m += blockDim.x) {
-        const float sc = combine_t<NF, EXACT, CALIB>(corr + m, L, cp, n00);
+        const float sc = combine_t<NF, EXACT, CALIB>([&](int k) { return corr[(size_t)k * L + m]; }, cp, n00);
         const int x = m * S + s;
         const uint32_t idx = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
         map[idx] = sc;
