@@ -50,7 +50,8 @@ Engine::~Engine() {
         s.stack.release();
     }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
-                      &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_})
+                      &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
+                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_})
         b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);

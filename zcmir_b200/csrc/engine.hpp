@@ -44,6 +44,15 @@ struct Side {
     bool half = false;
 };
 
+// Scores (and optionally the symmetric gradient and Gauss–Newton matrix) at one pose.
+struct PoseEval {
+    double fwd = 0, inv = 0, mean = 0, n = 0;  // scores; n: the forward overlap
+    bool has_inv = false, has_grad = false, has_hess = false;
+    std::array<double, 45> sums{};             // the forward direction's moment sums
+    std::array<double, 8> grad{};              // over the group's tangent coordinates
+    std::array<double, 64> hess{};             // nk × nk
+};
+
 // One map's plan and device-side description.
 struct MapJob {
     Frame fr;
@@ -105,6 +114,15 @@ class Engine {
     bool bench_maps(const Mat3& H, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
                     size_t out_len);
 
+    // poses (engine_pose.cpp): both directions (or the forward one) of many poses in one pass
+    bool eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::vector<PoseEval>& out,
+                    bool forward_only = false);
+    bool moments(const Mat3& H, double* out45);
+    bool score3(const Mat3& H, double* out3);
+    bool gradient(const Mat3& H, bool hess, zc_grad_result* out);
+    bool climb(zc_climb_result* out);
+    void log_event(const std::string& text);
+
   private:
     bool build_side(int s);
     bool line_plan(int n, LinePlan& p);
@@ -113,6 +131,8 @@ class Engine {
     FeatScratch fs_;
     DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
+    DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
+    std::vector<float> pose_host_;
     std::map<int, float2*> tw_;
 };
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -159,9 +160,17 @@ void zc_swap(zc_engine* e) {
     if (e) std::swap(e->side[0], e->side[1]);
 }
 
-int32_t zc_moments(zc_engine* e, const double*, double*) { return unsupported(e, "moments"); }
-int32_t zc_score(zc_engine* e, const double*, double*) { return unsupported(e, "score"); }
-int32_t zc_gradient(zc_engine* e, const double*, uint32_t, zc_grad_result*) { return unsupported(e, "gradient"); }
+int32_t zc_moments(zc_engine* e, const double H[9], double out[45]) {
+    return guarded(e, "moments", [&] { return e->moments(mat(H), out); });
+}
+
+int32_t zc_score(zc_engine* e, const double H[9], double out[3]) {
+    return guarded(e, "score", [&] { return e->score3(mat(H), out); });
+}
+
+int32_t zc_gradient(zc_engine* e, const double H[9], uint32_t hess, zc_grad_result* out) {
+    return guarded(e, "gradient", [&] { return e->gradient(mat(H), hess != 0, out); });
+}
 
 int32_t zc_shift_map(zc_engine* e, const double H[9], uint32_t flags, uint32_t cap, zc_shift_result* out, float* map,
                      size_t map_len) {
@@ -190,7 +199,9 @@ void zc_get_pose(zc_engine* e, double H[9]) {
         for (int i = 0; i < 9; ++i) H[i] = e->H[i];
 }
 
-int32_t zc_climb(zc_engine* e, zc_climb_result*) { return unsupported(e, "climb"); }
+int32_t zc_climb(zc_engine* e, zc_climb_result* out) {
+    return guarded(e, "climb", [&] { return e->climb(out); });
+}
 int32_t zc_search(zc_engine* e, zc_search_result*) { return unsupported(e, "search"); }
 
 void zc_cancel(zc_engine* e) {
@@ -239,7 +250,21 @@ void zc_gpu_counts(zc_engine* e, uint32_t out[4]) {
     }
 }
 
-int32_t zc_bench_moments(zc_engine* e, uint32_t, uint32_t) { return unsupported(e, "bench_moments"); }
+int32_t zc_bench_moments(zc_engine* e, uint32_t n_poses, uint32_t iters) {
+    // `iters` score passes over n_poses poses spread about the current pose (src/exports.zig:123-136)
+    return guarded(e, "bench_moments", [&] {
+        std::vector<zc::Mat3> Hs(std::max(1u, n_poses));
+        for (size_t i = 0; i < Hs.size(); ++i) {
+            const double t = (double)i * 0.37, a = 0.01 * std::sin(t);
+            Hs[i] = zc::mul3({std::cos(a), -std::sin(a), 3 * std::cos(t), std::sin(a), std::cos(a), 3 * std::sin(t), 0, 0, 1},
+                             e->H);
+        }
+        std::vector<zc::PoseEval> r;
+        for (uint32_t k = 0; k < std::max(1u, iters); ++k)
+            if (!e->eval_poses(Hs, false, false, r, true)) return false;
+        return true;
+    });
+}
 
 void zc_tune_parts(uint32_t, uint32_t, uint32_t, uint32_t) {}
 

@@ -225,17 +225,16 @@ __global__ void __launch_bounds__(320) k_acf(const float* __restrict__ feat, int
     if (lag >= 289) return;
     const int dx = lag % 17 - 8, dy = lag / 17 - 8;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    const int tx_end = min(kAcfTile, w - x0), ty_end = min(kAcfTile, h - y0);
-    for (int ty = 0; ty < ty_end; ++ty) {
-        const int gy2 = y0 + ty + dy;
-        if (gy2 < 0 || gy2 >= h) continue;
-        for (int tx = 0; tx < tx_end; ++tx) {
-            const int gx2 = x0 + tx + dx;
-            if (gx2 < 0 || gx2 >= w) continue;
-            const int a = (ty + kAcfHalo) * kAcfSpan + tx + kAcfHalo;
-            const int b = a + dy * kAcfSpan + dx;
+    // pixels t of the tile whose partner t + τ lies in the image: a rectangle
+    const int tx0 = max(0, -dx - x0), tx1 = min(min(kAcfTile, w - x0), w - dx - x0);
+    const int ty0 = max(0, -dy - y0), ty1 = min(min(kAcfTile, h - y0), h - dy - y0);
+    for (int ty = ty0; ty < ty1; ++ty) {
+        const int a0 = (ty + kAcfHalo) * kAcfSpan + kAcfHalo;
+        const int b0 = a0 + dy * kAcfSpan + dx;
+#pragma unroll 4
+        for (int tx = tx0; tx < tx1; ++tx) {
 #pragma unroll
-            for (int p = 0; p < 4; ++p) acc[p] = fmaf(sh[p][a], sh[p][b], acc[p]);
+            for (int p = 0; p < 4; ++p) acc[p] = fmaf(sh[p][a0 + tx], sh[p][b0 + tx], acc[p]);
         }
     }
     const size_t o = ((size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 289 + lag) * 4;

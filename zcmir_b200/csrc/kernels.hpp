@@ -86,4 +86,19 @@ cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const Cor
 int row_split(int nx, int n_corr);
 size_t row_pass_smem(int L, int n_corr, int tl);
 
+// ── pose scores and gradients (pose.cu) ──
+struct PoseSide {
+    const float* feat;  // 4 whitened planes, plane-major
+    int w, h;
+};
+// the 45 sums of n poses of one direction (a sampled at H⁻¹x for every b pixel x); hinv: n
+// inverse poses (f32, row-major); sums: n × 45 float64 (zeroed here)
+cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st);
+// score (float64) and the 102 gradient coefficients (f32) of each pose's sums
+cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, double* score, cudaStream_t st);
+// tangent sums per pose: 8 gradient + 36 Gauss–Newton (upper triangle) float64 (zeroed here);
+// gens: 8 generators (9 f32 each) in b's pixel coordinates
+cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
+                         int n, bool hess, double* out, cudaStream_t st);
+
 }  // namespace zc
