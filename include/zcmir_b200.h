@@ -24,6 +24,19 @@ int32_t zcb_bench_maps(zc_engine* e, const double H[9], uint32_t flags, uint32_t
 int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, size_t* out_len, char* err,
                            size_t err_cap, size_t* err_len);
 
+/* Scores of n poses (Hs: n row-major 3×3 maps, each as zc_score's H) into out[3n], per pose the
+ * mean, forward and inverse score exactly as zc_score writes them, allocating no device memory.
+ * No counterpart in the reference (whose only pose score is zc_score, src/exports.zig:417). For
+ * hosts that cannot let a call allocate: zc_score grows its buffers with cudaMalloc/cudaFree,
+ * and cudaFree waits for the whole device (stalling the host's other streams), while a host that
+ * gave the GPU's free memory to its own pool can see that allocation fail. The scratch is one
+ * file-scope device array of 103,936 bytes: n ≤ 64 (larger n is rejected with an error), and
+ * calls that overlap in time (any engines on the same device) race on it; it keeps the last
+ * call's contents. The first call on each device looks up the array's address (make it before
+ * any stream capture begins). The feature planes must already be built for the current
+ * settings (by zc_set_image_gray, zc_score or zc_features); otherwise -1 with zc_error. 0 / -1. */
+int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,6 +119,8 @@ class Engine {
                     bool forward_only = false);
     bool moments(const Mat3& H, double* out45);
     bool score3(const Mat3& H, double* out3);
+    // scores of n ≤ 64 poses with every device buffer in a file-scope array (score_static.cu)
+    bool score_static(const double* Hs, int n, double* out3);
     bool gradient(const Mat3& H, bool hess, zc_grad_result* out);
     bool climb(zc_climb_result* out);
     void log_event(const std::string& text);

@@ -363,4 +363,9 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
     return 0;
 }
 
+int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out) {
+    // allocates no device memory: the scratch is a file-scope array (score_static.cu)
+    return guarded(e, "score_static", [&] { return e->score_static(Hs, (int)n, out); });
+}
+
 }  // extern "C"
