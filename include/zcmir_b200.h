@@ -24,6 +24,18 @@ int32_t zcb_bench_maps(zc_engine* e, const double H[9], uint32_t flags, uint32_t
 int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, size_t* out_len, char* err,
                            size_t err_cap, size_t* err_len);
 
+/* The sweep's batched maps alone (the first stage of zc_search) with the engine's sw_* settings
+ * and prior pose H0 (NULL: the pose zc_search would use). For every candidate (θ-major, then σ,
+ * shear, stretch) its n_peak (1..16) best lane maxima — score in fixed pixels, map index
+ * (0xffffffff: none) — into scores / idx (cap ≥ candidates × n_peak; both NULL: not returned).
+ * batch: candidates per launch (0: from a 1 GB budget). info[16]: [0] candidates, [1] cell (px),
+ * [2] device ms of the maps, [3] grid G, [4..5] fixed window Fx, Fy (cells), [6..7] its first
+ * cell, [8] overlap floor (cells), [9] largest plane side, [10] plane-size groups, [11] batches,
+ * [12] kernel launches, [13..14] canvas origin (px), [15] peaks. No counterpart in the reference
+ * (its sweep is internal to zc_search, src/search.zig:300-494). 0 / -1 with zc_error. */
+int32_t zcb_sweep(zc_engine* e, const double H0[9], uint32_t n_peak, uint32_t batch, float* scores, uint32_t* idx,
+                  size_t cap, double* info, size_t info_len);
+
 /* Scores of n poses (Hs: n row-major 3×3 maps, each as zc_score's H) into out[3n], per pose the
  * mean, forward and inverse score exactly as zc_score writes them, allocating no device memory.
  * No counterpart in the reference (whose only pose score is zc_score, src/exports.zig:417). For

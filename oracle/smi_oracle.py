@@ -438,7 +438,7 @@ def _chol4(G, nf):
     return L, ok
 
 
-def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, ridge=RIDGE):
+def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, ridge=RIDGE, n00=None):
     """Per-shift score from the correlation sums (``shaders/smi.wgsl:825-915``), float64.
 
     corr: (45, ...) sums (already scaled). Global: n·Σ clamp(C_ij, ±1)². Exact: n·‖L_A⁻¹ C
@@ -450,7 +450,8 @@ def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, rid
     n = c[0]
     calib = exact and calibrated
     neff = n / max(area, 1.0)
-    n00 = c[0, 0]
+    # the zero-lag overlap: lag 0 of the map, or where a sweep candidate sits (n00 given)
+    n00 = c[0, 0] if n00 is None else float(n00)
     floor_n = float(min_n) if calib else max(float(min_n), 0.08 * max(n00, 0.0))
     dead = (n < floor_n) | (calib & (neff <= 10.0))
     den = np.maximum(n, 1e-8)

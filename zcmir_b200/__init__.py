@@ -102,6 +102,16 @@ class Search:
     count_b: int
 
 
+@dataclass
+class Sweep:
+    """The sweep's batched maps (zcb_sweep): per candidate (θ-major, then σ, shear, stretch) its
+    best lane maxima — scores in fixed pixels, map indices (0xffffffff: none) — and the run's
+    figures (candidates, cell, device ms, plane sizes, batches, launches)."""
+    scores: np.ndarray
+    index: np.ndarray
+    info: dict
+
+
 class Registrar:
     """One GPU engine and one image pair, whose features stay on the GPU between calls.
 
@@ -304,6 +314,32 @@ class Registrar:
         r = _native.SearchResult()
         self._check(self._lib.zc_search(self._e, ctypes.byref(r)), "search")
         return Search(np.array(list(r.H)).reshape(3, 3), r.score, r.prev, bool(r.improved), r.count_a, r.count_b)
+
+    def _sweep_count(self):
+        s = self.settings
+        n = min(max(int(s["sw_nth"]), 1), 720) * min(max(int(s["sw_ns"]), 1), 129)
+        if s["sw_shear"] and float(s["sw_shear_max"]) > 0:
+            n *= min(max(int(s["sw_nshear"]), 1), 15)
+        if s["sw_aniso"] and float(s["sw_aniso_max"]) > 0:
+            n *= min(max(int(s["sw_naniso"]), 1), 15)
+        return n
+
+    def sweep(self, H0=None, n_peak=4, batch=0):
+        """The sweep's batched maps alone (the first stage of search()) at prior pose H0 (None: the
+        one search() uses), with the sw_* settings."""
+        nc = self._sweep_count()
+        sc = np.zeros((nc, n_peak), np.float32)
+        ix = np.zeros((nc, n_peak), np.uint32)
+        info = np.zeros(16)
+        a, h = (None, None) if H0 is None else _mat(H0)
+        self._check(self._lib.zcb_sweep(self._e, h, n_peak, batch, _fp(sc), ix.ctypes.data_as(_native.u32p), sc.size,
+                                        info.ctypes.data_as(_native.f64p), 16), "sweep")
+        keys = ("candidates", "cell", "ms", "grid", "Fx", "Fy", "fx0", "fy0", "min_n", "n", "groups", "batches",
+                "launches", "ox", "oy", "peaks")
+        d = {k: float(v) for k, v in zip(keys, info)}
+        if int(d["candidates"]) != nc:
+            raise RuntimeError(f"sweep: {int(d['candidates'])} candidates, expected {nc}")
+        return Sweep(sc, ix, d)
 
     # ── profiling ──
     def profile(self, on=True):

@@ -87,6 +87,7 @@ SIGS = {
     "zc_result_sizes": ([u32p], None),
     "zcb_bench_maps": ([P, f64p, U32, U32, U32, U32, f64p, SZ], I32),
     "zcb_score_static": ([P, f64p, U32, f64p], I32),
+    "zcb_sweep": ([P, f64p, U32, U32, f32p, u32p, SZ, f64p, SZ], I32),
     "zcb_settings_apply": ([ctypes.c_char_p, SZ, ctypes.c_char_p, SZ, ctypes.POINTER(SZ), ctypes.c_char_p, SZ, ctypes.POINTER(SZ)], I32),
 }
 

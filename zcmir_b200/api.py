@@ -5,6 +5,7 @@ starts from the defaults, so one call never changes another. Calls are serialise
 """
 import difflib
 import threading
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -89,6 +90,28 @@ def _prepare(moving, fixed, preprocess, kw):
     return reg, s, m, f
 
 
+@dataclass
+class Registration:
+    """A registered pair (python/zcmir/api.py:205-222, without the spline and keypoint fields):
+    H maps moving pixel coordinates to fixed ones (row-major 3×3, 1-based)."""
+    H: np.ndarray
+    score: float
+    model: str
+    moving_shape: tuple
+    fixed_shape: tuple
+    method: str = "refine"
+    iterations: int = 0
+
+    def __repr__(self):
+        return f"Registration({self.model}, score {self.score:.4g}, {self.method})"
+
+    def map_points(self, points):
+        """Moving (x, y) points (1-based, (n, 2)) to fixed coordinates by H."""
+        p = np.asarray(points, np.float64).reshape(-1, 2)
+        q = np.c_[p, np.ones(len(p))] @ self.H.T
+        return q[:, :2] / q[:, 2:]
+
+
 def shift_map(moving, fixed, H=None, *, preprocess=True, **settings):
     """The score at every translation of the moving image about pose H (default: identity)."""
     with _LOCK:
@@ -112,7 +135,8 @@ def register(moving, fixed, *, init=None, model="homography", preprocess=True, *
         reg, s, m, f = _prepare(moving, fixed, preprocess, dict(model=model, **settings))
         reg.pose = np.asarray(init, np.float64).reshape(3, 3)
         c = reg.climb()
-        return {"H": reg.pose, "score": reg.score(reg.pose).mean, "iterations": c.iterations, "moved": c.moved}
+        return Registration(H=reg.pose, score=reg.score(reg.pose).mean, model=s["group"], moving_shape=m.shape,
+                            fixed_shape=f.shape, method="refine", iterations=c.iterations)
 
 
 def refine(moving, fixed, H, **kw):
@@ -120,10 +144,38 @@ def refine(moving, fixed, H, **kw):
     return register(moving, fixed, init=H, **kw)
 
 
-def search(moving, fixed, H=None, *, mode="sweep", preprocess=True, **settings):
-    """Brute force over rotation × scale × shift about H."""
+def search(moving, fixed, H=None, *, mode="sweep", rotation=None, scale=None, shear=None, stretch=None,
+           preprocess=True, **settings):
+    """Brute force (python/zcmir/api.py:354-391): "sweep" scores every rotation × scale (× shear
+    × stretch) × shift, screens the best peaks by batched Gauss–Newton and climbs the finalists;
+    the pose H is kept unless the search scores higher. ("cloud" is not part of this build.)
+
+    Sweep ranges (each also settable through the sw_* settings):
+      rotation  degrees: a half-range (30 → ±30°) or a (from, to) range, which may run through
+                ±180°; default the full circle
+      scale     (min, max) of the moving image's scale; default (0.5, 2)
+      shear     largest shear either way, or (largest, values); off by default
+      stretch   largest stretch either way as a fraction, or (largest, values); off by default
+    """
+    if rotation is not None:
+        if np.ndim(rotation) == 0:
+            settings.update(sw_rot_range=False, sw_rot=float(rotation))
+        else:
+            lo, hi = rotation
+            settings.update(sw_rot_range=True, sw_rot_lo=float(lo), sw_rot_hi=float(hi))
+    if scale is not None:
+        settings.update(sw_smin=float(scale[0]), sw_smax=float(scale[1]))
+    for v, key in ((shear, "shear"), (stretch, "aniso")):
+        if v is None:
+            continue
+        mx, n = (v, None) if np.ndim(v) == 0 else v
+        settings[f"sw_{key}"] = float(mx) > 0
+        settings[f"sw_{key}_max"] = float(mx)
+        if n is not None:
+            settings[f"sw_n{key}"] = int(n)
     with _LOCK:
         reg, s, m, f = _prepare(moving, fixed, preprocess, dict(search_mode=mode, **settings))
         reg.pose = np.eye(3) if H is None else np.asarray(H, np.float64)
-        r = reg.search()
-        return {"H": reg.pose, "score": r.score, "previous": r.previous, "improved": r.improved}
+        reg.search()
+        return Registration(H=reg.pose, score=reg.score(reg.pose).mean, model=s["group"], moving_shape=m.shape,
+                            fixed_shape=f.shape, method=f"search ({mode})")

@@ -33,6 +33,43 @@ void DevBuf::release() {
     cap = 0;
 }
 
+// The correlation plan (src/smi.zig:90-158): the real planes kept (15 exact, 5 global; without
+// the fourth feature's planes when `three`) and, per correlation slot, its moving and fixed
+// plane slots and its number in the full 45-correlation order.
+CorrPlanDev corr_plan_dev(bool exact, bool three) {
+    int lst_a[45], lst_b[45], nl = 0;
+    lst_a[nl] = 0, lst_b[nl++] = 0;
+    for (int i = 0; i < 4; ++i) lst_a[nl] = 1 + i, lst_b[nl++] = 0;
+    for (int j = 0; j < 4; ++j) lst_a[nl] = 0, lst_b[nl++] = 1 + j;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) lst_a[nl] = 1 + i, lst_b[nl++] = 1 + j;
+    if (exact) {
+        for (int k = 0; k < 10; ++k) lst_a[nl] = 5 + k, lst_b[nl++] = 0;
+        for (int k = 0; k < 10; ++k) lst_a[nl] = 0, lst_b[nl++] = 5 + k;
+    }
+    const int n_planes = exact ? 15 : 5;
+    int slot[15];
+    CorrPlanDev P{};
+    for (int pl = 0; pl < n_planes; ++pl) {
+        const bool fourth = pl == 4 || pl == 8 || pl == 11 || pl == 13 || pl == 14;
+        if (three && fourth) {
+            slot[pl] = -1;
+            continue;
+        }
+        slot[pl] = P.n_real;
+        P.planes[P.n_real++] = pl;
+    }
+    for (int c = 0; c < nl; ++c) {
+        const int sa = slot[lst_a[c]], sb = slot[lst_b[c]];
+        if (sa < 0 || sb < 0) continue;
+        P.ca[P.n_corr] = sa;
+        P.cb[P.n_corr] = sb;
+        P.cnum[P.n_corr] = c;
+        P.n_corr++;
+    }
+    return P;
+}
+
 Engine::Engine(int dev) : device(dev) {
     if (const char* v = getenv("ZCMIR_B200_ROW_PASS")) row_pass = v;
     cudaSetDevice(dev);
@@ -51,7 +88,8 @@ Engine::~Engine() {
     }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
-                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_})
+                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &sw_il_[0], &sw_il_[1], &sw_poses_,
+                      &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);
@@ -257,39 +295,9 @@ bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap,
     g.ny = mp.ny;
     g.WP = ((g.nx / 2 + 1) + 7) / 8 * 8;
     job.identity_grid = (g.cw == g.W && g.ch == g.Hh);
-    // correlation plan (src/smi.zig:90-158)
     const bool three = side[0].mode == 1;
-    int lst_a[45], lst_b[45], nl = 0;
-    lst_a[nl] = 0, lst_b[nl++] = 0;
-    for (int i = 0; i < 4; ++i) lst_a[nl] = 1 + i, lst_b[nl++] = 0;
-    for (int j = 0; j < 4; ++j) lst_a[nl] = 0, lst_b[nl++] = 1 + j;
-    for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) lst_a[nl] = 1 + i, lst_b[nl++] = 1 + j;
-    if (exact) {
-        for (int k = 0; k < 10; ++k) lst_a[nl] = 5 + k, lst_b[nl++] = 0;
-        for (int k = 0; k < 10; ++k) lst_a[nl] = 0, lst_b[nl++] = 5 + k;
-    }
-    const int n_planes = exact ? 15 : 5;
-    int slot[15];
-    CorrPlanDev& P = job.plan;
-    P = CorrPlanDev{};
-    for (int pl = 0; pl < n_planes; ++pl) {
-        const bool fourth = pl == 4 || pl == 8 || pl == 11 || pl == 13 || pl == 14;
-        if (three && fourth) {
-            slot[pl] = -1;
-            continue;
-        }
-        slot[pl] = P.n_real;
-        P.planes[P.n_real++] = pl;
-    }
-    for (int c = 0; c < nl; ++c) {
-        const int sa = slot[lst_a[c]], sb = slot[lst_b[c]];
-        if (sa < 0 || sb < 0) continue;
-        P.ca[P.n_corr] = sa;
-        P.cb[P.n_corr] = sb;
-        P.cnum[P.n_corr] = c;
-        P.n_corr++;
-    }
+    job.plan = corr_plan_dev(exact, three);
+    const CorrPlanDev& P = job.plan;
     if (!line_plan(g.nx, job.row) || !line_plan(g.ny, job.col)) return false;
     job.S = row_split(g.nx, P.n_corr);
     if (job.S == 0) return fail("shift_map: row of " + std::to_string(g.nx) + " does not split to fit shared memory");

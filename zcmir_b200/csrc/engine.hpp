@@ -14,6 +14,7 @@
 #include "geom.hpp"
 #include "kernels.hpp"
 #include "settings.hpp"
+#include "sweep.hpp"
 
 namespace zc {
 
@@ -65,6 +66,39 @@ struct MapJob {
     bool identity_grid;
     bool exact, calibrated;
 };
+
+// One candidate of the sweep with its window on the sweep canvas (src/search.zig:340-366).
+struct SweepCand {
+    int it, is, ik, ia;
+    double th, s;
+    Mat3 H;
+    int gx0, gy0, nx, ny;  // first window cell, plane size
+    float taps;
+};
+
+// The sweep's batched maps reduced to peaks (src/search.zig SweepOut).
+struct SweepOut {
+    std::vector<SweepCand> cands;       // θ-major, then σ, shear, stretch
+    std::vector<SweepPeak> peaks;       // slot order (by plane size), then rank
+    std::vector<float> best;            // each candidate's top score, fixed pixels
+    std::vector<float> lane_score;      // [nc][n_peak] lane maxima per candidate, fixed pixels
+    std::vector<uint32_t> lane_idx;     // their map indices (0xffffffff: none)
+    double cell = 0, ox = 0, oy = 0;
+    int G = 0, fx0 = 0, fy0 = 0, Fx = 0, Fy = 0, n = 0;
+    unsigned min_n = 0;
+    int groups = 0, batches = 0, launches = 0;
+    float ms = 0;                       // device time of the maps (CUDA events)
+};
+
+// A pose and its score (the batched Gauss–Newton screen).
+struct ScoredPose {
+    Mat3 H;
+    double score;
+};
+
+// The correlation plan for exact (15 planes) or global (5) scores, without the fourth feature's
+// planes when `three` (src/smi.zig:90-158).
+CorrPlanDev corr_plan_dev(bool exact, bool three);
 
 // Stages of a map timed by the profiler / the benchmark entry point.
 enum Stage { kCanvas = 0, kFwdRows, kFwdCols, kInvCols, kInvRows, kNumStages };
@@ -125,6 +159,18 @@ class Engine {
     bool climb(zc_climb_result* out);
     void log_event(const std::string& text);
 
+    // the rotation × scale sweep (engine_sweep.cpp): every candidate's map reduced to n_peak
+    // peaks; batch 0 picks the batch from a memory budget
+    bool sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
+                    SweepOut& out, int batch = 0);
+    // Gauss–Newton on many poses at once (src/search.zig gnBatch)
+    bool gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
+                  std::vector<ScoredPose>& out);
+    // sweep → NMS → batched Gauss–Newton screen → finalists (src/search.zig runSweep)
+    bool search(zc_search_result* out);
+    // the sweep grid, canvas size and prior pose the settings ask for
+    void sweep_settings(SweepGrid& gv, int& G, Mat3& H0);
+
   private:
     bool build_side(int s);
     bool line_plan(int n, LinePlan& p);
@@ -134,6 +180,7 @@ class Engine {
     DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
+    DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;
     std::vector<float> pose_host_;
     std::map<int, float2*> tw_;
 };

@@ -1,0 +1,449 @@
+// The rotation × scale sweep and the search built on it, restated from the reference's
+// src/search.zig (Sweep.sweep 300-494, gnBatch 539-614, runSweep 663-820).
+//
+// Every candidate pose's translation map on a coarse G×G canvas: candidates are grouped by plane
+// size; per group the fixed window's spectra are formed once, then batches of candidates run
+// pack → forward rows → forward columns → products + inverse columns → inverse rows with the
+// per-shift score → peaks, all on the engine's stream, with only the peaks read back at the end.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "engine.hpp"
+#include "lie.hpp"
+
+namespace zc {
+
+namespace {
+
+constexpr size_t kSweepBudget = 1ull << 30;  // device bytes of one batch's work buffers
+constexpr int kSweepMaxBatch = 128;
+
+size_t pitch_of(int nx) { return (size_t)((nx / 2 + 1) + 7) / 8 * 8; }
+
+}  // namespace
+
+bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
+                        SweepOut& out, int batch) {
+    if (!need_images()) return false;
+    if (n_peak < 1 || n_peak > 16) return fail("sweep: n_peak must be 1..16");
+    if (gv.count() == 0) return fail("sweep: empty candidate grid");
+    const bool three = side[0].mode == 1;
+    const CorrPlanDev plan = corr_plan_dev(exact, three);
+    const Side &A = side[0], &B = side[1];
+    const double fw = B.w, fh = B.h, mw = A.w, mh = A.h;
+    const bool ladder = set.e("fft_sizes") != "compact";
+    out = SweepOut{};
+    // canvas: a square around the fixed image, large enough for the moving image at the largest
+    // stretch (capped at twice the fixed size)
+    const auto cm = map_pt(H0, (mw + 1) / 2, (mh + 1) / 2);
+    double s_max = -INFINITY;
+    for (double s : gv.sigmas)
+        for (double k : gv.shears)
+            for (double a : gv.anisos) s_max = std::max(s_max, sv2(cand_linear(0, s, k, a))[0]);
+    const double D = std::min(2 * std::max(fw, fh), std::max(std::max(fw, fh), s_max * std::hypot(mw, mh)));
+    const double cell = D / G, ox = (fw + 1) / 2 - D / 2, oy = (fh + 1) / 2 - D / 2;
+    const auto fcx = sweep_cells(0.5, fw + 0.5, ox, cell, G), fcy = sweep_cells(0.5, fh + 0.5, oy, cell, G);
+    const int Fx = fcx[1] - fcx[0], Fy = fcy[1] - fcy[0];
+    out.cell = cell, out.ox = ox, out.oy = oy, out.G = G, out.fx0 = fcx[0], out.fy0 = fcy[0], out.Fx = Fx, out.Fy = Fy;
+    // candidates (θ-major), their footprints, plane sizes and taps
+    const double s0r = std::sqrt(std::fabs(H0[0] * H0[4] - H0[1] * H0[3]));
+    const double s0 = (s0r == 0 || std::isnan(s0r)) ? 1 : s0r;
+    const int nc = (int)gv.count();
+    out.cands.reserve(nc);
+    for (size_t i = 0; i < gv.thetas.size(); ++i)
+        for (size_t j = 0; j < gv.sigmas.size(); ++j)
+            for (size_t ik = 0; ik < gv.shears.size(); ++ik)
+                for (size_t ia = 0; ia < gv.anisos.size(); ++ia) {
+                    const double th = gv.thetas[i], s = gv.sigmas[j];
+                    const Lin2 L = cand_linear(th, s, gv.shears[ik], gv.anisos[ia]);
+                    const Mat3 H = mul3(about_c(cm, L), H0);
+                    double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
+                    const double q[4][2] = {{0.5, 0.5}, {mw + 0.5, 0.5}, {mw + 0.5, mh + 0.5}, {0.5, mh + 0.5}};
+                    for (const auto& p : q) {
+                        const auto m = map_pt(H, p[0], p[1]);
+                        x0 = std::min(x0, m[0]), x1 = std::max(x1, m[0]);
+                        y0 = std::min(y0, m[1]), y1 = std::max(y1, m[1]);
+                    }
+                    const bool ok = std::isfinite(x0 + x1 + y0 + y1);
+                    const auto mcx = ok ? sweep_cells(x0, x1, ox, cell, G) : std::array<int, 2>{0, G};
+                    const auto mcy = ok ? sweep_cells(y0, y1, oy, cell, G) : std::array<int, 2>{0, G};
+                    SweepCand c;
+                    c.it = (int)i, c.is = (int)j, c.ik = (int)ik, c.ia = (int)ia, c.th = th, c.s = s, c.H = H;
+                    c.gx0 = mcx[0], c.gy0 = mcy[0];
+                    c.nx = (int)sweep_plane_len((unsigned)(mcx[1] - mcx[0] + Fx - 1), ladder);
+                    c.ny = (int)sweep_plane_len((unsigned)(mcy[1] - mcy[0] + Fy - 1), ladder);
+                    // box-filter taps per cell side from the candidate's smallest stretch
+                    c.taps = (float)std::min(6.0, std::max(1.0, std::ceil(cell / (sv2(L)[1] * s0) - 1e-3)));
+                    out.cands.push_back(c);
+                }
+    // slots: candidates grouped by plane size (stable)
+    std::vector<int> perm(nc);
+    for (int k = 0; k < nc; ++k) perm[k] = k;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+        const uint64_t ka = ((uint64_t)out.cands[a].nx << 32) | (uint64_t)out.cands[a].ny;
+        const uint64_t kb = ((uint64_t)out.cands[b].nx << 32) | (uint64_t)out.cands[b].ny;
+        return ka < kb;
+    });
+    std::vector<float> poses((size_t)(nc + 1) * 12, 0.f);
+    for (int k = 0; k < nc; ++k) {
+        const SweepCand& c = out.cands[perm[k]];
+        const Mat3 Hi = inv3(c.H);
+        for (int q = 0; q < 9; ++q) poses[(size_t)k * 12 + q] = (float)Hi[q];
+        poses[(size_t)k * 12 + 9] = c.taps;
+        poses[(size_t)k * 12 + 10] = (float)c.gx0;
+        poses[(size_t)k * 12 + 11] = (float)c.gy0;
+    }
+    // the fixed window's pose: identity, taps from the cell, its first cell
+    float* fp = poses.data() + (size_t)nc * 12;
+    fp[0] = fp[4] = fp[8] = 1.f;
+    fp[9] = (float)std::min(6.0, std::max(1.0, std::ceil(cell - 1e-3)));
+    fp[10] = (float)fcx[0];
+    fp[11] = (float)fcy[0];
+    // work buffers, sized once for the largest planes
+    int nx_max = 0, ny_max = 0;
+    size_t per_max = 0, fgrid = (size_t)5 * Fx * Fy;
+    auto per_item = [&](int nx, int ny) {
+        const size_t pstride = (size_t)ny * pitch_of(nx);
+        return (size_t)5 * (nx - Fx + 1) * (ny - Fy + 1) * 4 + (size_t)(plan.n_real + plan.n_corr) * pstride * 8 +
+               (size_t)nx * ny * 4;
+    };
+    for (const SweepCand& c : out.cands) {
+        nx_max = std::max(nx_max, c.nx), ny_max = std::max(ny_max, c.ny);
+        per_max = std::max(per_max, per_item(c.nx, c.ny));
+    }
+    out.n = std::max(nx_max, ny_max);
+    int bmax = batch > 0 ? batch : (int)std::max<size_t>(1, std::min<size_t>(kSweepMaxBatch, kSweepBudget / per_max));
+    if (const char* v = getenv("ZCMIR_B200_SWEEP_BATCH"))
+        if (batch <= 0 && atoi(v) > 0) bmax = atoi(v);
+    size_t grid_max = 0, half_max = 0, q_max = 0, map_max = 0, fhalf_max = 0;
+    for (const SweepCand& c : out.cands) {
+        const size_t pstride = (size_t)c.ny * pitch_of(c.nx);
+        grid_max = std::max(grid_max, (size_t)5 * (c.nx - Fx + 1) * (c.ny - Fy + 1));
+        half_max = std::max(half_max, (size_t)plan.n_real * pstride);
+        q_max = std::max(q_max, (size_t)plan.n_corr * pstride);
+        map_max = std::max(map_max, (size_t)c.nx * c.ny);
+        fhalf_max = std::max(fhalf_max, (size_t)plan.n_real * pstride);
+    }
+    const size_t na = (size_t)A.w * A.h, nb = (size_t)B.w * B.h;
+    bool ok = cuda_ok(sw_il_[0].ensure(na * 32), "sweep") && cuda_ok(sw_il_[1].ensure(nb * 32), "sweep") &&
+              cuda_ok(sw_poses_.ensure(poses.size() * 4), "sweep") && cuda_ok(sw_fgrid_.ensure(fgrid * 4), "sweep") &&
+              cuda_ok(sw_fhalf_.ensure(fhalf_max * 8), "sweep") &&
+              cuda_ok(sw_grid_.ensure(grid_max * 4 * bmax), "sweep") &&
+              cuda_ok(sw_half_.ensure(half_max * 8 * bmax), "sweep") && cuda_ok(sw_q_.ensure(q_max * 8 * bmax), "sweep") &&
+              cuda_ok(sw_map_.ensure(map_max * 4 * bmax), "sweep") && cuda_ok(sw_n0_.ensure((size_t)bmax * 8), "sweep") &&
+              cuda_ok(sw_ps_.ensure((size_t)nc * n_peak * 4), "sweep") &&
+              cuda_ok(sw_pi_.ensure((size_t)nc * n_peak * 4), "sweep");
+    if (!ok) return false;
+    if (!cuda_ok(cudaMemcpyAsync(sw_poses_.p, poses.data(), poses.size() * 4, cudaMemcpyHostToDevice, st), "sweep"))
+        return false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    auto done = [&](bool r) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return r;
+    };
+    const SweepCanvas cv{(float)ox, (float)oy, (float)cell, G};
+    const float4* ila = sw_il_[0].as<float4>();
+    const float4* ilb = sw_il_[1].as<float4>();
+    int launches = 0;
+    if (!cuda_ok(sweep_interleave(A.stack.as<float>(), (int)na, sw_il_[0].as<float4>(), st), "sweep") ||
+        !cuda_ok(sweep_interleave(B.stack.as<float>(), (int)nb, sw_il_[1].as<float4>(), st), "sweep") ||
+        !cuda_ok(sweep_pack(ilb, B.w, B.h, sw_poses_.as<float>(), nc, 1, Fx, Fy, cv, nullptr, 0, 0, 0, 0,
+                            sw_fgrid_.as<float>(), nullptr, st),
+                 "sweep"))
+        return done(false);
+    launches += 3;
+    out.min_n = (unsigned)std::max(12.0, std::floor(min_overlap * (fw * fh) / (cell * cell) + 0.5));
+    CombineParams cp{};
+    cp.exact = exact ? 1 : 0;
+    cp.calib = 0;
+    cp.nf = three ? 3 : 4;
+    cp.min_n = (float)out.min_n;
+    cp.area = 1.0;
+    cp.ridge = 1e-4;
+    for (int k0 = 0; k0 < nc;) {
+        const int nx = out.cands[perm[k0]].nx, ny = out.cands[perm[k0]].ny;
+        int k1 = k0;
+        while (k1 < nc && out.cands[perm[k1]].nx == nx && out.cands[perm[k1]].ny == ny) ++k1;
+        MapGeom gm{};
+        gm.nx = nx, gm.ny = ny, gm.WP = (int)pitch_of(nx);
+        gm.cw = nx - Fx + 1, gm.ch = ny - Fy + 1;
+        gm.W = gm.cw, gm.Hh = gm.ch;
+        MapGeom gf = gm;
+        gf.cw = Fx, gf.ch = Fy;
+        LinePlan row, col, line;
+        if (!line_plan(nx, row) || !line_plan(ny, col)) return done(false);
+        const int S = row_split(nx, plan.n_corr);
+        if (S == 0) return done(fail("sweep: a plane row of " + std::to_string(nx) + " does not fit the row pass"));
+        if (!line_plan(nx / S, line)) return done(false);
+        const float2* tw = twiddles(nx);
+        if (!tw) return done(fail("sweep: twiddles: out of device memory"));
+        cp.inv_nn = 1.0 / ((double)nx * (double)ny);
+        const size_t pstride = (size_t)ny * gm.WP;
+        const size_t wn = (size_t)gm.cw * gm.ch;
+        // the fixed window's spectra for this plane size
+        if (!cuda_ok(forward_rows(sw_fgrid_.as<float>(), gf, plan, row, sw_fhalf_.as<float2>(), st), "sweep") ||
+            !cuda_ok(forward_cols(sw_fhalf_.as<float2>(), gf, plan, col, st), "sweep"))
+            return done(false);
+        launches += 2;
+        for (int c0 = k0; c0 < k1; c0 += bmax) {
+            const int b = std::min(bmax, k1 - c0);
+            const size_t hs = (size_t)plan.n_real * pstride, qs = (size_t)plan.n_corr * pstride;
+            if (!cuda_ok(sweep_pack(ila, A.w, A.h, sw_poses_.as<float>(), c0, b, gm.cw, gm.ch, cv, sw_fgrid_.as<float>(),
+                                    fcx[0], fcy[0], Fx, Fy, sw_grid_.as<float>(), sw_n0_.as<double>(), st),
+                         "sweep") ||
+                !cuda_ok(forward_rows(sw_grid_.as<float>(), gm, plan, row, sw_half_.as<float2>(), st, b, 5 * wn, hs),
+                         "sweep") ||
+                !cuda_ok(forward_cols(sw_half_.as<float2>(), gm, plan, col, st, b), "sweep") ||
+                !cuda_ok(inverse_columns(sw_half_.as<float2>(), sw_fhalf_.as<float2>(), gm, plan, col,
+                                         sw_q_.as<float2>(), st, b, hs, 0, qs),
+                         "sweep") ||
+                !cuda_ok(inverse_rows_score(sw_q_.as<float2>(), gm, plan, line, S, tw, cp, sw_n0_.as<double>(),
+                                            sw_map_.as<float>(), nullptr, nullptr, st, b, qs, (size_t)nx * ny),
+                         "sweep") ||
+                !cuda_ok(sweep_peaks(sw_map_.as<float>(), nx, ny, (size_t)nx * ny, b, n_peak, c0, sw_ps_.as<float>(),
+                                     sw_pi_.as<uint32_t>(), st),
+                         "sweep"))
+                return done(false);
+            launches += 6;
+            out.batches++;
+        }
+        out.groups++;
+        k0 = k1;
+    }
+    cudaEventRecord(e1, st);
+    std::vector<float> ps((size_t)nc * n_peak);
+    std::vector<uint32_t> pi((size_t)nc * n_peak);
+    if (!cuda_ok(cudaMemcpyAsync(ps.data(), sw_ps_.p, ps.size() * 4, cudaMemcpyDeviceToHost, st), "sweep") ||
+        !cuda_ok(cudaMemcpyAsync(pi.data(), sw_pi_.p, pi.size() * 4, cudaMemcpyDeviceToHost, st), "sweep") ||
+        !cuda_ok(cudaStreamSynchronize(st), "sweep"))
+        return done(false);
+    cudaEventElapsedTime(&out.ms, e0, e1);
+    out.launches = launches;
+    counts[0] += launches;
+    counts[1]++;
+    counts[2] += 2;
+    counts[3]++;
+    // peaks → poses (src/search.zig:460-493): scores in fixed pixels (n counts cells)
+    const double c2 = cell * cell;
+    out.best.assign(nc, 0.f);
+    out.lane_score.assign((size_t)nc * n_peak, 0.f);
+    out.lane_idx.assign((size_t)nc * n_peak, 0xffffffffu);
+    for (int slot = 0; slot < nc; ++slot) {
+        const int ci = perm[slot];
+        const SweepCand& cd = out.cands[ci];
+        for (int k = 0; k < n_peak; ++k) {
+            const double v = (double)ps[(size_t)slot * n_peak + k] * c2;
+            const uint32_t t = pi[(size_t)slot * n_peak + k];
+            out.lane_score[(size_t)ci * n_peak + k] = (float)v;
+            out.lane_idx[(size_t)ci * n_peak + k] = t;
+            if (!(v > 0) || (uint64_t)t >= (uint64_t)cd.nx * cd.ny) continue;
+            if (k == 0) out.best[ci] = (float)v;
+            // lag (moving index − fixed index) in [−(F − 1), window − 1], then the moving
+            // image's canvas displacement gx0 + lag − fx0 cells; the correction is T(−d)
+            const int py = (int)(t / (uint32_t)cd.nx), px = (int)(t - (uint32_t)py * (uint32_t)cd.nx);
+            const int wx = cd.nx - Fx + 1, wy = cd.ny - Fy + 1;
+            const int lx = px < wx ? px : px - cd.nx, ly = py < wy ? py : py - cd.ny;
+            SweepPeak p;
+            p.score = v;
+            p.cand = ci, p.it = cd.it, p.is = cd.is, p.ik = cd.ik, p.ia = cd.ia, p.th = cd.th, p.s = cd.s;
+            p.sx = cd.gx0 + lx - fcx[0];
+            p.sy = cd.gy0 + ly - fcy[0];
+            p.H = mul3(translate(-p.sx * cell, -p.sy * cell), cd.H);
+            out.peaks.push_back(p);
+        }
+    }
+    return done(true);
+}
+
+bool Engine::gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
+                      std::vector<ScoredPose>& cur) {
+    const bool homog = set.e("group") == "homography";
+    const int nk = n_keys(homog);
+    const double rw = side[1].w, rh = side[1].h;
+    cur.clear();
+    for (const Mat3& H : Hs) cur.push_back({H, -INFINITY});
+    static const double mults[5] = {0.5, 1, 2, 4, 8};
+    auto beats = [](double nw, double old) { return nw > old + std::max(1e-6 * std::fabs(old), 1e-12); };
+    auto move = [&](const Mat3& H, const double* v, double a) {
+        Coords x{};
+        for (int k = 0; k < nk; ++k) x[k] = a * v[k];
+        return composeN(H, x, homog, rw, rh);
+    };
+    std::vector<size_t> act(Hs.size());
+    for (size_t i = 0; i < act.size(); ++i) act[i] = i;
+    struct Try {
+        size_t i;
+        Mat3 H;
+    };
+    for (unsigned it = 0; it < iters && !cancel && !act.empty(); ++it) {
+        std::vector<Mat3> hs;
+        for (size_t i : act) hs.push_back(cur[i].H);
+        std::vector<PoseEval> ev;
+        if (!eval_poses(hs, true, true, ev)) return false;
+        std::vector<Try> tries;
+        for (size_t k = 0; k < act.size(); ++k) {
+            const size_t i = act[k];
+            const PoseEval& g = ev[k];
+            cur[i].score = g.mean;
+            if (!amps.empty()) {
+                // the unit ascent direction (src/lie.zig unitAscent)
+                double d[8] = {0}, n = 0;
+                for (int q = 0; q < nk; ++q) d[q] = g.grad[q], n += d[q] * d[q];
+                n = std::sqrt(n);
+                if (n >= 1e-18)
+                    for (int q = 0; q < nk; ++q) d[q] /= n;
+                double dn = 0;
+                for (int q = 0; q < nk; ++q) dn += d[q] * d[q];
+                if (std::sqrt(dn) > 1e-12)
+                    for (double a : amps) tries.push_back({i, move(cur[i].H, d, a)});
+            }
+            double Am[64], half[8], step[8];
+            for (int q = 0; q < nk * nk; ++q) Am[q] = g.hess[q];
+            for (int q = 0; q < nk; ++q) Am[q * nk + q] += 1e-4 * std::max(Am[q * nk + q], 1e-12);
+            for (int q = 0; q < nk; ++q) half[q] = 0.5 * g.grad[q];
+            if (!solve_linear(Am, half, nk, step)) continue;
+            double nrm = 0;
+            for (int q = 0; q < nk; ++q) nrm += step[q] * step[q];
+            nrm = std::sqrt(nrm);
+            for (double m : mults) {
+                const double s = m * (nrm * m > 0.25 ? 0.25 / (nrm * m) : 1.0);
+                tries.push_back({i, move(cur[i].H, step, s)});
+            }
+        }
+        if (tries.empty()) break;
+        std::vector<Mat3> th;
+        for (const Try& t : tries) th.push_back(t.H);
+        std::vector<PoseEval> sc;
+        if (!eval_poses(th, false, false, sc)) return false;
+        std::vector<char> moved(Hs.size(), 0);
+        for (size_t k = 0; k < tries.size(); ++k)
+            if (beats(sc[k].mean, cur[tries[k].i].score)) {
+                cur[tries[k].i] = {tries[k].H, sc[k].mean};
+                moved[tries[k].i] = 1;
+            }
+        std::vector<size_t> next;
+        for (size_t i : act)
+            if (moved[i]) next.push_back(i);
+        act.swap(next);
+    }
+    return true;
+}
+
+void Engine::sweep_settings(SweepGrid& gv, int& G, Mat3& H0) {
+    auto clampf = [](double x, double lo, double hi) { return std::min(hi, std::max(lo, x)); };
+    const unsigned g = set.u("sw_grid");
+    G = (g == 32 || g == 64 || g == 128 || g == 256) ? (int)g : 128;
+    const double rot_deg = clampf(set.f("sw_rot"), 0, 180);
+    // a range wider than the circle is the circle; hi < lo runs through ±180° (170 → −170)
+    const bool range = set.b("sw_rot_range");
+    const double rot_lo = range ? clampf(set.f("sw_rot_lo"), -360, 360) : -rot_deg;
+    double rot_hi = range ? clampf(set.f("sw_rot_hi"), -360, 360) : rot_deg;
+    if (rot_hi < rot_lo) rot_hi += 360;
+    rot_hi = std::min(rot_hi, rot_lo + 360);
+    SweepGridOpts o;
+    o.rot_lo = rot_lo, o.rot_hi = rot_hi;
+    o.n_theta = std::clamp(set.u("sw_nth"), 1u, 720u);
+    o.s_min = clampf(set.f("sw_smin"), 0.05, 1);
+    o.s_max = clampf(set.f("sw_smax"), 1, 20);
+    o.n_sigma = std::clamp(set.u("sw_ns"), 1u, 129u);
+    o.shear_max = set.b("sw_shear") ? clampf(set.f("sw_shear_max"), 0, 1) : 0;
+    o.n_shear = std::clamp(set.u("sw_nshear"), 1u, 15u);
+    o.aniso_max = set.b("sw_aniso") ? clampf(set.f("sw_aniso_max"), 0, 1) : 0;
+    o.n_aniso = std::clamp(set.u("sw_naniso"), 1u, 15u);
+    gv = sweep_grid(o);
+    const double lw = side[0].w, lh = side[0].h, rw = side[1].w, rh = side[1].h;
+    H0 = set.b("sw_rel") ? H : translate((rw - lw) / 2, (rh - lh) / 2);
+}
+
+bool Engine::search(zc_search_result* out) {
+    if (!need_images()) return false;
+    if (set.e("search_mode") != "sweep")
+        return fail("search: search_mode \"" + set.e("search_mode") + "\" is not part of this build (search_mode=\"sweep\" is)");
+    if (set.e("metric") != "smi")
+        return fail("search: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    cancel = false;
+    if (set.b("ffd")) log_event("the spline stage is not part of this build; searching the homography only");
+    SweepGrid gv;
+    int G;
+    Mat3 H0;
+    sweep_settings(gv, G, H0);
+    const unsigned kk = set.u("sw_k");
+    const unsigned K = (kk == 8 || kk == 16 || kk == 32) ? kk : 32;
+    const unsigned n_fin = std::clamp(set.u("sw_fin"), 1u, 16u);
+    const double min_ov = std::min(0.5, std::max(0.0, set.f("min_overlap")));
+    const Mat3 Hcur = H;
+    const double c_mov[2] = {(side[0].w + 1) / 2.0, (side[0].h + 1) / 2.0};
+    std::vector<PoseEval> e0;
+    if (!eval_poses({Hcur}, false, false, e0)) return false;
+    const double s_cur = e0[0].mean;
+    const bool exact = set.b("exact");
+    SweepOut res;
+    if (!sweep_maps(H0, gv, G, exact, 4, min_ov, res)) return false;
+    const std::vector<SweepPeak> top = nms4(res.peaks, (unsigned)gv.thetas.size(), K, gv.wrap);
+    char buf[320];
+    snprintf(buf, sizeof buf, "search  %zuθ × %zuσ%s  %d maps  %d² grid (%.1f px, FFT ≤ %d²)  %s  %zu peaks  (%.2f ms)",
+             gv.thetas.size(), gv.sigmas.size(), gv.shears.size() * gv.anisos.size() > 1 ? " × shear × stretch" : "",
+             (int)res.cands.size(), G, res.cell, res.n, exact ? "exact" : "global", top.size(), res.ms);
+    log_event(buf);
+    zc_search_result r{};
+    std::memcpy(r.H, Hcur.data(), sizeof r.H);
+    r.score = s_cur;
+    r.prev = s_cur;
+    r.count_a = (uint32_t)top.size();
+    if (top.empty()) {
+        log_event("search  no peak above the overlap floor");
+        *out = r;
+        return true;
+    }
+    const std::vector<double> amps =
+        geo_amps(set.f("g_a0"), set.f("g_decay"), set.u("g_steps") > 0 ? set.u("g_steps") : 7);
+    std::vector<Mat3> starts;
+    for (const SweepPeak& p : top) starts.push_back(p.H);
+    std::vector<ScoredPose> screened;
+    if (!gn_batch(starts, 4, amps, screened)) return false;
+    // finalists: the best after the short climb, plus the best coarse peaks
+    std::vector<size_t> order(screened.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return screened[a].score > screened[b].score; });
+    std::vector<size_t> fin;
+    for (size_t k = 0; k < std::min<size_t>(n_fin, order.size()); ++k)
+        if (std::find(fin.begin(), fin.end(), order[k]) == fin.end()) fin.push_back(order[k]);
+    for (size_t i = 0; i < std::min<size_t>(n_fin, top.size()); ++i)
+        if (std::find(fin.begin(), fin.end(), i) == fin.end()) fin.push_back(i);
+    std::vector<Mat3> fin_h;
+    for (size_t i : fin) fin_h.push_back(screened[i].H);
+    std::vector<ScoredPose> finals;
+    if (!gn_batch(fin_h, 25, amps, finals)) return false;
+    size_t bi = 0;
+    for (size_t i = 0; i < finals.size(); ++i)
+        if (finals[i].score > finals[bi].score) bi = i;
+    const ScoredPose best = finals[bi];
+    const auto rs = sim_of(best.H, H0, c_mov[0], c_mov[1]);
+    snprintf(buf, sizeof buf, "search  screen %zu × 4 steps, climb %zu × ≤25 Gauss–Newton  best nS %.1f", top.size(),
+             finals.size(), best.score);
+    log_event(buf);
+    r.count_b = (uint32_t)finals.size();
+    auto beats = [](double nw, double old) { return nw > old + std::max(1e-6 * std::fabs(old), 1e-12); };
+    if (beats(best.score, s_cur)) {
+        H = best.H;
+        std::memcpy(r.H, best.H.data(), sizeof r.H);
+        r.score = best.score;
+        r.improved = 1;
+        snprintf(buf, sizeof buf, "search done  nS %.1f (was %.1f)  θ %.1f° σ %.3f", best.score, s_cur,
+                 rs[0] * 180 / M_PI, rs[1]);
+    } else {
+        snprintf(buf, sizeof buf, "search done  kept the current pose (nS %.1f ≥ %.1f)", s_cur, best.score);
+    }
+    log_event(buf);
+    *out = r;
+    return true;
+}
+
+}  // namespace zc

@@ -202,7 +202,9 @@ void zc_get_pose(zc_engine* e, double H[9]) {
 int32_t zc_climb(zc_engine* e, zc_climb_result* out) {
     return guarded(e, "climb", [&] { return e->climb(out); });
 }
-int32_t zc_search(zc_engine* e, zc_search_result*) { return unsupported(e, "search"); }
+int32_t zc_search(zc_engine* e, zc_search_result* out) {
+    return guarded(e, "search", [&] { return e->search(out); });
+}
 
 void zc_cancel(zc_engine* e) {
     if (e) e->cancel = true;
@@ -361,6 +363,32 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
     if (out_len) *out_len = j.size();
     if (err_len) *err_len = 0;
     return 0;
+}
+
+int32_t zcb_sweep(zc_engine* e, const double H0p[9], uint32_t n_peak, uint32_t batch, float* scores, uint32_t* idx,
+                  size_t cap, double* info, size_t info_len) {
+    return guarded(e, "sweep", [&] {
+        if (info_len < 16 || !info) return e->fail("sweep: info needs 16 entries");
+        zc::SweepGrid gv;
+        int G;
+        zc::Mat3 Hd;
+        e->sweep_settings(gv, G, Hd);
+        const zc::Mat3 H0 = H0p ? mat(H0p) : Hd;
+        const double min_ov = std::min(0.5, std::max(0.0, e->set.f("min_overlap")));
+        zc::SweepOut r;
+        if (!e->sweep_maps(H0, gv, G, e->set.b("exact"), (int)n_peak, min_ov, r, (int)batch)) return false;
+        const size_t n = r.lane_score.size();
+        if (scores && idx) {
+            if (cap < n) return e->fail("sweep: BufferTooSmall");
+            std::copy(r.lane_score.begin(), r.lane_score.end(), scores);
+            std::copy(r.lane_idx.begin(), r.lane_idx.end(), idx);
+        }
+        const double v[16] = {(double)r.cands.size(), r.cell, (double)r.ms, (double)r.G, (double)r.Fx, (double)r.Fy,
+                              (double)r.fx0, (double)r.fy0, (double)r.min_n, (double)r.n, (double)r.groups,
+                              (double)r.batches, (double)r.launches, r.ox, r.oy, (double)r.peaks.size()};
+        std::copy(v, v + 16, info);
+        return true;
+    });
 }
 
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out) {

@@ -62,20 +62,26 @@ cudaError_t resample_grid(const float* canvas, int W, int Hh, int cw, int ch, fl
 // Σ grid_a[0]·grid_b[0] (float64) into *out: the overlap count at lag 0
 cudaError_t lag0_count(const float* grid_a, const float* grid_b, int cw, int ch, double* out, cudaStream_t st);
 
+// The transforms below run `batch` independent items at once (a sweep's candidates), item b at
+// the given strides (in elements) from the first; batch 1 is one map.
+
 // forward transforms of one side: real planes of the grid → row R2C (rows < ch) into the half
-// spectra [n_real][ny][WP] complex; then the column FFTs of the half spectra in place
+// spectra [n_real][ny][WP] complex; then the column FFTs of the half spectra in place (the
+// batch's half spectra contiguous: half_stride = n_real·ny·WP)
 cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& row,
-                         float2* half, cudaStream_t st);
+                         float2* half, cudaStream_t st, int batch = 1, size_t grid_stride = 0, size_t half_stride = 0);
 cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
-                         cudaStream_t st);
-// products and inverse column FFTs: Q[slot][ny][WP]
+                         cudaStream_t st, int batch = 1);
+// products and inverse column FFTs: Q[slot][ny][WP] (b_stride 0: one fixed side for every item)
 cudaError_t inverse_columns(const float2* half_a, const float2* half_b, const MapGeom& g, const CorrPlanDev& plan,
-                            const LinePlan& col, float2* Q, cudaStream_t st);
+                            const LinePlan& col, float2* Q, cudaStream_t st, int batch = 1, size_t a_stride = 0,
+                            size_t b_stride = 0, size_t q_stride = 0);
 // inverse row FFTs fused with the per-shift score and the argmax: map (ny × nx f32), best key
-// (u64), zero-lag score
+// (u64), zero-lag score (best and zero may be null); n00: one zero-lag overlap per item
 cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
                                int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
-                               unsigned long long* best, float* zero, cudaStream_t st);
+                               unsigned long long* best, float* zero, cudaStream_t st, int batch = 1,
+                               size_t q_stride = 0, size_t map_stride = 0);
 // the same pass with the sums in tensor memory: a whole row per block (nx ∈ {512, 1024, 2048})
 bool rows_tmem_supported(int nx, int n_corr);
 cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const float2* tw_nx,
@@ -85,6 +91,24 @@ cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const Cor
 // when none fits
 int row_split(int nx, int n_corr);
 size_t row_pass_smem(int L, int n_corr, int tl);
+
+// ── the rotation × scale sweep (sweep.cu) ──
+// The sweep's G×G canvas of cells: cell (cx, cy) spans dest pixels [ox + cx·cell, …) (1-based).
+struct SweepCanvas {
+    float ox, oy, cell;
+    int G;
+};
+// plane-major 5-plane stack of n pixels → 8 floats per pixel (w, w f0..w f3, 0, 0, 0)
+cudaError_t sweep_interleave(const float* stack, int n, float4* il, cudaStream_t st);
+// the windows [batch][5][win_y][win_x] of slots slot0.. (poses: 12 floats per slot: dest →
+// source map, taps, first window cell); with fw (the fixed window's weights, [Fy][Fx] at cell
+// (fx0, fy0)) each item's zero-lag overlap into n0[batch] (cleared here)
+cudaError_t sweep_pack(const float4* il, int sw, int sh, const float* poses, int slot0, int batch, int win_x,
+                       int win_y, const SweepCanvas& cv, const float* fw, int fx0, int fy0, int Fx, int Fy, float* grid,
+                       double* n0, cudaStream_t st);
+// the n_peak best lane maxima of each map (map b at maps + b·map_stride) into slots slot0..
+cudaError_t sweep_peaks(const float* maps, int nx, int ny, size_t map_stride, int batch, int n_peak, int slot0,
+                        float* ps, uint32_t* pi, cudaStream_t st);
 
 // ── pose scores and gradients (pose.cu) ──
 struct PoseSide {

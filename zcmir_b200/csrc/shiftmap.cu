@@ -139,13 +139,16 @@ __device__ __forceinline__ float real_plane_row(int r, const float* row, int cw,
 
 // One block per grid row y < ch; lines = packed plane pairs (2z, 2z+1), lpb of them at a time.
 // The row's 5 stack values per cell are staged in shared memory once (after the line buffers).
+// Batched over blockIdx.y: item b reads grid + b·gbs and writes half + b·hbs.
 template <class F>
 __global__ void __launch_bounds__(256, 2) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int WP,
                                                      CorrPlanDev plan, F f, int lpb, float2* __restrict__ half,
-                                                     size_t pstride) {
+                                                     size_t pstride, size_t gbs, size_t hbs) {
     extern __shared__ float2 smem[];
     const int nx = f.n(), tl = f.tl();
     const int y = blockIdx.x;
+    grid += (size_t)blockIdx.y * gbs;
+    half += (size_t)blockIdx.y * hbs;
     const int line = threadIdx.x / tl;
     const int t = threadIdx.x - line * tl;
     const int pl = padded_len(nx);
@@ -228,17 +231,19 @@ __global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size
 
 // ── inverse: products and column IFFTs ──────────────────────────────────────────────────────
 
-// block (correlation slot k, column tile): P = A·conj(B) on the tile, inverse column FFT → Q
+// block (correlation slot k, column tile, item): P = A·conj(B) on the tile, inverse column FFT
+// → Q; item b reads ha + b·abs, hb + b·bbs and writes Q + b·qbs
 template <class F>
 __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ ha, const float2* __restrict__ hb,
                                                      size_t pstride, int WP, int ncols, CorrPlanDev plan, F f, int tx,
-                                                     float2* __restrict__ Q) {
+                                                     float2* __restrict__ Q, size_t abs_, size_t bbs, size_t qbs) {
     extern __shared__ float2 smem[];
     const int k = blockIdx.x;
     const int x0 = blockIdx.y * tx;
-    const float2* A = ha + (size_t)plan.ca[k] * pstride;
-    const float2* B = hb + (size_t)plan.cb[k] * pstride;
-    float2* O = Q + (size_t)k * pstride;
+    const size_t item = blockIdx.z;
+    const float2* A = ha + item * abs_ + (size_t)plan.ca[k] * pstride;
+    const float2* B = hb + item * bbs + (size_t)plan.cb[k] * pstride;
+    float2* O = Q + item * qbs + (size_t)k * pstride;
     const int ny = f.n(), pl = line_pitch(ny), tl = f.tl();
     const int total = tx * ny;
     for (int e0 = 0; e0 < total; e0 += 4 * blockDim.x) {
@@ -270,17 +275,21 @@ __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ 
 
 // ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
 
-// block (row y, split s): every correlation pair's row (Hermitian full row from the half
+// block (row y, split s, item): every correlation pair's row (Hermitian full row from the half
 // spectrum) pre-combined for outputs x ≡ s (mod S), inverse FFT of length L = nx/S, the sums
 // kept in shared memory; then the score of each of the row's L shifts and the block argmax.
+// Item b reads Q + b·qbs and n00p[b], writes map + b·mbs; best and zero_out may be null.
 template <class F, int NF, bool EXACT, bool CALIB, int SS>
 __global__ void __launch_bounds__(512, 1) k_inv_rows(const float2* __restrict__ Q, size_t pstride, int WP, int nx, int S,
                                                      CorrPlanDev plan, F f, int lpb, const float2* __restrict__ tw_nx,
                                                      CombineParams cp, const double* __restrict__ n00p,
                                                      float* __restrict__ map, unsigned long long* best,
-                                                     float* zero_out) {
+                                                     float* zero_out, size_t qbs, size_t mbs) {
     extern __shared__ float2 smem[];
     const int y = blockIdx.x / S, s = blockIdx.x - (blockIdx.x / S) * S;
+    Q += (size_t)blockIdx.y * qbs;
+    map += (size_t)blockIdx.y * mbs;
+    n00p += blockIdx.y;
     const int L = f.n(), pl = padded_len(L), tl = f.tl();
     float* corr = reinterpret_cast<float*>(smem + lpb * pl);  // [n_corr][L]
     const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
@@ -364,8 +373,9 @@ __global__ void __launch_bounds__(512, 1) k_inv_rows(const float2* __restrict__ 
             bv = sc;
             bi = idx;
         }
-        if (idx == 0) *zero_out = sc;
+        if (idx == 0 && zero_out) *zero_out = sc;
     }
+    if (!best) return;
     unsigned long long key = (bi == 0xffffffffu) ? 0ull : argmax_key(bv, bi);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -437,7 +447,7 @@ static int line_threads(const LinePlan& p) {
 }
 
 cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& row,
-                         float2* half, cudaStream_t st) {
+                         float2* half, cudaStream_t st, int batch, size_t grid_stride, size_t half_stride) {
     const size_t pstride = (size_t)g.ny * g.WP;
     const int tl = line_threads(row);
     const int n_cplx = (plan.n_real + 1) / 2;
@@ -446,7 +456,8 @@ cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev&
     const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)5 * g.cw * sizeof(float);
     return with_line(row, [&](auto f) {
         cudaFuncSetAttribute(k_fwd_rows<decltype(f)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_fwd_rows<<<g.ch, lines * tl, sm, st>>>(grid, g.cw, g.ch, g.WP, plan, f, lines, half, pstride);
+        k_fwd_rows<<<dim3(g.ch, batch), lines * tl, sm, st>>>(grid, g.cw, g.ch, g.WP, plan, f, lines, half, pstride,
+                                                              grid_stride, half_stride);
         return cudaGetLastError();
     });
 }
@@ -458,12 +469,12 @@ static int col_tile(const LinePlan& col) {
 }
 
 cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
-                         cudaStream_t st) {
+                         cudaStream_t st, int batch) {
     const size_t pstride = (size_t)g.ny * g.WP;
     const int ncols = g.nx / 2 + 1;
     const int tx = col_tile(col), tl = line_threads(col);
     const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
-    dim3 gc((ncols + tx - 1) / tx, plan.n_real);
+    dim3 gc((ncols + tx - 1) / tx, plan.n_real * batch);
     return with_line(col, [&](auto f) {
         cudaFuncSetAttribute(k_cols<decltype(f), false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_cols<decltype(f), false><<<gc, tx * tl, sm, st>>>(half, pstride, g.WP, ncols, g.ch, f, tx);
@@ -472,15 +483,16 @@ cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan
 }
 
 cudaError_t inverse_columns(const float2* ha, const float2* hb, const MapGeom& g, const CorrPlanDev& plan,
-                            const LinePlan& col, float2* Q, cudaStream_t st) {
+                            const LinePlan& col, float2* Q, cudaStream_t st, int batch, size_t a_stride,
+                            size_t b_stride, size_t q_stride) {
     const size_t pstride = (size_t)g.ny * g.WP;
     const int ncols = g.nx / 2 + 1;
     const int tx = col_tile(col), tl = line_threads(col);
     const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
-    dim3 gc(plan.n_corr, (ncols + tx - 1) / tx);
+    dim3 gc(plan.n_corr, (ncols + tx - 1) / tx, batch);
     return with_line(col, [&](auto f) {
         cudaFuncSetAttribute(k_inv_cols<decltype(f)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_inv_cols<<<gc, tx * tl, sm, st>>>(ha, hb, pstride, g.WP, ncols, plan, f, tx, Q);
+        k_inv_cols<<<gc, tx * tl, sm, st>>>(ha, hb, pstride, g.WP, ncols, plan, f, tx, Q, a_stride, b_stride, q_stride);
         return cudaGetLastError();
     });
 }
@@ -524,20 +536,29 @@ int row_split(int nx, int n_corr) {
     return 0;
 }
 
+struct RowBatch {
+    int n;
+    size_t q, m;
+};
+
 template <class F, int NF, bool EXACT, bool CALIB>
 static cudaError_t launch_rows(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, F f, int S,
                                const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
-                               unsigned long long* best, float* zero, int lpb, size_t sm, cudaStream_t st) {
+                               unsigned long long* best, float* zero, int lpb, size_t sm, cudaStream_t st,
+                               const RowBatch& rb) {
     auto k = S == 1 ? k_inv_rows<F, NF, EXACT, CALIB, 1> : S == 2 ? k_inv_rows<F, NF, EXACT, CALIB, 2>
                                                                  : k_inv_rows<F, NF, EXACT, CALIB, 0>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k<<<g.ny * S, 512, sm, st>>>(Q, (size_t)g.ny * g.WP, g.WP, g.nx, S, plan, f, lpb, tw_nx, cp, n00, map, best, zero);
+    k<<<dim3(g.ny * S, rb.n), 512, sm, st>>>(Q, (size_t)g.ny * g.WP, g.WP, g.nx, S, plan, f, lpb, tw_nx, cp, n00, map,
+                                             best, zero, rb.q, rb.m);
     return cudaGetLastError();
 }
 
 cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,
                                int S, const float2* tw_nx, const CombineParams& cp, const double* n00, float* map,
-                               unsigned long long* best, float* zero, cudaStream_t st) {
+                               unsigned long long* best, float* zero, cudaStream_t st, int batch, size_t q_stride,
+                               size_t map_stride) {
+    const RowBatch rb{batch, q_stride, map_stride};
     const int tl = row_threads(line);
     const int lpb = row_lines(tl);
     if (lpb * tl > 512) return cudaErrorInvalidConfiguration;
@@ -545,13 +566,13 @@ cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlan
     return with_row_line(line, [&](auto f) {
         using Fp = decltype(f);
         if (cp.nf == 4) {
-            if (!cp.exact) return launch_rows<Fp, 4, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
-            if (cp.calib) return launch_rows<Fp, 4, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
-            return launch_rows<Fp, 4, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+            if (!cp.exact) return launch_rows<Fp, 4, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
+            if (cp.calib) return launch_rows<Fp, 4, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
+            return launch_rows<Fp, 4, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
         }
-        if (!cp.exact) return launch_rows<Fp, 3, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
-        if (cp.calib) return launch_rows<Fp, 3, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
-        return launch_rows<Fp, 3, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st);
+        if (!cp.exact) return launch_rows<Fp, 3, false, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
+        if (cp.calib) return launch_rows<Fp, 3, true, true>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
+        return launch_rows<Fp, 3, true, false>(Q, g, plan, f, S, tw_nx, cp, n00, map, best, zero, lpb, sm, st, rb);
     });
 }
 

@@ -7,6 +7,9 @@
 * ``pair_segmented`` (1024² map workload): modality A = a blob field (uint16 range); modality
   B = an 8-level piecewise-constant segmentation of it with a random level → intensity
   permutation plus N(0, 0.03²), shifted by a random integer shift in ±200 px.
+* ``pair_similarity`` (512² sweep workload): the same two modalities with the moving image under
+  a random similarity about the image centre: rotation in [0°, 360°), scale log-uniform in
+  [0.8, 1.25], shift in ±n/8 px.
 
 The true pose maps moving → fixed (1-based pixels): H = translate(dx, dy), i.e. the moving pixel
 x shows the fixed content at x + (dx, dy). The shift map at the identity pose then peaks at the
@@ -68,4 +71,39 @@ def pair_segmented(n=1024, seed=1, max_shift=200, levels=8, noise=0.03, shift=No
     moving = perm[lab] / (levels - 1.0) + noise * rng.standard_normal((n, n))
     to16 = lambda a: (np.clip(a, 0, 1) * 65535 + 0.5).astype(np.uint16)
     H = np.array([[1, 0, dx], [0, 1, dy], [0, 0, 1.0]])
+    return to16(moving), to16(fixed), H
+
+
+def similarity(n, deg, scale, tx, ty):
+    """Moving → fixed (1-based): rotate by deg and scale about the centre, then shift."""
+    c = (n + 1) / 2
+    th = np.deg2rad(deg)
+    R = np.array([[scale * np.cos(th), -scale * np.sin(th), 0], [scale * np.sin(th), scale * np.cos(th), 0], [0, 0, 1.0]])
+    T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
+    return T(c + tx, c + ty) @ R @ T(-c, -c)
+
+
+def pair_similarity(n=512, seed=2, deg=None, scale=None, shift=None, levels=8, noise=0.03):
+    """(moving, fixed, H_true) uint16: fixed = blob field (modality A); moving(x) = the segmented
+    modality B of the field at H·x, for a random similarity H (unless given)."""
+    from scipy.ndimage import map_coordinates
+
+    rng = np.random.default_rng(seed)
+    deg = float(rng.uniform(0, 360)) if deg is None else float(deg)
+    scale = float(np.exp(rng.uniform(np.log(0.8), np.log(1.25)))) if scale is None else float(scale)
+    if shift is None:
+        shift = tuple(float(v) for v in rng.integers(-(n // 8), n // 8 + 1, size=2))
+    H = similarity(n, deg, scale, *shift)
+    pad = n
+    big = blob_field(n + 2 * pad, n + 2 * pad, rng, n_blobs=64)
+    fixed = big[pad:pad + n, pad:pad + n]
+    yy, xx = np.mgrid[0:n, 0:n].astype(np.float64)
+    X = np.stack([xx + 1, yy + 1, np.ones_like(xx)], -1) @ H.T
+    fx, fy = X[..., 0] / X[..., 2] - 1 + pad, X[..., 1] / X[..., 2] - 1 + pad
+    src = map_coordinates(big, [fy, fx], order=1, mode="nearest")
+    edges = np.quantile(src, np.linspace(0, 1, levels + 1)[1:-1])
+    lab = np.digitize(src, edges)
+    perm = rng.permutation(levels)
+    moving = perm[lab] / (levels - 1.0) + noise * rng.standard_normal((n, n))
+    to16 = lambda a: (np.clip(a, 0, 1) * 65535 + 0.5).astype(np.uint16)
     return to16(moving), to16(fixed), H
