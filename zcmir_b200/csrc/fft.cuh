@@ -188,22 +188,28 @@ __device__ __forceinline__ void line_fft(float2* __restrict__ buf, const LinePla
     }
 }
 
-// ── power-of-two lines with the whole schedule known at compile time ──
-// N = 2^a points, N/16 threads per line (one radix-16 butterfly, or 16/R of radix R, per thread
-// per stage), ⌈a/4⌉ stages with balanced radices; strides, twiddle steps and index arithmetic
-// fold to constants.
+// ── lines of N = 2^a·3^b points with the whole schedule known at compile time ──
+// ⌈a/4⌉ power-of-two stages with balanced radices (16/8/4/2), then b radix-3 stages; TL threads
+// per line, each taking ⌈(N/R)/TL⌉ butterflies of a radix-R stage. Strides, twiddle steps and
+// index arithmetic fold to constants.
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+constexpr int twos_of(int n) { return (n > 0 && n % 2 == 0) ? 1 + twos_of(n / 2) : 0; }
+constexpr int threes_of(int n) { return (n > 0 && n % 3 == 0) ? 1 + threes_of(n / 3) : 0; }
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 
 template <int N>
-struct Pow2 {
-    static constexpr int kLog = ilog2(N);
-    static constexpr int kStages = (kLog + 3) / 4;
-    static constexpr int kThreads = N / 16;
-    static constexpr int bits(int s) { return kLog / kStages + (s < kLog % kStages ? 1 : 0); }
+struct Mix {
+    static constexpr int kA = twos_of(N), kB = threes_of(N);
+    static_assert(ipow(2, twos_of(N)) * ipow(3, threes_of(N)) == N, "line length must be 2^a·3^b");
+    static constexpr int kP2 = (kA + 3) / 4;
+    static constexpr int kStages = kP2 + kB;
+    static constexpr int radix(int s) {
+        return s < kP2 ? 1 << (kA / kP2 + (s < kA % kP2 ? 1 : 0)) : 3;
+    }
 };
 
 template <int R, int NS, int N, int TL, bool INV>
-__device__ __forceinline__ void p2_stage(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
+__device__ __forceinline__ void mix_stage(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
     constexpr int M = N / R, BM = (M + TL - 1) / TL, TWS = N / (NS * R);
     float2 v[BM][R];
     if (act) {
@@ -222,7 +228,7 @@ __device__ __forceinline__ void p2_stage(float2* __restrict__ buf, const float2*
         for (int b = 0; b < BM; ++b) {
             const int j = t + b * TL;
             if (M % TL == 0 || j < M) {
-                const int k = j & (NS - 1);
+                const int k = j % NS;
                 if (NS > 1) {
 #pragma unroll
                     for (int r = 1; r < R; ++r) {
@@ -242,36 +248,40 @@ __device__ __forceinline__ void p2_stage(float2* __restrict__ buf, const float2*
 }
 
 template <int N, int TL, bool INV, int S = 0, int NS = 1>
-__device__ __forceinline__ void p2_fft(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
-    if constexpr (S < Pow2<N>::kStages) {
-        constexpr int R = 1 << Pow2<N>::bits(S);
-        p2_stage<R, NS, N, TL, INV>(buf, tw, t, act);
-        p2_fft<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
+__device__ __forceinline__ void mix_fft(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
+    if constexpr (S < Mix<N>::kStages) {
+        constexpr int R = Mix<N>::radix(S);
+        mix_stage<R, NS, N, TL, INV>(buf, tw, t, act);
+        mix_fft<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
     }
 }
 
 // Line-FFT policies the map kernels are written against: n(), threads per line, run<INV>().
 struct GenericLine {
     LinePlan p;
-    __device__ __forceinline__ int n() const { return p.n; }
-    __device__ __forceinline__ int tl() const { return p.tl; }
+    __host__ __device__ __forceinline__ int n() const { return p.n; }
+    __host__ __device__ __forceinline__ int tl() const { return p.tl; }
     template <bool INV>
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
         line_fft<INV>(buf, p, act ? t : (1 << 30));
     }
 };
 
-// TPL: threads per line (N/16 by default: one radix-16 butterfly each; N/8 gives every thread
-// 8 points of the loads and stores around the transform, half of them idle in radix-16 stages)
+// A compile-time line of N = 2^a·3^b points. TPL: threads per line (N/16 by default: one
+// radix-16 butterfly each; N/8 gives every thread 8 points of the loads and stores around the
+// transform, half of them idle in radix-16 stages)
 template <int N, int TPL = N / 16>
-struct Pow2Line {
+struct FixedLine {
     const float2* tw;
-    __device__ __forceinline__ static constexpr int n() { return N; }
-    __device__ __forceinline__ static constexpr int tl() { return TPL; }
+    __host__ __device__ __forceinline__ static constexpr int n() { return N; }
+    __host__ __device__ __forceinline__ static constexpr int tl() { return TPL; }
     template <bool INV>
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
-        p2_fft<N, TPL, INV>(buf, tw, t, act && t < TPL);
+        mix_fft<N, TPL, INV>(buf, tw, t, act && t < TPL);
     }
 };
+
+template <int N, int TPL = N / 16>
+using Pow2Line = FixedLine<N, TPL>;
 
 }  // namespace zc
