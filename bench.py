@@ -13,6 +13,11 @@ The path does not shard (one map needs all 45 correlations of every shift): N GP
 independent replicas, one process each (torchrun), and `value` is the maps/s of all ranks, timed
 as the slowest rank.
 
+The line also carries `sweep`: the rotation × scale sweep of a 512² pair (360 rotations × 9
+scales = 3240 candidate maps on a 128² canvas) as poses/s (candidate maps per second, device
+time of the batched maps), its `e2e` (set_images + search from host images: sweep, NMS, batched
+Gauss–Newton screen and finalists, as searches/s) and a CPU baseline on a sample of 90 candidates.
+
 --impl reference: the CPU restatement of the reference's path (the oracle, float64, scipy FFTs on
 all host cores) on the same pair; rank 0 only.
 """
@@ -52,21 +57,44 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def smi_id(local):
+    """nvidia-smi's name for CUDA device `local` (its UUID; the CUDA index can differ from
+    nvidia-smi's when CUDA_VISIBLE_DEVICES is set)."""
+    try:
+        import torch
+
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        return ids[local] if local < len(ids) else str(local)
+
+
 class Clocks:
     """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index, self.lines, self.p = index, [], None
+    def __init__(self, local, interval_ms=20):
+        self.index, self.interval, self.lines, self.p, self.first = smi_id(local), interval_ms, [], None, 0
+
+    def _read(self):
+        for ln in self.p.stdout:
+            self.lines.append(ln)
 
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=lambda: self.lines.extend(self.p.stdout), daemon=True)
+                                       "-lms", str(self.interval)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler runs; earlier samples are not counted
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10 and self.p.poll() is None:
+                time.sleep(0.005)
+            self.first = len(self.lines)
         except OSError:
             self.p = None
         return self
@@ -80,7 +108,7 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        for ln in self.lines[self.first:]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 6:
                 continue
@@ -102,7 +130,7 @@ def stage_bytes(p):
     nx, ny, cw, ch, P, C = p["nx"], p["ny"], p["cw"], p["ch"], p["n_real"], p["n_corr"]
     half = (nx // 2 + 1) * 8
     return {
-        "canvas": 2 * (5 * 1024 * 1024 * 4) * 2,
+        "canvas": 2 * (5 * p["canvas_w"] * p["canvas_h"] * 4) * 2,
         "fwd_rows": 2 * (5 * cw * ch * 4 + P * ch * half),
         "fwd_cols": 2 * (P * ch * half + P * ny * half),
         "inv_cols": 2 * P * ny * half + C * ny * half,
@@ -114,7 +142,7 @@ def survey_bytes(p):
     """The whole map's compulsory HBM bytes (both stacks read, both sides' half spectra written and
     read once, the map written)."""
     nx, ny, P = p["nx"], p["ny"], p["n_real"]
-    return 2 * 5 * 1024 * 1024 * 4 + 2 * (2 * P * nx * (ny // 2 + 1) * 8) + nx * ny * 4
+    return 2 * 5 * p["canvas_w"] * p["canvas_h"] * 4 + 2 * (2 * P * nx * (ny // 2 + 1) * 8) + nx * ny * 4
 
 
 def cpu_map_seconds(m, f):
@@ -147,6 +175,81 @@ def make_pair():
 
     m, f, H = synth.pair_segmented(n=1024, seed=1)
     return (m / 65535.0).astype(np.float32), (f / 65535.0).astype(np.float32), H
+
+
+SWEEP_SETTINGS = dict(half=False, sw_nth=360, sw_ns=9, sw_smin=0.8, sw_smax=1.25, sw_grid=128)
+SWEEP_CONFIG = {"workload": "smi_sweep_512_rot360x9_grid128", "image": [512, 512], "candidates": 3240,
+                "rotations": "0-359 deg, 1 deg steps", "scales": "9 log-spaced in [0.8, 1.25]", "grid": 128,
+                "pair": "blob field vs 8-level segmented modality under a seeded similarity (seed 2)",
+                "l2": "per-sweep working set ~1.3 GB per batch of candidates > 126 MB L2"}
+
+
+def sweep_cpu_sample(m, f, n_sample=90):
+    """Poses/s of the float64 oracle on an evenly spaced sample of the sweep's candidates."""
+    from oracle import smi_oracle as O
+    from oracle import sweep_oracle as S
+
+    pa, pb = O.prepare(m), O.prepare(f)
+    gv = S.sweep_grid(n_theta=360, n_sigma=9, s_min=0.8, s_max=1.25)
+    nc = 360 * 9
+    only = set(range(0, nc, nc // n_sample))
+    t0 = time.perf_counter()
+    S.sweep(pa, pb, np.eye(3), gv, G=128, exact=True, only=only)
+    return len(only) / (time.perf_counter() - t0), len(only)
+
+
+def run_sweep(reg_cls, args, barrier, dist, torch, ws):
+    """The c3 sweep: 3240 candidate maps per step, device-timed (zcb_sweep), then search end to end
+    through the public API from host images."""
+    from zcmir_b200 import synth
+
+    m16, f16, H = synth.pair_similarity(n=512, seed=2)
+    m, f = (m16 / 65535.0).astype(np.float32), (f16 / 65535.0).astype(np.float32)
+    reg = reg_cls(**SWEEP_SETTINGS)
+    reg.set_images(m, f, preprocess=False)
+    for _ in range(args.warmup):
+        sw = reg.sweep(n_peak=4, batch=128)
+    barrier()
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms = [reg.sweep(n_peak=4, batch=128).info["ms"] for _ in range(args.steps)]
+    barrier()
+    ms_step = float(np.mean(ms))
+    info = reg.sweep(n_peak=4, batch=128).info
+    if dist:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    # e2e: the images from host memory, features, sweep, NMS, Gauss–Newton screen and finalists
+    for _ in range(max(1, args.warmup // 2)):
+        reg.set_images(m, f, preprocess=False)
+        reg.pose = np.eye(3)
+        reg.search()
+    barrier()
+    t0 = time.perf_counter()
+    n_e2e = max(3, args.steps // 2)
+    for _ in range(n_e2e):
+        reg.set_images(m, f, preprocess=False)
+        reg.pose = np.eye(3)
+        r = reg.search()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    corner = 0.0
+    for x, y in [(1, 1), (512, 1), (512, 512), (1, 512)]:
+        a, b = r.H @ [x, y, 1.0], H @ [x, y, 1.0]
+        corner = max(corner, float(np.hypot(*(a[:2] / a[2] - b[:2] / b[2]))))
+    out = {"metric": "sweep poses/s", "value": ws * info["candidates"] / (ms_step * 1e-3), "unit": "poses/s",
+           "ms_per_step": ms_step, "config": dict(SWEEP_CONFIG, parallelism=f"replicas{ws}"),
+           "launches_per_step": int(info["launches"]), "clocks": clk.summary(), "plane_sizes": int(info["groups"]), "batches": int(info["batches"]),
+           "e2e": {"value": ws / e2e_s, "unit": "searches/s", "seconds_per_search": e2e_s,
+                   "h2d_bytes_per_step": int(m.nbytes + f.nbytes), "d2h_bytes_per_step": 104,
+                   "what": "set_images + search (sweep, NMS, 4-step batched Gauss-Newton screen, 25-step finalists)",
+                   "corner_error_px": corner}}
+    reg.close()
+    return out, m, f
 
 
 def run_reference(args, rank):
@@ -231,6 +334,7 @@ def run_gpu(args, rank, ws, local):
         e2e_s = float(t.item())
     assert (e.dx, e.dy) == (sm.dx, sm.dy)
 
+    line = None
     if rank == 0:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
         hbm = peaks.get("hbm_gbs")
@@ -267,8 +371,15 @@ def run_gpu(args, rank, ws, local):
             sec, _ = cpu_map_seconds(m, f)
             line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "maps/s", "cores": os.cpu_count(), "kind": "port",
                                     "sample": "one full 1024² map of the same pair (float64 oracle, scipy FFTs)"}
-        print(json.dumps(line), flush=True)
     reg.close()
+    sweep, sm_, sf_ = run_sweep(zc.Registrar, args, barrier, dist, torch, ws)
+    if rank == 0:
+        if ws == 1 and not args.no_cpu:
+            v, n = sweep_cpu_sample(sm_, sf_)
+            sweep["cpu_baseline"] = {"value": v, "unit": "poses/s", "cores": os.cpu_count(), "kind": "port",
+                                     "sample": f"{n} evenly spaced candidates of the 3240 (float64 oracle, numpy FFTs)"}
+        line["sweep"] = sweep
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -277,7 +388,7 @@ def run_gpu(args, rank, ws, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

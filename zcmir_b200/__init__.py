@@ -367,6 +367,7 @@ class Registrar:
             "ms_per_map": float(out[0]), "stages_ms": dict(zip(stages, map(float, out[1:6]))),
             "nx": int(out[8]), "ny": int(out[9]), "cw": int(out[10]), "ch": int(out[11]),
             "n_real": int(out[12]), "n_corr": int(out[13]), "split": int(out[14]), "canvas_w": int(out[15]),
+            "canvas_h": int(out[7]),
         }
 
     # ── lifetime ──

@@ -490,6 +490,7 @@ bool Engine::bench_maps(const Mat3& Hm, unsigned flags, unsigned cap, unsigned w
     out[12] = job.plan.n_real;
     out[13] = job.plan.n_corr;
     out[14] = job.S;
+    out[7] = job.g.Hh;
     out[15] = job.g.W;
     return true;
 }
