@@ -28,13 +28,33 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
  * and prior pose H0 (NULL: the pose zc_search would use). For every candidate (θ-major, then σ,
  * shear, stretch) its n_peak (1..16) best lane maxima — score in fixed pixels, map index
  * (0xffffffff: none) — into scores / idx (cap ≥ candidates × n_peak; both NULL: not returned).
- * batch: candidates per launch (0: from a 1 GB budget). info[16]: [0] candidates, [1] cell (px),
+ * batch: candidates per launch (0: from a 1 GB budget). shard / nshard: only the candidates in
+ * slots ≡ shard (mod nshard) of the plane-size order are mapped (one rank's share of a sweep
+ * split across GPUs); the others' entries stay (0, 0xffffffff), so the shards' outputs merge by
+ * a sum of scores and a minimum of indices. info[16]: [0] candidates, [1] cell (px),
  * [2] device ms of the maps, [3] grid G, [4..5] fixed window Fx, Fy (cells), [6..7] its first
  * cell, [8] overlap floor (cells), [9] largest plane side, [10] plane-size groups, [11] batches,
  * [12] kernel launches, [13..14] canvas origin (px), [15] peaks. No counterpart in the reference
  * (its sweep is internal to zc_search, src/search.zig:300-494). 0 / -1 with zc_error. */
-int32_t zcb_sweep(zc_engine* e, const double H0[9], uint32_t n_peak, uint32_t batch, float* scores, uint32_t* idx,
-                  size_t cap, double* info, size_t info_len);
+int32_t zcb_sweep(zc_engine* e, const double H0[9], uint32_t n_peak, uint32_t batch, uint32_t shard, uint32_t nshard,
+                  float* scores, uint32_t* idx, size_t cap, double* info, size_t info_len);
+
+/* zc_search from gathered lane maxima: scores / idx hold every candidate's 4 lane maxima (n =
+ * candidates × 4, as zcb_sweep with n_peak 4 writes them, merged over shards); the engine's
+ * settings must be those of the sweep. Runs the rest of the search (peaks → poses, NMS, batched
+ * Gauss–Newton screen, finalists) and sets the pose as zc_search does. No counterpart in the
+ * reference (its search is one call, src/search.zig:663-820). 0 / -1 with zc_error. */
+int32_t zcb_search_lanes(zc_engine* e, const float* scores, const uint32_t* idx, size_t n, zc_search_result* out);
+
+/* Shift maps along a stack of n ≥ 2 slices (gray f32 images[i], w[i] × h[i]): each slice's
+ * features are built once, then slice k (moving) is mapped against slice k − 1 (fixed) for
+ * k = 1..n−1 at pose priors[9·(k−1)..] (NULL: the slices' centres aligned), with flags (1 exact,
+ * 2 calibrated) and cap as zc_shift_map; out[k−1] gets each map's result, *ms (nullable) the
+ * device time of the whole stack (features and maps). The engine's own image pair and pose are
+ * left as they were. No counterpart in the reference (its register_stack registers pair by pair
+ * through the functional API, python/zcmir/api.py:522-580). 0 / -1 with zc_error. */
+int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, const uint32_t* w, const uint32_t* h,
+                       const double* priors, uint32_t flags, uint32_t cap, zc_shift_result* out, double* ms);
 
 /* Scores of n poses (Hs: n row-major 3×3 maps, each as zc_score's H) into out[3n], per pose the
  * mean, forward and inverse score exactly as zc_score writes them, allocating no device memory.

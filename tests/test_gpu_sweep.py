@@ -132,3 +132,28 @@ def test_search_refusals():
         reg.configure(search_mode="sweep", metric="ncc")
         with pytest.raises(RuntimeError, match="ncc"):
             reg.search()
+
+
+def test_sweep_shards_merge_to_the_whole_sweep(small):
+    """Three shards of one sweep (zcb_sweep shard/nshard), merged as the ranks of a split sweep
+    merge them (sum of scores, minimum of indices), give the whole sweep; the search finished
+    from the merged lanes (zcb_search_lanes) reaches the same pose as search()."""
+    m, f, H = small
+    with zc.Registrar(half=False, sw_nth=12, sw_ns=3, sw_smin=0.8, sw_smax=1.25, sw_grid=64) as reg:
+        reg.set_images(m, f, preprocess=False)
+        whole = reg.sweep(n_peak=4)
+        parts = [reg.sweep(n_peak=4, shard=r, nshard=3) for r in range(3)]
+        owned = [(p.index != 0xFFFFFFFF).any(axis=1) for p in parts]
+        assert sum(o.astype(int) for o in owned).max() <= 1
+        sc = np.sum([p.scores for p in parts], axis=0)
+        ix = np.minimum.reduce([p.index for p in parts])
+        np.testing.assert_array_equal(ix, whole.index)
+        np.testing.assert_allclose(sc, whole.scores, rtol=1e-6, atol=0)
+        reg.pose = np.eye(3)
+        r1 = reg.search()
+        reg.pose = np.eye(3)
+        r2 = reg.search_lanes(sc, ix)
+        assert r2.count_a == r1.count_a and r2.improved == r1.improved
+        assert corner_dist(r2.H, r1.H, 128, 128) < 0.05
+        with pytest.raises(RuntimeError, match="lane entries"):
+            reg.search_lanes(sc[:-1], ix[:-1])

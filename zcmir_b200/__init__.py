@@ -22,7 +22,8 @@ from . import _native
 
 __all__ = [
     "Registrar", "ShiftMap", "Score", "Gradient", "Climb", "Search",
-    "shift_map", "score", "refine", "register", "search", "settings", "close", "__version__",
+    "shift_map", "score", "refine", "register", "register_stack", "stack_maps", "search", "settings", "close",
+    "Registration", "StackRegistration", "__version__",
 ]
 
 __version__ = "0.1.4"
@@ -183,7 +184,9 @@ class Registrar:
         return json.loads(buf.raw[:n])
 
     # ── images ──
-    def _set(self, side, img, preprocess):
+    @staticmethod
+    def _gray(img):
+        """A contiguous float32 gray image (uint16 scaled to [0, 1], RGB(A) to luma)."""
         a = np.asarray(img)
         if a.dtype == np.uint8:
             raise ValueError("uint8 images are always preprocessed (CLAHE), which this build leaves out: "
@@ -196,6 +199,10 @@ class Registrar:
             a = np.ascontiguousarray(a, dtype=np.float32)
         if a.ndim != 2:
             raise ValueError("expected a gray image (h, w)")
+        return a
+
+    def _set(self, side, img, preprocess):
+        a = self._gray(img)
         h, w = a.shape
         rc = self._lib.zc_set_image_gray(self._e, side, _fp(a), w, h, 1 if preprocess else 0)
         self._check(rc, "set_image")
@@ -298,6 +305,34 @@ class Registrar:
             exact=bool(r.exact), calibrated=bool(r.calibrated), map=m, ny=ny, peak_index=r.peak_index,
         )
 
+    def stack_maps(self, slices, priors=None, *, exact=True, calibrated=False, resolution=0):
+        """Shift maps along a stack: slice k (moving) against slice k − 1 (fixed) for every k ≥ 1,
+        each slice's features built once (zcb_stack_maps). priors: n − 1 poses (default: the
+        slices' centres aligned). Returns the n − 1 ShiftMaps (without their maps) and the device
+        ms of the whole stack. The engine's own images and pose are left as they were."""
+        imgs = [self._gray(x) for x in slices]
+        n = len(imgs)
+        if n < 2:
+            raise ValueError("stack_maps: a stack needs at least 2 slices")
+        ptrs = (_native.f32p * n)(*[a.ctypes.data_as(_native.f32p) for a in imgs])
+        w = np.array([a.shape[1] for a in imgs], np.uint32)
+        h = np.array([a.shape[0] for a in imgs], np.uint32)
+        pr = None
+        if priors is not None:
+            pr = np.ascontiguousarray(np.asarray(priors, np.float64).reshape(n - 1, 9))
+        out = (_native.ShiftResult * (n - 1))()
+        ms = ctypes.c_double(0)
+        flags = (1 if exact else 0) | (2 if calibrated else 0)
+        self._check(self._lib.zcb_stack_maps(self._e, n, ptrs, w.ctypes.data_as(_native.u32p),
+                                             h.ctypes.data_as(_native.u32p),
+                                             None if pr is None else pr.ctypes.data_as(_native.f64p), flags, resolution,
+                                             out, ctypes.byref(ms)), "stack_maps")
+        maps = [ShiftMap(peak=r.peak, dx=r.dx, dy=r.dy, zero=r.zero, n=r.n, cw=r.cw, ch=r.ch,
+                         canvas=(r.canvas_w, r.canvas_h), offset=(r.ox, r.oy), corr_area_px=r.corr_area_px,
+                         exact=bool(r.exact), calibrated=bool(r.calibrated), map=None, ny=r.n_y or r.n,
+                         peak_index=r.peak_index) for r in out]
+        return maps, ms.value
+
     def canvas(self, H=None, inverse=False):
         a, p = self._Hp(H)
         c = _native.Canvas()
@@ -324,15 +359,16 @@ class Registrar:
             n *= min(max(int(s["sw_naniso"]), 1), 15)
         return n
 
-    def sweep(self, H0=None, n_peak=4, batch=0):
+    def sweep(self, H0=None, n_peak=4, batch=0, shard=0, nshard=1):
         """The sweep's batched maps alone (the first stage of search()) at prior pose H0 (None: the
-        one search() uses), with the sw_* settings."""
+        one search() uses), with the sw_* settings; shard / nshard: this share of a sweep split
+        across ranks (the other candidates' entries stay (0, 0xffffffff))."""
         nc = self._sweep_count()
         sc = np.zeros((nc, n_peak), np.float32)
         ix = np.zeros((nc, n_peak), np.uint32)
         info = np.zeros(16)
         a, h = (None, None) if H0 is None else _mat(H0)
-        self._check(self._lib.zcb_sweep(self._e, h, n_peak, batch, _fp(sc), ix.ctypes.data_as(_native.u32p), sc.size,
+        self._check(self._lib.zcb_sweep(self._e, h, n_peak, batch, shard, nshard, _fp(sc), ix.ctypes.data_as(_native.u32p), sc.size,
                                         info.ctypes.data_as(_native.f64p), 16), "sweep")
         keys = ("candidates", "cell", "ms", "grid", "Fx", "Fy", "fx0", "fy0", "min_n", "n", "groups", "batches",
                 "launches", "ox", "oy", "peaks")
@@ -340,6 +376,15 @@ class Registrar:
         if int(d["candidates"]) != nc:
             raise RuntimeError(f"sweep: {int(d['candidates'])} candidates, expected {nc}")
         return Sweep(sc, ix, d)
+
+    def search_lanes(self, scores, index):
+        """search() from every candidate's 4 lane maxima gathered from sharded sweeps."""
+        sc = np.ascontiguousarray(scores, np.float32).reshape(-1)
+        ix = np.ascontiguousarray(index, np.uint32).reshape(-1)
+        r = _native.SearchResult()
+        self._check(self._lib.zcb_search_lanes(self._e, _fp(sc), ix.ctypes.data_as(_native.u32p), sc.size,
+                                               ctypes.byref(r)), "search")
+        return Search(np.array(list(r.H)).reshape(3, 3), r.score, r.prev, bool(r.improved), r.count_a, r.count_b)
 
     # ── profiling ──
     def profile(self, on=True):
@@ -389,4 +434,7 @@ class Registrar:
             pass
 
 
-from .api import close, refine, register, score, search, settings, shift_map  # noqa: E402
+from .api import (  # noqa: E402
+    Registration, StackRegistration, close, refine, register, register_stack, score, search, settings, shift_map,
+    stack_maps,
+)

@@ -87,7 +87,9 @@ SIGS = {
     "zc_result_sizes": ([u32p], None),
     "zcb_bench_maps": ([P, f64p, U32, U32, U32, U32, f64p, SZ], I32),
     "zcb_score_static": ([P, f64p, U32, f64p], I32),
-    "zcb_sweep": ([P, f64p, U32, U32, f32p, u32p, SZ, f64p, SZ], I32),
+    "zcb_stack_maps": ([P, U32, ctypes.POINTER(f32p), u32p, u32p, f64p, U32, U32, ctypes.POINTER(ShiftResult), f64p], I32),
+    "zcb_sweep": ([P, f64p, U32, U32, U32, U32, f32p, u32p, SZ, f64p, SZ], I32),
+    "zcb_search_lanes": ([P, f32p, u32p, SZ, ctypes.POINTER(SearchResult)], I32),
     "zcb_settings_apply": ([ctypes.c_char_p, SZ, ctypes.c_char_p, SZ, ctypes.POINTER(SZ), ctypes.c_char_p, SZ, ctypes.POINTER(SZ)], I32),
 }
 

@@ -4,6 +4,8 @@ Every function takes the engine's settings as keyword arguments (``settings()`` 
 starts from the defaults, so one call never changes another. Calls are serialised.
 """
 import difflib
+import json
+import math
 import threading
 from dataclasses import dataclass
 
@@ -101,6 +103,7 @@ class Registration:
     fixed_shape: tuple
     method: str = "refine"
     iterations: int = 0
+    redetected: bool = False
 
     def __repr__(self):
         return f"Registration({self.model}, score {self.score:.4g}, {self.method})"
@@ -110,6 +113,11 @@ class Registration:
         p = np.asarray(points, np.float64).reshape(-1, 2)
         q = np.c_[p, np.ones(len(p))] @ self.H.T
         return q[:, :2] / q[:, 2:]
+
+    def to_dict(self):
+        return {"H": np.asarray(self.H).tolist(), "score": float(self.score), "model": self.model,
+                "moving_shape": list(self.moving_shape), "fixed_shape": list(self.fixed_shape), "method": self.method,
+                "iterations": int(self.iterations), "redetected": bool(self.redetected)}
 
 
 def shift_map(moving, fixed, H=None, *, preprocess=True, **settings):
@@ -179,3 +187,168 @@ def search(moving, fixed, H=None, *, mode="sweep", rotation=None, scale=None, sh
         reg.search()
         return Registration(H=reg.pose, score=reg.score(reg.pose).mean, model=s["group"], moving_shape=m.shape,
                             fixed_shape=f.shape, method=f"search ({mode})")
+
+
+# ── stacks (python/zcmir/api.py:430-580) ──────────────────────────────────────────────────────
+
+@dataclass
+class StackRegistration:
+    """A registered stack: one Registration per slice pair (None where none was made), each
+    slice's distance off the trend of its neighbours (fixed px), and the slices flagged as off it."""
+    slices: list
+    off_trend: list
+    flagged: list
+    threshold: float
+
+    def __len__(self):
+        return len(self.slices)
+
+    def __getitem__(self, i):
+        return self.slices[i]
+
+    def __repr__(self):
+        n = sum(r is not None for r in self.slices)
+        return (f"StackRegistration({n}/{len(self.slices)} registered, {sum(self.flagged)} flagged, "
+                f"threshold {self.threshold:.1f} px)")
+
+    @property
+    def H(self):
+        return [None if r is None else r.H for r in self.slices]
+
+    def to_json(self, path=None):
+        d = json.dumps({
+            "convention": "H maps moving pixel coordinates to fixed pixel coordinates, row-major 3x3, 1-based pixel centres",
+            "threshold_px": self.threshold,
+            "slices": [None if r is None else {**r.to_dict(), "off_trend_px": t, "flagged": bool(fl)}
+                       for r, t, fl in zip(self.slices, self.off_trend, self.flagged)],
+        }, indent=1)
+        if path:
+            with open(path, "w") as fh:
+                fh.write(d)
+        return d
+
+
+def _corners(r):
+    h, w = r.moving_shape[:2]
+    return np.array([[1, 1], [w, 1], [w, h], [1, h]], np.float64)
+
+
+def _apply(H, p):
+    q = np.c_[p, np.ones(len(p))] @ np.asarray(H).T
+    return q[:, :2] / q[:, 2:]
+
+
+def _pose_gap(r, H, refs):
+    """Largest corner distance (fixed px) between pose H and the mean of the reference poses."""
+    if not refs:
+        return None
+    c = _corners(r)
+    ref = np.mean([_apply(R, c) for R in refs], axis=0)
+    return float(np.max(np.hypot(*(_apply(H, c) - ref).T)))
+
+
+def _expected(res, k, c):
+    """Where slice k's corners c should land given its neighbours: their mean between two, a
+    straight-line extrapolation at the ends (a stack that drifts steadily flags nothing)."""
+    get = lambda j: res[j] if 0 <= j < len(res) else None
+    a, b = get(k - 1), get(k + 1)
+    if a is not None and b is not None:
+        return (_apply(a.H, c) + _apply(b.H, c)) / 2
+    for near, far in ((a, get(k - 2)), (b, get(k + 2))):
+        if near is not None:
+            return 2 * _apply(near.H, c) - _apply(far.H, c) if far is not None else _apply(near.H, c)
+    return None
+
+
+def _trend(res, jump):
+    e = []
+    for k, r in enumerate(res):
+        ref = None if r is None else _expected(res, k, _corners(r))
+        e.append(None if ref is None else float(np.max(np.hypot(*(_apply(r.H, _corners(r)) - ref).T))))
+    vals = sorted(v for v in e if v is not None)
+    thr = float(jump) if jump is not None else max(2.0, 4 * vals[len(vals) // 2]) if vals else math.inf
+    return e, [v is not None and len(vals) >= 3 and v > thr for v in e], thr
+
+
+def _detect(m, f, kw):
+    """A slice pair from scratch: the rotation × scale sweep (this build's global search; keypoint
+    detection is not part of it), the pose it returns climbed by its finalists' refine."""
+    r = search(m, f, **kw)
+    r.method = "search"
+    return r
+
+
+def register_stack(moving, fixed, *, start="previous", drop=0.15, jump=None, polish=False, progress=None,
+                   model="homography", preprocess=True, register_pair=None, detect_pair=None, **settings):
+    """Register a moving stack to a fixed stack, slice pair by slice pair (serial sections, time
+    series): the first pair by the sweep search, then each from the previous pair's pose
+    (refined), as python/zcmir/api.py:522-580 does with keypoints for the first pair.
+
+    moving, fixed: sequences of images.
+    start: "previous" (carry the previous pose) or "search" (every slice by the sweep search;
+        "keypoints" is taken as "search").
+    drop: re-detect (by the sweep search) when a slice's score falls more than this fraction below
+        the previous slice's (the better of the two poses is kept).
+    jump: the same when the pose jumps more than this many fixed px from the previous slice's
+        (None: automatic, 4× the median jump so far, at least 2 px); it also flags slices off the
+        trend of their neighbours in the result.
+    polish: afterwards refine each slice again from the next slice's pose (last to first) and
+        keep it when it scores higher.
+    progress: callable(i, n, registration) after each slice.
+    register_pair / detect_pair: the refine from a pose and the search from scratch (default: this
+        module's refine and search on the GPU).
+    """
+    if start not in ("previous", "search", "keypoints"):
+        raise ValueError('start: "previous" or "search"')
+    kw = dict(model=model, preprocess=preprocess, **settings)
+    refine_ = register_pair or (lambda m, f, H: register(m, f, init=H, **kw))
+    detect_ = detect_pair or (lambda m, f: _detect(m, f, kw))
+    n = min(len(moving), len(fixed))
+    res, jumps = [None] * n, []
+
+    def thr_now():
+        if jump is not None:
+            return float(jump)
+        if len(jumps) < 3:
+            return math.inf
+        v = sorted(jumps)
+        return max(2.0, 4 * v[len(v) // 2])
+
+    for i in range(n):
+        m, f = moving[i], fixed[i]
+        prev = res[i - 1] if i else None
+        if start != "previous" or prev is None:
+            r = detect_(m, f)
+        else:
+            r = refine_(m, f, prev.H)
+            r.method = "carry"
+            g = _pose_gap(r, r.H, [prev.H])
+            dropped = prev.score > 0 and r.score < prev.score * (1 - drop)
+            if dropped or g > thr_now():
+                k = detect_(m, f)
+                r = k if k.score > r.score else r
+                r.redetected = True
+        if prev is not None:
+            jumps.append(_pose_gap(r, r.H, [prev.H]))
+        res[i] = r
+        if progress:
+            progress(i, n, r)
+    if polish:
+        for i in range(n - 2, -1, -1):
+            r = refine_(moving[i], fixed[i], res[i + 1].H)
+            if r.score > res[i].score * (1 + 1e-4):
+                r.method, r.redetected = "carry", res[i].redetected
+                res[i] = r
+    e, flags, thr = _trend(res, jump)
+    return StackRegistration(res, e, flags, thr)
+
+
+def stack_maps(slices, priors=None, *, exact=True, calibrated=False, resolution=0, preprocess=False, **settings):
+    """Shift maps along one stack — slice k (moving) against slice k − 1 (fixed) — with every
+    slice's features built once on the GPU. Returns the n − 1 ShiftMaps and the device ms."""
+    if preprocess:
+        raise ValueError("stack_maps: preprocessing is not part of this build; pass preprocess=False")
+    with _LOCK:
+        reg = _engine()
+        reg.configure(**_resolve(**settings))
+        return reg.stack_maps(slices, priors, exact=exact, calibrated=calibrated, resolution=resolution)

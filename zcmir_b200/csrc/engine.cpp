@@ -91,6 +91,9 @@ Engine::~Engine() {
                       &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &sw_il_[0], &sw_il_[1], &sw_poses_,
                       &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
+    for (auto& s : stack_)
+        for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack}) b->release();
+    stack_res_.release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);
 }
@@ -418,7 +421,13 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     float zero;
     memcpy(&best, host, 8);
     memcpy(&zero, host + 8, 4);
+    map_result(job, best, zero, pair_area(), out);
+    return true;
+}
+
+void Engine::map_result(const MapJob& job, unsigned long long best, float zero, double area, zc_shift_result* out) {
     const MapGeom& g = job.g;
+    const size_t nn = (size_t)g.nx * g.ny;
     zc_shift_result r{};
     r.n = g.nx;
     r.n_y = g.ny;
@@ -430,7 +439,7 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     r.oy = g.oy;
     r.peak = key_float((uint32_t)(best >> 32));
     r.zero = zero;
-    r.corr_area_px = pair_area();
+    r.corr_area_px = area;
     r.exact = job.exact;
     r.calibrated = job.calibrated;
     const uint32_t idx = 0xffffffffu - (uint32_t)(best & 0xffffffffu);
@@ -443,7 +452,6 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
         r.dy = (double)ly * ((double)g.Hh / (double)g.ch);
     }
     *out = r;
-    return true;
 }
 
 bool Engine::shift_map_settings(const Mat3& Hm, zc_shift_result* out, float* map, size_t map_len) {

@@ -81,6 +81,7 @@ struct SweepOut {
     std::vector<SweepCand> cands;       // θ-major, then σ, shear, stretch
     std::vector<SweepPeak> peaks;       // slot order (by plane size), then rank
     std::vector<float> best;            // each candidate's top score, fixed pixels
+    std::vector<int> perm;              // slot order: candidates by plane size (stable)
     std::vector<float> lane_score;      // [nc][n_peak] lane maxima per candidate, fixed pixels
     std::vector<uint32_t> lane_idx;     // their map indices (0xffffffff: none)
     double cell = 0, ox = 0, oy = 0;
@@ -144,6 +145,13 @@ class Engine {
     bool shift_map(const Mat3& H, bool exact, bool calibrated, unsigned cap, double min_overlap, zc_shift_result* out,
                    float* map, size_t map_len);
     bool shift_map_settings(const Mat3& H, zc_shift_result* out, float* map, size_t map_len);
+    // a map's result from its best key (score bits, inverted index), zero-lag score and the
+    // pair's correlation area
+    void map_result(const MapJob& job, unsigned long long best, float zero, double area, zc_shift_result* out);
+    // maps along a stack (engine_stack.cpp): each slice's features once, then slice k (moving)
+    // against slice k − 1 (fixed) at priors[k − 1] for k = 1..n−1; ms: device time of it all
+    bool stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,
+                    bool calibrated, unsigned cap, zc_shift_result* out, float* ms);
     // benchmark: warmup + steps maps at H (device-resident inputs), per-step CUDA-event times
     bool bench_maps(const Mat3& H, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
                     size_t out_len);
@@ -162,7 +170,16 @@ class Engine {
     // the rotation × scale sweep (engine_sweep.cpp): every candidate's map reduced to n_peak
     // peaks; batch 0 picks the batch from a memory budget
     bool sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
-                    SweepOut& out, int batch = 0);
+                    SweepOut& out, int batch = 0, int shard = 0, int nshard = 1);
+    // the host half of a sweep: canvas, candidates, footprints, plane sizes and slot order
+    bool sweep_setup(const Mat3& H0, const SweepGrid& gv, int G, SweepOut& out);
+    // the peaks and their poses from the lane maxima (slot order)
+    void sweep_make_peaks(SweepOut& out, int n_peak);
+    // the search from a sweep's peaks: NMS, batched Gauss–Newton screen, finalists, the pose
+    bool search_finish(const SweepOut& res, const SweepGrid& gv, const Mat3& H0, zc_search_result* out);
+    // the search from every candidate's 4 lane maxima gathered from sharded sweeps
+    bool search_lanes(const float* scores, const uint32_t* idx, size_t n, zc_search_result* out);
+    bool search_check();
     // Gauss–Newton on many poses at once (src/search.zig gnBatch)
     bool gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
                   std::vector<ScoredPose>& out);
@@ -180,6 +197,8 @@ class Engine {
     DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
+    std::vector<Side> stack_;
+    DevBuf stack_res_;
     DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;
     std::vector<float> pose_host_;
     std::map<int, float2*> tw_;

@@ -25,13 +25,9 @@ size_t pitch_of(int nx) { return (size_t)((nx / 2 + 1) + 7) / 8 * 8; }
 
 }  // namespace
 
-bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
-                        SweepOut& out, int batch) {
+bool Engine::sweep_setup(const Mat3& H0, const SweepGrid& gv, int G, SweepOut& out) {
     if (!need_images()) return false;
-    if (n_peak < 1 || n_peak > 16) return fail("sweep: n_peak must be 1..16");
     if (gv.count() == 0) return fail("sweep: empty candidate grid");
-    const bool three = side[0].mode == 1;
-    const CorrPlanDev plan = corr_plan_dev(exact, three);
     const Side &A = side[0], &B = side[1];
     const double fw = B.w, fh = B.h, mw = A.w, mh = A.h;
     const bool ladder = set.e("fft_sizes") != "compact";
@@ -80,15 +76,37 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
                     out.cands.push_back(c);
                 }
     // slots: candidates grouped by plane size (stable)
-    std::vector<int> perm(nc);
+    std::vector<int>& perm = out.perm;
+    perm.resize(nc);
     for (int k = 0; k < nc; ++k) perm[k] = k;
     std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
         const uint64_t ka = ((uint64_t)out.cands[a].nx << 32) | (uint64_t)out.cands[a].ny;
         const uint64_t kb = ((uint64_t)out.cands[b].nx << 32) | (uint64_t)out.cands[b].ny;
         return ka < kb;
     });
-    std::vector<float> poses((size_t)(nc + 1) * 12, 0.f);
-    for (int k = 0; k < nc; ++k) {
+    return true;
+}
+
+bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
+                        SweepOut& out, int batch, int shard, int nshard) {
+    if (n_peak < 1 || n_peak > 16) return fail("sweep: n_peak must be 1..16");
+    if (nshard < 1 || shard < 0 || shard >= nshard) return fail("sweep: shard must be 0..nshard-1");
+    if (!sweep_setup(H0, gv, G, out)) return false;
+    const bool three = side[0].mode == 1;
+    const CorrPlanDev plan = corr_plan_dev(exact, three);
+    const Side &A = side[0], &B = side[1];
+    const double fw = B.w, fh = B.h;
+    const double cell = out.cell, ox = out.ox, oy = out.oy;
+    const std::array<int, 2> fcx{out.fx0, out.fx0 + out.Fx}, fcy{out.fy0, out.fy0 + out.Fy};
+    const int Fx = out.Fx, Fy = out.Fy;
+    const int nc = (int)out.cands.size();
+    // this shard's candidates in slot order: slots s ≡ shard (mod nshard), so every shard gets
+    // candidates of every plane size
+    std::vector<int> perm;
+    for (int s = shard; s < nc; s += nshard) perm.push_back(out.perm[s]);
+    const int nm = (int)perm.size();
+    std::vector<float> poses((size_t)(nm + 1) * 12, 0.f);
+    for (int k = 0; k < nm; ++k) {
         const SweepCand& c = out.cands[perm[k]];
         const Mat3 Hi = inv3(c.H);
         for (int q = 0; q < 9; ++q) poses[(size_t)k * 12 + q] = (float)Hi[q];
@@ -97,7 +115,7 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
         poses[(size_t)k * 12 + 11] = (float)c.gy0;
     }
     // the fixed window's pose: identity, taps from the cell, its first cell
-    float* fp = poses.data() + (size_t)nc * 12;
+    float* fp = poses.data() + (size_t)nm * 12;
     fp[0] = fp[4] = fp[8] = 1.f;
     fp[9] = (float)std::min(6.0, std::max(1.0, std::ceil(cell - 1e-3)));
     fp[10] = (float)fcx[0];
@@ -134,8 +152,8 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
               cuda_ok(sw_grid_.ensure(grid_max * 4 * bmax), "sweep") &&
               cuda_ok(sw_half_.ensure(half_max * 8 * bmax), "sweep") && cuda_ok(sw_q_.ensure(q_max * 8 * bmax), "sweep") &&
               cuda_ok(sw_map_.ensure(map_max * 4 * bmax), "sweep") && cuda_ok(sw_n0_.ensure((size_t)bmax * 8), "sweep") &&
-              cuda_ok(sw_ps_.ensure((size_t)nc * n_peak * 4), "sweep") &&
-              cuda_ok(sw_pi_.ensure((size_t)nc * n_peak * 4), "sweep");
+              cuda_ok(sw_ps_.ensure((size_t)std::max(nm, 1) * n_peak * 4), "sweep") &&
+              cuda_ok(sw_pi_.ensure((size_t)std::max(nm, 1) * n_peak * 4), "sweep");
     if (!ok) return false;
     if (!cuda_ok(cudaMemcpyAsync(sw_poses_.p, poses.data(), poses.size() * 4, cudaMemcpyHostToDevice, st), "sweep"))
         return false;
@@ -154,7 +172,7 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     int launches = 0;
     if (!cuda_ok(sweep_interleave(A.stack.as<float>(), (int)na, sw_il_[0].as<float4>(), st), "sweep") ||
         !cuda_ok(sweep_interleave(B.stack.as<float>(), (int)nb, sw_il_[1].as<float4>(), st), "sweep") ||
-        !cuda_ok(sweep_pack(ilb, B.w, B.h, sw_poses_.as<float>(), nc, 1, Fx, Fy, cv, nullptr, 0, 0, 0, 0,
+        !cuda_ok(sweep_pack(ilb, B.w, B.h, sw_poses_.as<float>(), nm, 1, Fx, Fy, cv, nullptr, 0, 0, 0, 0,
                             sw_fgrid_.as<float>(), nullptr, st),
                  "sweep"))
         return done(false);
@@ -167,10 +185,10 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     cp.min_n = (float)out.min_n;
     cp.area = 1.0;
     cp.ridge = 1e-4;
-    for (int k0 = 0; k0 < nc;) {
+    for (int k0 = 0; k0 < nm;) {
         const int nx = out.cands[perm[k0]].nx, ny = out.cands[perm[k0]].ny;
         int k1 = k0;
-        while (k1 < nc && out.cands[perm[k1]].nx == nx && out.cands[perm[k1]].ny == ny) ++k1;
+        while (k1 < nm && out.cands[perm[k1]].nx == nx && out.cands[perm[k1]].ny == ny) ++k1;
         MapGeom gm{};
         gm.nx = nx, gm.ny = ny, gm.WP = (int)pitch_of(nx);
         gm.cw = nx - Fx + 1, gm.ch = ny - Fy + 1;
@@ -218,8 +236,8 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
         k0 = k1;
     }
     cudaEventRecord(e1, st);
-    std::vector<float> ps((size_t)nc * n_peak);
-    std::vector<uint32_t> pi((size_t)nc * n_peak);
+    std::vector<float> ps((size_t)nm * n_peak);
+    std::vector<uint32_t> pi((size_t)nm * n_peak);
     if (!cuda_ok(cudaMemcpyAsync(ps.data(), sw_ps_.p, ps.size() * 4, cudaMemcpyDeviceToHost, st), "sweep") ||
         !cuda_ok(cudaMemcpyAsync(pi.data(), sw_pi_.p, pi.size() * 4, cudaMemcpyDeviceToHost, st), "sweep") ||
         !cuda_ok(cudaStreamSynchronize(st), "sweep"))
@@ -230,36 +248,46 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     counts[1]++;
     counts[2] += 2;
     counts[3]++;
-    // peaks → poses (src/search.zig:460-493): scores in fixed pixels (n counts cells)
+    // each candidate's lane maxima, scores in fixed pixels (n counts cells); other shards' stay empty
     const double c2 = cell * cell;
-    out.best.assign(nc, 0.f);
     out.lane_score.assign((size_t)nc * n_peak, 0.f);
     out.lane_idx.assign((size_t)nc * n_peak, 0xffffffffu);
+    for (int j = 0; j < nm; ++j)
+        for (int k = 0; k < n_peak; ++k) {
+            out.lane_score[(size_t)perm[j] * n_peak + k] = (float)((double)ps[(size_t)j * n_peak + k] * c2);
+            out.lane_idx[(size_t)perm[j] * n_peak + k] = pi[(size_t)j * n_peak + k];
+        }
+    sweep_make_peaks(out, n_peak);
+    return done(true);
+}
+
+// Peaks → poses (src/search.zig:460-493) from the lane maxima, slot by slot (the reference's order).
+void Engine::sweep_make_peaks(SweepOut& out, int n_peak) {
+    const int nc = (int)out.cands.size();
+    out.peaks.clear();
+    out.best.assign(nc, 0.f);
     for (int slot = 0; slot < nc; ++slot) {
-        const int ci = perm[slot];
+        const int ci = out.perm[slot];
         const SweepCand& cd = out.cands[ci];
         for (int k = 0; k < n_peak; ++k) {
-            const double v = (double)ps[(size_t)slot * n_peak + k] * c2;
-            const uint32_t t = pi[(size_t)slot * n_peak + k];
-            out.lane_score[(size_t)ci * n_peak + k] = (float)v;
-            out.lane_idx[(size_t)ci * n_peak + k] = t;
+            const double v = out.lane_score[(size_t)ci * n_peak + k];
+            const uint32_t t = out.lane_idx[(size_t)ci * n_peak + k];
             if (!(v > 0) || (uint64_t)t >= (uint64_t)cd.nx * cd.ny) continue;
             if (k == 0) out.best[ci] = (float)v;
             // lag (moving index − fixed index) in [−(F − 1), window − 1], then the moving
             // image's canvas displacement gx0 + lag − fx0 cells; the correction is T(−d)
             const int py = (int)(t / (uint32_t)cd.nx), px = (int)(t - (uint32_t)py * (uint32_t)cd.nx);
-            const int wx = cd.nx - Fx + 1, wy = cd.ny - Fy + 1;
+            const int wx = cd.nx - out.Fx + 1, wy = cd.ny - out.Fy + 1;
             const int lx = px < wx ? px : px - cd.nx, ly = py < wy ? py : py - cd.ny;
             SweepPeak p;
             p.score = v;
             p.cand = ci, p.it = cd.it, p.is = cd.is, p.ik = cd.ik, p.ia = cd.ia, p.th = cd.th, p.s = cd.s;
-            p.sx = cd.gx0 + lx - fcx[0];
-            p.sy = cd.gy0 + ly - fcy[0];
-            p.H = mul3(translate(-p.sx * cell, -p.sy * cell), cd.H);
+            p.sx = cd.gx0 + lx - out.fx0;
+            p.sy = cd.gy0 + ly - out.fy0;
+            p.H = mul3(translate(-p.sx * out.cell, -p.sy * out.cell), cd.H);
             out.peaks.push_back(p);
         }
     }
-    return done(true);
 }
 
 bool Engine::gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
@@ -362,30 +390,58 @@ void Engine::sweep_settings(SweepGrid& gv, int& G, Mat3& H0) {
     H0 = set.b("sw_rel") ? H : translate((rw - lw) / 2, (rh - lh) / 2);
 }
 
-bool Engine::search(zc_search_result* out) {
+bool Engine::search_check() {
     if (!need_images()) return false;
     if (set.e("search_mode") != "sweep")
         return fail("search: search_mode \"" + set.e("search_mode") + "\" is not part of this build (search_mode=\"sweep\" is)");
     if (set.e("metric") != "smi")
         return fail("search: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
-    cancel = false;
-    if (set.b("ffd")) log_event("the spline stage is not part of this build; searching the homography only");
+    return true;
+}
+
+bool Engine::search(zc_search_result* out) {
+    if (!search_check()) return false;
     SweepGrid gv;
     int G;
     Mat3 H0;
     sweep_settings(gv, G, H0);
+    const double min_ov = std::min(0.5, std::max(0.0, set.f("min_overlap")));
+    SweepOut res;
+    if (!sweep_maps(H0, gv, G, set.b("exact"), 4, min_ov, res)) return false;
+    return search_finish(res, gv, H0, out);
+}
+
+bool Engine::search_lanes(const float* scores, const uint32_t* idx, size_t n, zc_search_result* out) {
+    if (!search_check()) return false;
+    SweepGrid gv;
+    int G;
+    Mat3 H0;
+    sweep_settings(gv, G, H0);
+    SweepOut res;
+    if (!sweep_setup(H0, gv, G, res)) return false;
+    const size_t need = res.cands.size() * 4;
+    if (n != need || !scores || !idx)
+        return fail("search_lanes: " + std::to_string(n) + " lane entries for " + std::to_string(res.cands.size()) +
+                    " candidates × 4 (the sweep settings must match the sweep's)");
+    res.lane_score.assign(scores, scores + n);
+    res.lane_idx.assign(idx, idx + n);
+    sweep_make_peaks(res, 4);
+    return search_finish(res, gv, H0, out);
+}
+
+bool Engine::search_finish(const SweepOut& res, const SweepGrid& gv, const Mat3& H0, zc_search_result* out) {
+    cancel = false;
+    if (set.b("ffd")) log_event("the spline stage is not part of this build; searching the homography only");
+    const int G = res.G;
     const unsigned kk = set.u("sw_k");
     const unsigned K = (kk == 8 || kk == 16 || kk == 32) ? kk : 32;
     const unsigned n_fin = std::clamp(set.u("sw_fin"), 1u, 16u);
-    const double min_ov = std::min(0.5, std::max(0.0, set.f("min_overlap")));
     const Mat3 Hcur = H;
     const double c_mov[2] = {(side[0].w + 1) / 2.0, (side[0].h + 1) / 2.0};
     std::vector<PoseEval> e0;
     if (!eval_poses({Hcur}, false, false, e0)) return false;
     const double s_cur = e0[0].mean;
     const bool exact = set.b("exact");
-    SweepOut res;
-    if (!sweep_maps(H0, gv, G, exact, 4, min_ov, res)) return false;
     const std::vector<SweepPeak> top = nms4(res.peaks, (unsigned)gv.thetas.size(), K, gv.wrap);
     char buf[320];
     snprintf(buf, sizeof buf, "search  %zuθ × %zuσ%s  %d maps  %d² grid (%.1f px, FFT ≤ %d²)  %s  %zu peaks  (%.2f ms)",

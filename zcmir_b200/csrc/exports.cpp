@@ -9,6 +9,7 @@
 #include <cstring>
 #include <exception>
 #include <string>
+#include <vector>
 
 #include "../../include/zcmir_b200.h"
 #include "engine.hpp"
@@ -365,8 +366,12 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
     return 0;
 }
 
-int32_t zcb_sweep(zc_engine* e, const double H0p[9], uint32_t n_peak, uint32_t batch, float* scores, uint32_t* idx,
-                  size_t cap, double* info, size_t info_len) {
+int32_t zcb_search_lanes(zc_engine* e, const float* scores, const uint32_t* idx, size_t n, zc_search_result* out) {
+    return guarded(e, "search_lanes", [&] { return e->search_lanes(scores, idx, n, out); });
+}
+
+int32_t zcb_sweep(zc_engine* e, const double H0p[9], uint32_t n_peak, uint32_t batch, uint32_t shard, uint32_t nshard,
+                  float* scores, uint32_t* idx, size_t cap, double* info, size_t info_len) {
     return guarded(e, "sweep", [&] {
         if (info_len < 16 || !info) return e->fail("sweep: info needs 16 entries");
         zc::SweepGrid gv;
@@ -376,7 +381,9 @@ int32_t zcb_sweep(zc_engine* e, const double H0p[9], uint32_t n_peak, uint32_t b
         const zc::Mat3 H0 = H0p ? mat(H0p) : Hd;
         const double min_ov = std::min(0.5, std::max(0.0, e->set.f("min_overlap")));
         zc::SweepOut r;
-        if (!e->sweep_maps(H0, gv, G, e->set.b("exact"), (int)n_peak, min_ov, r, (int)batch)) return false;
+        if (!e->sweep_maps(H0, gv, G, e->set.b("exact"), (int)n_peak, min_ov, r, (int)batch, (int)shard,
+                           (int)std::max(nshard, 1u)))
+            return false;
         const size_t n = r.lane_score.size();
         if (scores && idx) {
             if (cap < n) return e->fail("sweep: BufferTooSmall");
@@ -387,6 +394,23 @@ int32_t zcb_sweep(zc_engine* e, const double H0p[9], uint32_t n_peak, uint32_t b
                               (double)r.fx0, (double)r.fy0, (double)r.min_n, (double)r.n, (double)r.groups,
                               (double)r.batches, (double)r.launches, r.ox, r.oy, (double)r.peaks.size()};
         std::copy(v, v + 16, info);
+        return true;
+    });
+}
+
+int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, const uint32_t* w, const uint32_t* h,
+                       const double* priors, uint32_t flags, uint32_t cap, zc_shift_result* out, double* ms) {
+    return guarded(e, "stack_maps", [&] {
+        std::vector<int> ws(n), hs(n);
+        for (uint32_t i = 0; i < n; ++i) ws[i] = (int)w[i], hs[i] = (int)h[i];
+        std::vector<zc::Mat3> pr;
+        if (priors)
+            for (uint32_t k = 0; k + 1 < n; ++k) pr.push_back(mat(priors + 9 * k));
+        float t = 0;
+        if (!e->stack_maps((int)n, images, ws.data(), hs.data(), priors ? pr.data() : nullptr, (flags & 1) != 0,
+                           (flags & 2) != 0, cap, out, &t))
+            return false;
+        if (ms) *ms = t;
         return true;
     });
 }

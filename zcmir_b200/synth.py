@@ -10,6 +10,10 @@
 * ``pair_similarity`` (512² sweep workload): the same two modalities with the moving image under
   a random similarity about the image centre: rotation in [0°, 360°), scale log-uniform in
   [0.8, 1.25], shift in ±n/8 px.
+* ``stack_drift`` (stack workload): slices of one field with sizes uniform in [384, 1024] per side,
+  each slice a random similarity drift of the previous one (rotation N(0, 2°), log scale
+  N(0, 0.02), shift N(0, 8 px) per step), modalities alternating between the field and its
+  inverted nonlinear remap 1 − field², plus N(0, 0.02²).
 
 The true pose maps moving → fixed (1-based pixels): H = translate(dx, dy), i.e. the moving pixel
 x shows the fixed content at x + (dx, dy). The shift map at the identity pose then peaks at the
@@ -107,3 +111,41 @@ def pair_similarity(n=512, seed=2, deg=None, scale=None, shift=None, levels=8, n
     moving = perm[lab] / (levels - 1.0) + noise * rng.standard_normal((n, n))
     to16 = lambda a: (np.clip(a, 0, 1) * 65535 + 0.5).astype(np.uint16)
     return to16(moving), to16(fixed), H
+
+
+def stack_drift(n=32, size=(384, 1024), seed=3, drift=(2.0, 0.02, 8.0), noise=0.02):
+    """(slices, truths): n uint16 slices; truths[k − 1] maps slice k pixels to slice k − 1 pixels
+    (1-based), for k = 1..n−1."""
+    from scipy.ndimage import map_coordinates
+
+    rng = np.random.default_rng(seed)
+    sizes = [(int(rng.integers(size[0], size[1] + 1)), int(rng.integers(size[0], size[1] + 1))) for _ in range(n)]
+    th, ls, t = 0.0, 0.0, np.zeros(2)
+    poses = []
+    for k in range(n):
+        if k:
+            th += np.deg2rad(rng.normal(0, drift[0]))
+            ls += rng.normal(0, drift[1])
+            t = t + rng.normal(0, drift[2], 2)
+        poses.append((th, np.exp(ls), t.copy()))
+    side = int(1.6 * size[1] + 8 * drift[2] * np.sqrt(n)) + 64
+    field = blob_field(side, side, rng)
+    cw = (side + 1) / 2
+    slices, W = [], []
+    for (w, h), (a, sc, tt) in zip(sizes, poses):
+        c = np.array([(w + 1) / 2, (h + 1) / 2])
+        R = sc * np.array([[np.cos(a), -np.sin(a)], [np.sin(a), np.cos(a)]])
+        # slice pixel x (1-based) ↦ field pixel cw + R (x − c) + t
+        M = np.eye(3)
+        M[:2, :2] = R
+        M[:2, 2] = cw + tt - R @ c
+        W.append(M)
+        yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+        X = np.stack([xx + 1, yy + 1, np.ones_like(xx)], -1) @ M.T
+        v = map_coordinates(field, [X[..., 1] - 1, X[..., 0] - 1], order=1, mode="nearest")
+        if len(slices) % 2:
+            v = 1.0 - v ** 2
+        v = v + noise * rng.standard_normal(v.shape)
+        slices.append((np.clip(v, 0, 1) * 65535 + 0.5).astype(np.uint16))
+    truths = [np.linalg.inv(W[k - 1]) @ W[k] for k in range(1, n)]
+    return slices, truths
