@@ -1,0 +1,103 @@
+"""GPU parity of the roto-scale (log-polar) map, zc_rs_map, against the CPU oracle, and the
+reference's known answers for it.
+
+Tolerances: the peak index exact, the peak within 1e-4 relative; every cell within 1e-4 of the
+peak where the transform's own overlap (the weight correlation before each log-radius row is
+scaled by e^{kΔλ}·Δλ·Δθ) is at least 20 % of its largest, and within 1e-2 where it is at least
+1 % (below that the calibrated score amplifies the FP32 noise without bound: float32 FFTs on the
+CPU reach 40 % of the peak there, as float32 FFTs would in the reference). The row
+scale runs from r_in/r_out to r_out/r_in (≈ 1/200 … 200 here): it multiplies the FP32 FFT's
+round-off, which is relative to the transform's largest value, so rows of small raw overlap get
+large scaled sums with large relative error — float32 FFTs on the CPU show the same (1.7 % of
+cells over 1e-4 when the mask uses the scaled overlap, none with the raw one). Known answers: examples/03_smi.py:365 (the landsat-b
+pose turned by 6° and scaled by 1.08 about the engine's centre peaks within 2° of 6°) and
+tests/test_api.py:148-149 (at the registered pose |dθ|, |dσ| < 0.02)."""
+import numpy as np
+import pytest
+
+import zcmir_b200 as zc
+from oracle import rs_oracle as R
+from oracle import smi_oracle as O
+from zcmir_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def prep_from(feat, mode="laplacian"):
+    f = np.asarray(feat, np.float32)
+    return {"w": f.shape[2], "h": f.shape[1], "mode": mode, "feat": f, "acf": O.acf(f),
+            "stack": np.concatenate([np.ones((1,) + f.shape[1:], np.float32), f])}
+
+
+def turned(c, deg, s, H):
+    a = np.deg2rad(deg)
+    R_ = np.array([[s * np.cos(a), -s * np.sin(a), 0], [s * np.sin(a), s * np.cos(a), 0], [0, 0, 1.0]])
+    T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
+    return T(*c) @ R_ @ T(*-np.asarray(c)) @ H
+
+
+def check(g, o, n0, tight=1e-4, loose=1e-2):
+    peak = max(abs(o).max(), 1e-30)
+    err = np.abs(g.astype(np.float64) - o) / peak
+    disagree = (g == 0) != (o == 0)
+    big = n0 >= 0.2 * n0.max()
+    assert err[big & ~disagree].max() <= tight, err[big & ~disagree].max()
+    some = n0 >= 0.01 * n0.max()
+    assert err[some & ~disagree].max() <= loose, err[some & ~disagree].max()
+    assert disagree[some].mean() < 1e-3
+
+
+@pytest.mark.parametrize("calibrated", [False, True])
+def test_rs_map_matches_oracle(calibrated):
+    m, f, H = synth.pair_remap(n=192, shift=(6, -4), seed=2)
+    with zc.Registrar(half=False, calibrated=calibrated) as reg:
+        reg.set_images(m, f, preprocess=False)
+        Hp = turned((96.5, 96.5), 9.0, 1.05, H)
+        r = reg.rs_map(Hp)
+        pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
+    ref = R.rs_map(pa, pb, Hp, exact=True, calibrated=calibrated)
+    p = ref["plan"]
+    assert (r.n, r.n_th, r.n_lam) == (p["n"], p["n_th"], p["n_lam"])
+    assert r.r0 == pytest.approx(p["r0"], rel=1e-12) and r.r1 == pytest.approx(p["r1"], rel=1e-12)
+    assert r.dlam == pytest.approx(p["dlam"], rel=1e-12)
+    assert r.center == pytest.approx(ref["center"], rel=1e-12)
+    _, _, corr = R.rs_map_one(pa, pb, Hp, ref["center"], exact=True, calibrated=calibrated)
+    k = np.arange(p["n"])
+    k = np.where(k > p["n"] // 2, k - p["n"], k)
+    raw_n0 = corr[0] / (np.exp(k * p["dlam"]) * p["dlam"] * p["dth"])[:, None]
+    check(r.fwd, ref["fwd"], raw_n0)
+    check(r.map, ref["map"], raw_n0)
+    assert r.peak_index == ref["peak_index"]
+    assert abs(r.peak - ref["peak"]) <= 1e-4 * abs(ref["peak"])
+    assert (r.dth, r.dsg) == pytest.approx((ref["dth"], ref["dsg"]), abs=1e-12)
+    # the map undoes the applied turn: about −9° and 1/1.05 at this pose
+    assert abs(np.rad2deg(r.dth) + 9) < 2 and abs(r.dsg + np.log(1.05)) < 0.03
+
+
+def test_rs_known_answers(golden):
+    d = np.load(golden / "landsat_b.npz")
+    truth = d["truth"]
+    with zc.Registrar(half=False) as reg:
+        reg.set_images(d["moving"].astype(np.float32) / 255, d["fixed"].astype(np.float32) / 255, preprocess=False)
+        c = reg.rs_map(truth, return_maps=False).center
+        r = reg.rs_map(turned(c, 6.0, 1.08, truth))
+        assert abs(-np.rad2deg(r.dth) - 6) < 2 and abs(np.exp(-r.dsg) - 1.08) < 0.03
+        t = reg.rs_map(truth, return_maps=False)
+        assert abs(t.dth) < 0.02 and abs(t.dsg) < 0.02
+
+
+def test_rs_one_sided_and_scale_mask():
+    m, f, H = synth.pair_remap(n=128, shift=(3, 2), seed=3)
+    with zc.Registrar(half=False, rs_smin=0.9, rs_smax=1.1) as reg:
+        reg.set_images(m, f, preprocess=False)
+        one = reg.rs_map(H, symmetric=False)
+        assert not one.symmetric and one.inv is None
+        np.testing.assert_array_equal(np.isnan(one.map), False)
+        k = np.arange(one.n)
+        k = np.where(k > one.n // 2, k - one.n, k)
+        sg = -k * one.dlam
+        masked = (sg < np.log(0.9) - 1e-6) | (sg > np.log(1.1) + 1e-6)
+        inside = (sg > np.log(0.9) + 1e-6) & (sg < np.log(1.1) - 1e-6)
+        assert (one.map[masked] == 0).all() and (one.map[inside] != 0).any()
+        # without the inverse-frame map the finished map is the forward map, masked
+        np.testing.assert_array_equal(one.map[inside], one.fwd[inside])

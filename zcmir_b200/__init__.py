@@ -21,8 +21,8 @@ import numpy as np
 from . import _native
 
 __all__ = [
-    "Registrar", "ShiftMap", "Score", "Gradient", "Climb", "Search",
-    "shift_map", "score", "refine", "register", "register_stack", "stack_maps", "search", "settings", "close",
+    "Registrar", "ShiftMap", "RotoScaleMap", "Score", "Gradient", "Climb", "Search",
+    "shift_map", "rs_map", "score", "refine", "register", "register_stack", "stack_maps", "search", "settings", "close",
     "Registration", "StackRegistration", "__version__",
 ]
 
@@ -101,6 +101,30 @@ class Search:
     improved: bool
     count_a: int
     count_b: int
+
+
+@dataclass
+class RotoScaleMap:
+    """Score over every rotation and scale of the moving image about a centre (fixed pixels,
+    1-based). map / fwd / inv: n × n, columns θ (n_th of them over 2π), rows log radius (Δλ each),
+    lag 0 at [0, 0]; dth, dsg: the peak as the rotation (rad) and log scale that correct the pose."""
+    peak: float
+    dth: float
+    dsg: float
+    zero: float
+    center: tuple
+    n: int
+    n_th: int
+    n_lam: int
+    dlam: float
+    r0: float
+    r1: float
+    symmetric: bool
+    calibrated: bool
+    map: np.ndarray | None = None
+    fwd: np.ndarray | None = None
+    inv: np.ndarray | None = None
+    peak_index: int = 0
 
 
 @dataclass
@@ -333,6 +357,26 @@ class Registrar:
                          peak_index=r.peak_index) for r in out]
         return maps, ms.value
 
+    def rs_map(self, H=None, *, center=None, symmetric=True, return_maps=True):
+        """Roto-scale map at H about center (fixed pixels, 1-based; default the moving image's
+        centroid under H); the settings decide the score and the resolution (map_res)."""
+        a, p = self._Hp(H)
+        res = int(self.settings["map_res"])
+        n_max = 512 if res == 0 else min(res, 8192)  # the auto plan stays within 512 angles
+        cap = n_max * n_max if return_maps else 0
+        bufs = [np.empty(cap, np.float32) if return_maps else None for _ in range(3)]
+        ptr = [_fp(b) if b is not None else None for b in bufs]
+        c = (ctypes.c_double * 2)(*center) if center is not None else None
+        r = _native.RsResult()
+        self._check(self._lib.zc_rs_map(self._e, p, c, 1 if symmetric else 0, ctypes.byref(r), ptr[0], ptr[1],
+                                        ptr[2] if symmetric else None, cap), "rs_map")
+        nn = r.n * r.n
+        get = lambda b: b[:nn].reshape(r.n, r.n).copy() if b is not None else None
+        return RotoScaleMap(peak=r.peak, dth=r.dth, dsg=r.dsg, zero=r.zero, center=(r.cx, r.cy), n=r.n, n_th=r.n_th,
+                            n_lam=r.n_lam, dlam=r.dlam, r0=r.r0, r1=r.r1, symmetric=bool(r.symmetric),
+                            calibrated=bool(r.calibrated), map=get(bufs[0]), fwd=get(bufs[1]),
+                            inv=get(bufs[2]) if symmetric else None, peak_index=r.peak_index)
+
     def canvas(self, H=None, inverse=False):
         a, p = self._Hp(H)
         c = _native.Canvas()
@@ -435,6 +479,6 @@ class Registrar:
 
 
 from .api import (  # noqa: E402
-    Registration, StackRegistration, close, refine, register, register_stack, score, search, settings, shift_map,
-    stack_maps,
+    Registration, StackRegistration, close, refine, register, register_stack, rs_map, score, search, settings,
+    shift_map, stack_maps,
 )

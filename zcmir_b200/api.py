@@ -127,6 +127,14 @@ def shift_map(moving, fixed, H=None, *, preprocess=True, **settings):
         return reg.shift_map(np.eye(3) if H is None else np.asarray(H, np.float64))
 
 
+def rs_map(moving, fixed, H=None, *, center=None, symmetric=True, preprocess=True, **settings):
+    """The score at every rotation and scale of the moving image about pose H (default: identity)
+    and a centre (default: the moving image's centroid under H)."""
+    with _LOCK:
+        reg, *_ = _prepare(moving, fixed, preprocess, settings)
+        return reg.rs_map(np.eye(3) if H is None else np.asarray(H, np.float64), center=center, symmetric=symmetric)
+
+
 def score(moving, fixed, H, *, preprocess=True, **settings):
     """The registration score at pose H (the mean of both directions when symmetric)."""
     with _LOCK:

@@ -28,6 +28,21 @@ __host__ __device__ constexpr int tri_kc(int i, int j) {
     return (i < j ? i : j) * 4 - ((i < j ? i : j) * ((i < j ? i : j) + 1)) / 2 + (i < j ? j : i);
 }
 
+// The score's parameters for the shifts of row y of an ny-row map: a log-polar map scales row
+// y's sums by e^{kΔλ}·Δλ·Δθ (k the row's wrapped log-radius lag, smi.wgsl:777-795 extract_pair).
+__device__ __forceinline__ CombineParams row_params(const CombineParams& cp, int y, int ny) {
+    CombineParams r = cp;
+    if (cp.lp_dlam != 0.0) {
+        const int k = y <= ny / 2 ? y : y - ny;
+        r.inv_nn = cp.inv_nn * exp((double)k * cp.lp_dlam) * cp.lp_dlam * cp.lp_dth;
+    }
+    return r;
+}
+// the zero-lag overlap in the map's units (row 0 of a log-polar map carries Δλ·Δθ)
+__device__ __forceinline__ double lag0_units(const CombineParams& cp, double n00) {
+    return cp.lp_dlam != 0.0 ? n00 * cp.lp_dlam * cp.lp_dth : n00;
+}
+
 // Per-shift score (smi.wgsl:825-915, combine_cell) in float64 with every index known at compile
 // time (NF features, exact or global whitening, calibrated or not), so the 4×4 algebra stays in
 // registers. `get(slot)` returns this shift's (unscaled) sum of the plan's slot `slot`; the

@@ -94,6 +94,7 @@ Engine::~Engine() {
     for (auto& s : stack_)
         for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack}) b->release();
     stack_res_.release();
+    for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_}) b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);
 }

@@ -8,6 +8,7 @@
 #include <deque>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/zcmir.h"
@@ -101,6 +102,20 @@ struct ScoredPose {
 // planes when `three` (src/smi.zig:90-158).
 CorrPlanDev corr_plan_dev(bool exact, bool three);
 
+// One direction's roto-scale map plan (src/smi.zig RsPlan).
+struct RsPlan {
+    int n = 0, n_th = 0, n_lam = 0;
+    double log0 = 0, span = 0, dlam = 0, dth = 0, r0 = 0, r1 = 0, cx = 0, cy = 0;
+};
+
+// Swaps two sides for the life of the object (the map code works on side[0], side[1]).
+struct SideSwap {
+    Side& a;
+    Side& b;
+    SideSwap(Side& x, Side& y) : a(x), b(y) { std::swap(a, b); }
+    ~SideSwap() { std::swap(a, b); }
+};
+
 // Stages of a map timed by the profiler / the benchmark entry point.
 enum Stage { kCanvas = 0, kFwdRows, kFwdCols, kInvCols, kInvRows, kNumStages };
 extern const char* const kStageNames[kNumStages];
@@ -148,6 +163,13 @@ class Engine {
     // a map's result from its best key (score bits, inverted index), zero-lag score and the
     // pair's correlation area
     void map_result(const MapJob& job, unsigned long long best, float zero, double area, zc_shift_result* out);
+    // roto-scale map (engine_rs.cpp): pose H about c (fixed pixels, 1-based; null: the moving
+    // image's centroid under H); symmetric: with the inverse-frame map. Optional host outputs
+    // (len ≥ n²): the finished map, the raw forward and inverse maps.
+    bool rs_map(const Mat3& H, const double* c, bool symmetric, zc_rs_result* out, float* map, float* fwd, float* inv,
+                size_t len);
+    bool rs_map_one(const Mat3& H, const double c[2], double r0, double r1, bool exact, bool calibrated, unsigned cap,
+                    DevBuf& dst, RsPlan& p);
     // maps along a stack (engine_stack.cpp): each slice's features once, then slice k (moving)
     // against slice k − 1 (fixed) at priors[k − 1] for k = 1..n−1; ms: device time of it all
     bool stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,
@@ -197,6 +219,7 @@ class Engine {
     DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
+    DevBuf rs_fwd_, rs_inv_, rs_map_;
     std::vector<Side> stack_;
     DevBuf stack_res_;
     DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;

@@ -13,18 +13,6 @@
 
 namespace zc {
 
-namespace {
-
-// Swaps two sides for the life of the object (the engine's map code works on side[0], side[1]).
-struct SideSwap {
-    Side& a;
-    Side& b;
-    SideSwap(Side& x, Side& y) : a(x), b(y) { std::swap(a, b); }
-    ~SideSwap() { std::swap(a, b); }
-};
-
-}  // namespace
-
 bool Engine::stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors,
                         bool exact, bool calibrated, unsigned cap, zc_shift_result* out, float* ms) {
     if (n < 2) return fail("stack_maps: a stack needs at least 2 slices");

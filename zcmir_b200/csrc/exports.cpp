@@ -187,8 +187,9 @@ int32_t zc_shift_map_set(zc_engine* e, const double H[9], zc_shift_result* out, 
     return guarded(e, "shift_map", [&] { return e->shift_map_settings(mat(H), out, map, map_len); });
 }
 
-int32_t zc_rs_map(zc_engine* e, const double*, const double*, uint32_t, zc_rs_result*, float*, float*, float*, size_t) {
-    return unsupported(e, "rs_map");
+int32_t zc_rs_map(zc_engine* e, const double H[9], const double* c, uint32_t symmetric, zc_rs_result* out, float* map,
+                  float* fwd, float* inv, size_t len) {
+    return guarded(e, "rs_map", [&] { return e->rs_map(mat(H), c, symmetric != 0, out, map, fwd, inv, len); });
 }
 
 void zc_set_pose(zc_engine* e, const double H[9]) {

@@ -42,6 +42,9 @@ struct CombineParams {
     double area;     // feature correlation area in cells (calibrated z)
     double ridge;
     double inv_nn;   // 1/(nx·ny): the inverse FFT's scale
+    // log-polar maps: each correlation at log-radius lag k (row k, wrapped) is scaled by
+    // e^{kΔλ}·Δλ·Δθ so the sums integrate dest area; 0 for shift maps
+    double lp_dlam = 0, lp_dth = 0;
 };
 
 // Correlation plan on the device: plane numbers per slot, and per correlation slot its
@@ -109,6 +112,14 @@ cudaError_t sweep_pack(const float4* il, int sw, int sh, const float* poses, int
 // the n_peak best lane maxima of each map (map b at maps + b·map_stride) into slots slot0..
 cudaError_t sweep_peaks(const float* maps, int nx, int ny, size_t map_stride, int batch, int n_peak, int slot0,
                         float* ps, uint32_t* pi, cudaStream_t st);
+
+// ── the roto-scale map (rs.cu) ──
+// canvas stack (5 planes, W × Hh) → log-polar grid [5][n_lam][n_th] about (cx, cy), ρ-weighted
+cudaError_t rs_logpolar(const float* canvas, int W, int Hh, float cx, float cy, float log0, float span, int n_th,
+                        int n_lam, float* grid, cudaStream_t st);
+// symmetric average (inv may be null), scale mask, argmax key and lag-0 cell of an n × n map
+cudaError_t rs_finish(const float* fwd, const float* inv, bool mirror, int n, float dlam, float lo, float hi,
+                      float* out, unsigned long long* best, float* zero, cudaStream_t st);
 
 // ── pose scores and gradients (pose.cu) ──
 struct PoseSide {

@@ -305,11 +305,12 @@ __global__ void __launch_bounds__(512, 1) k_inv_rows(const float2* __restrict__ 
         }
         __syncthreads();
     }
-    const double n00 = *n00p;
+    const double n00 = lag0_units(cp, *n00p);
+    const CombineParams cpr = row_params(cp, y, (int)(pstride / WP));
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
     for (int m = threadIdx.x; m < L; m += blockDim.x) {
-        const float sc = combine_t<NF, EXACT, CALIB>([&](int k) { return corr[(size_t)k * L + m]; }, cp, n00);
+        const float sc = combine_t<NF, EXACT, CALIB>([&](int k) { return corr[(size_t)k * L + m]; }, cpr, n00);
         const int x = m * S + s;
         const uint32_t idx = (uint32_t)y * (uint32_t)nx + (uint32_t)x;
         map[idx] = sc;
@@ -397,13 +398,14 @@ __global__ void __launch_bounds__(512, 1) k_rows_multi(const float2* __restrict_
         }
         __syncthreads();
     }
-    const double n00 = *n00p;
+    const double n00 = lag0_units(cp, *n00p);
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
     for (int m = threadIdx.x; m < rows * nx; m += blockDim.x) {
         const int r = m / nx, x = m - r * nx;
         const float* c = corr + (size_t)r * plan.n_corr * nx + x;
-        const float sc = combine_t<NF, EXACT, CALIB>([&](int k) { return c[(size_t)k * nx]; }, cp, n00);
+        const float sc =
+            combine_t<NF, EXACT, CALIB>([&](int k) { return c[(size_t)k * nx]; }, row_params(cp, y0 + r, ny), n00);
         const uint32_t idx = (uint32_t)(y0 + r) * (uint32_t)nx + (uint32_t)x;
         map[idx] = sc;
         if (sc > bv || (sc == bv && idx < bi)) {
