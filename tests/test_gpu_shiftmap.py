@@ -172,8 +172,8 @@ def test_errors_and_boundaries():
             reg.set_moving(np.zeros((4, 64), np.float32), preprocess=False)
         with pytest.raises(RuntimeError, match="UnknownSetting"):
             reg.configure(nope=1)
-        with pytest.raises(RuntimeError, match="preprocess"):
-            reg.set_moving(np.zeros((64, 64), np.float32), preprocess=True)
+        with pytest.raises(ValueError, match="always preprocessed"):
+            reg.set_moving(np.zeros((64, 64), np.uint8), preprocess=False)
         m, f, _ = synth.pair_remap(n=64, seed=9)
         reg.set_images(m, f, preprocess=False)
         small = np.empty(16, np.float32)

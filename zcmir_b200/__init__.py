@@ -213,8 +213,7 @@ class Registrar:
         """A contiguous float32 gray image (uint16 scaled to [0, 1], RGB(A) to luma)."""
         a = np.asarray(img)
         if a.dtype == np.uint8:
-            raise ValueError("uint8 images are always preprocessed (CLAHE), which this build leaves out: "
-                             "pass float gray in [0, 1] (or uint16) with preprocess=False")
+            a = a.astype(np.float32) / np.float32(255)
         if a.ndim == 3 and a.shape[2] in (3, 4):
             a = a[:, :, :3].astype(np.float64) @ np.array([0.299, 0.587, 0.114])
         if a.dtype == np.uint16:
@@ -226,7 +225,23 @@ class Registrar:
         return a
 
     def _set(self, side, img, preprocess):
-        a = self._gray(img)
+        """python/zcmir/__init__.py:283-307: uint8 images (gray, RGB or RGBA) go up as RGBA8 and are
+        always preprocessed; other images as float gray, preprocessed when asked."""
+        a = np.asarray(img)
+        if a.dtype == np.uint8:
+            if a.ndim == 2:
+                a = np.repeat(a[:, :, None], 3, axis=2)
+            if a.ndim != 3 or a.shape[2] not in (3, 4):
+                raise ValueError("uint8 images: (h, w), (h, w, 3) or (h, w, 4)")
+            if a.shape[2] == 3:
+                a = np.concatenate([a, np.full(a.shape[:2] + (1,), 255, np.uint8)], axis=2)
+            a = np.ascontiguousarray(a)
+            h, w = a.shape[:2]
+            if not preprocess:
+                raise ValueError("uint8 images are always preprocessed (pass float gray to skip it)")
+            return self._check(self._lib.zc_set_image_rgba(self._e, side, a.ctypes.data_as(_native.u8p), w, h),
+                               "set_image")
+        a = self._gray(a)
         h, w = a.shape
         rc = self._lib.zc_set_image_gray(self._e, side, _fp(a), w, h, 1 if preprocess else 0)
         self._check(rc, "set_image")

@@ -64,6 +64,7 @@ SIGS = {
     "zc_settings": ([P, ctypes.c_char_p, SZ], SZ),
     "zc_set_image": ([P, U32, f32p, U32, U32], I32),
     "zc_set_image_gray": ([P, U32, f32p, U32, U32, U32], I32),
+    "zc_set_image_rgba": ([P, U32, u8p, U32, U32], I32),
     "zc_work_image": ([P, U32, f32p, SZ], I32),
     "zc_features": ([P, U32, f32p, SZ], I32),
     "zc_moments": ([P, f64p, f64p], I32),

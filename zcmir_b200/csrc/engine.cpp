@@ -94,7 +94,7 @@ Engine::~Engine() {
     for (auto& s : stack_)
         for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack}) b->release();
     stack_res_.release();
-    for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_}) b->release();
+    for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_}) b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);
 }
@@ -114,10 +114,6 @@ bool Engine::cuda_ok(cudaError_t e, const char* what) {
 bool Engine::set_image(int s, const float* data, int w, int h, bool preprocess) {
     // the reference's setImageGray checks (src/engine.zig:430-434)
     if (s < 0 || s > 1 || w < 8 || h < 8 || !data) return fail("set_image_gray: BadImage");
-    if (preprocess && (set.b("clahe") || set.b("band") || set.b("invert")))
-        return fail(
-            "set_image_gray: preprocessing (CLAHE, band pass, invert) is not part of this build's SMI path; "
-            "pass preprocess=False, or configure clahe=false, band=false, invert=false");
     Side& sd = side[s];
     const size_t n = (size_t)w * h;
     if (!cuda_ok(sd.raw.ensure(n * 4), "set_image_gray")) return false;
@@ -128,6 +124,82 @@ bool Engine::set_image(int s, const float* data, int w, int h, bool preprocess) 
     sd.preprocess = preprocess;
     sd.built = false;
     return build_side(s);
+}
+
+bool Engine::set_image_rgba(int s, const unsigned char* rgba, int w, int h) {
+    if (s < 0 || s > 1 || w < 8 || h < 8 || !rgba) return fail("set_image_rgba: BadImage");
+    Side& sd = side[s];
+    const size_t n = (size_t)w * h;
+    if (!cuda_ok(pp_rgba_.ensure(n * 4), "set_image_rgba") || !cuda_ok(sd.raw.ensure(n * 4), "set_image_rgba") ||
+        !cuda_ok(cudaMemcpyAsync(pp_rgba_.p, rgba, n * 4, cudaMemcpyHostToDevice, st), "set_image_rgba") ||
+        !cuda_ok(rgba_to_gray(pp_rgba_.as<unsigned char>(), (int)n, sd.raw.as<float>(), st), "set_image_rgba"))
+        return false;
+    counts[0] += 1;
+    sd.has = true;
+    sd.w = w;
+    sd.h = h;
+    sd.preprocess = true;
+    sd.built = false;
+    return build_side(s);
+}
+
+std::string Engine::bake_key() const {
+    char b[160];
+    snprintf(b, sizeof b, "%d %u %u %d %.17g %.17g %d %d", set.b("clahe"), set.u("clahe_grid"), set.u("clahe_bins"),
+             set.b("band"), set.f("bp_fine"), set.f("bp_coarse"), set.b("invert"), set.b("half"));
+    return b;
+}
+
+bool Engine::bake(int s) {
+    Side& sd = side[s];
+    const int n = sd.w * sd.h;
+    const bool half = set.b("half");
+    float* work = sd.work.as<float>();
+    sd.bake = sd.preprocess ? bake_key() : std::string();
+    if (!sd.preprocess) return cuda_ok(cudaMemcpyAsync(work, sd.raw.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "features");
+    // CLAHE (clip limit 40, the settings' grid and bins) from the f32 image, else its texels
+    if (set.b("clahe")) {
+        if (!cuda_ok(pp_clahe_.ensure(clahe_scratch_bytes((int)set.u("clahe_grid"), (int)set.u("clahe_bins"))), "clahe") ||
+            !cuda_ok(clahe(sd.raw.as<float>(), sd.w, sd.h, 40.0, (int)set.u("clahe_bins"), (int)set.u("clahe_grid"), half,
+                           pp_clahe_.p, work, st),
+                     "clahe"))
+            return false;
+        counts[0] += 3;
+    } else {
+        if (!cuda_ok(cudaMemcpyAsync(work, sd.raw.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "features")) return false;
+        if (half && !cuda_ok(round_texels(work, n, st), "features")) return false;
+    }
+    if (set.b("band")) {
+        // difference of Gaussians: fine = blur^f, coarse = blur^(c − f) of fine (src/gls.zig:531-557)
+        const double fp = set.f("bp_fine") > 0 ? set.f("bp_fine") : 1.0;
+        const double cp = set.f("bp_coarse") > 0 ? set.f("bp_coarse") : 6.0;
+        const int fine_n = (int)std::max(1.0, std::min(16.0, std::round(fp * fp)));
+        const int coarse_n = std::max(fine_n + 1, (int)std::min(64.0, std::round(cp * cp)));
+        if (!cuda_ok(pp_tmp_.ensure((size_t)n * 4 * 5), "band") || !cuda_ok(pp_mm_.ensure(8), "band")) return false;
+        float* t = pp_tmp_.as<float>();
+        float *mid = t, *ping = t + n, *fine = t + 2 * (size_t)n, *coarse = t + 3 * (size_t)n, *d = t + 4 * (size_t)n;
+        auto passes = [&](const float* src, float* dst, int k) {
+            const float* from = src;
+            for (int i = 0; i < k; ++i) {
+                float* to = (i == k - 1) ? dst : ping;
+                if (to == from) to = (from == ping) ? d : ping;
+                if (!cuda_ok(gauss_blur(from, sd.w, sd.h, half, mid, to, st), "band")) return false;
+                counts[0] += 2;
+                from = to;
+            }
+            if (from != dst) return cuda_ok(cudaMemcpyAsync(dst, from, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "band");
+            return true;
+        };
+        if (!passes(work, fine, fine_n) || !passes(fine, coarse, coarse_n - fine_n) ||
+            !cuda_ok(dog_rescale(fine, coarse, n, half, d, pp_mm_.as<unsigned>(), work, st), "band"))
+            return false;
+        counts[0] += 2;
+    }
+    if (set.b("invert")) {
+        if (!cuda_ok(invert_texels(work, n, half, st), "invert")) return false;
+        counts[0] += 1;
+    }
+    return true;
 }
 
 bool Engine::build_side(int s) {
@@ -150,7 +222,7 @@ bool Engine::build_side(int s) {
     fs_.acf_part = fs_acfpart_.as<float>();
     fs_.acf_part_cap = fs_acfpart_.cap / 4;
     fs_.acf = fs_acf_.as<double>();
-    if (!cuda_ok(cudaMemcpyAsync(sd.work.p, sd.raw.p, n * 4, cudaMemcpyDeviceToDevice, st), "features")) return false;
+    if (!bake(s)) return false;
     if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rank_tmp_.as<float>(), sd.feat.as<float>(),
                                 sd.mag.as<float>(), sd.stack.as<float>(), fs_, st),
                  "features"))
@@ -175,7 +247,7 @@ bool Engine::need_images() {
     const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
     for (int s = 0; s < 2; ++s) {
         Side& sd = side[s];
-        if (!sd.built || sd.mode != mode || sd.half != set.b("half"))
+        if (!sd.built || sd.mode != mode || sd.half != set.b("half") || (sd.preprocess && sd.bake != bake_key()))
             if (!build_side(s)) return false;
     }
     return true;

@@ -44,6 +44,7 @@ struct Side {
     bool built = false;
     int mode = -1;
     bool half = false;
+    std::string bake;  // the preprocessing settings the work image was made with
 };
 
 // Scores (and optionally the symmetric gradient and Gauss–Newton matrix) at one pose.
@@ -149,6 +150,8 @@ class Engine {
 
     // images and features
     bool set_image(int s, const float* data, int w, int h, bool preprocess);
+    // RGBA8 → gray (0.299 R + 0.587 G + 0.114 B), always preprocessed (src/engine.zig:422-426)
+    bool set_image_rgba(int s, const unsigned char* rgba, int w, int h);
     bool need_images();
     bool features(int s, float* out, size_t len);
     bool work_image(int s, float* out, size_t len);
@@ -212,6 +215,10 @@ class Engine {
 
   private:
     bool build_side(int s);
+    // the work image of side s from its raw image: CLAHE, band pass, invert as set (preprocessed
+    // sides), else the raw image as is
+    bool bake(int s);
+    std::string bake_key() const;
     bool line_plan(int n, LinePlan& p);
     const float2* twiddles(int n);
 
@@ -220,6 +227,7 @@ class Engine {
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
     DevBuf rs_fwd_, rs_inv_, rs_map_;
+    DevBuf pp_rgba_, pp_clahe_, pp_tmp_, pp_mm_;
     std::vector<Side> stack_;
     DevBuf stack_res_;
     DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;

@@ -134,10 +134,8 @@ int32_t zc_set_image(zc_engine* e, uint32_t side, const float* data, uint32_t w,
     return zc_set_image_gray(e, side, data, w, h, 0);
 }
 
-int32_t zc_set_image_rgba(zc_engine* e, uint32_t, const uint8_t*, uint32_t, uint32_t) {
-    if (e) e->err.clear();
-    return unsupported(e, "set_image_rgba (RGBA images are always preprocessed with CLAHE; pass float gray with "
-                          "preprocess=False)");
+int32_t zc_set_image_rgba(zc_engine* e, uint32_t side, const uint8_t* data, uint32_t w, uint32_t h) {
+    return guarded(e, "set_image_rgba", [&] { return e->set_image_rgba((int)side, data, (int)w, (int)h); });
 }
 
 int32_t zc_work_image(zc_engine* e, uint32_t side, float* out, size_t len) {

@@ -113,6 +113,19 @@ cudaError_t sweep_pack(const float4* il, int sw, int sh, const float* poses, int
 cudaError_t sweep_peaks(const float* maps, int nx, int ny, size_t map_stride, int batch, int n_peak, int slot0,
                         float* ps, uint32_t* pi, cudaStream_t st);
 
+// ── preprocessing (preprocess.cu); with `half` every output is rounded to f16 texels ──
+cudaError_t rgba_to_gray(const unsigned char* rgba, int n, float* gray, cudaStream_t st);
+size_t clahe_scratch_bytes(int grid, int bins);
+cudaError_t clahe(const float* src, int w, int h, double clip, int bins, int grid, bool half, void* scratch,
+                  float* dst, cudaStream_t st);
+// one σ = 1 Gaussian blur (rows then columns) through tmp
+cudaError_t gauss_blur(const float* src, int w, int h, bool half, float* tmp, float* dst, cudaStream_t st);
+// clamp(fine) − clamp(coarse) rescaled to [0, 1] into out; d (n floats), mm (2 u32) scratch
+cudaError_t dog_rescale(const float* fine, const float* coarse, int n, bool half, float* d, unsigned* mm, float* out,
+                        cudaStream_t st);
+cudaError_t invert_texels(float* a, int n, bool half, cudaStream_t st);
+cudaError_t round_texels(float* a, int n, cudaStream_t st);
+
 // ── the roto-scale map (rs.cu) ──
 // canvas stack (5 planes, W × Hh) → log-polar grid [5][n_lam][n_th] about (cx, cy), ρ-weighted
 cudaError_t rs_logpolar(const float* canvas, int W, int Hh, float cx, float cy, float log0, float span, int n_th,
