@@ -396,6 +396,31 @@ def correlations(planes_a, planes_b, plane_ids, corrs, nx, ny):
     return out
 
 
+def direct_sums_blocked(grid_a, grid_b, plane_ids, corrs, tx, ty, rows=256):
+    """direct_sums from the two 5-plane grids (5, h, w), the real planes formed in float64 a block
+    of rows at a time: the 45 sums at lag (tx, ty) as one 15 × 15 product per block, without
+    holding the planes of a large image."""
+    _, h, w = grid_a.shape
+    out = np.zeros(45)
+    ys, ye = max(0, -ty), min(h, h - ty)
+    xs, xe = max(0, -tx), min(w, w - tx)
+    if ye <= ys or xe <= xs:
+        return out
+    slot = {p: k for k, p in enumerate(plane_ids)}
+    P = len(plane_ids)
+    G = np.zeros((P, P))
+    for r0 in range(ys, ye, rows):
+        r1 = min(ye, r0 + rows)
+        a5 = np.asarray(grid_a[:, r0 + ty:r1 + ty, xs + tx:xe + tx], np.float64)
+        b5 = np.asarray(grid_b[:, r0:r1, xs:xe], np.float64)
+        A = real_planes(a5, plane_ids).reshape(P, -1)
+        B = real_planes(b5, plane_ids).reshape(P, -1)
+        G += A @ B.T
+    for a, b, c in corrs:
+        out[c] = G[slot[a], slot[b]]
+    return out
+
+
 def direct_sums(planes_a, planes_b, plane_ids, corrs, tx, ty):
     """The correlation sums at one lag (tx, ty) as direct float64 dot products (no FFT)."""
     slot = {p: k for k, p in enumerate(plane_ids)}
@@ -438,15 +463,17 @@ def _chol4(G, nf):
     return L, ok
 
 
-def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, ridge=RIDGE, n00=None):
-    """Per-shift score from the correlation sums (``shaders/smi.wgsl:825-915``), float64.
+def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, ridge=RIDGE, n00=None, dtype=np.float64):
+    """Per-shift score from the correlation sums (``shaders/smi.wgsl:825-915``), in float64 (or in
+    `dtype`: float32 restates the centring and Cholesky in single precision, as a precision study
+    compares).
 
     corr: (45, ...) sums (already scaled). Global: n·Σ clamp(C_ij, ±1)². Exact: n·‖L_A⁻¹ C
     L_B⁻ᵀ‖². Calibrated (exact only): the Wilson–Hilferty z of Pillai's F. Floors: n < max(min_n,
     8 % of the zero-lag n) (calibrated: n < min_n or n_eff ≤ 10) score 0; failed Cholesky and
     NaN score 0."""
     shape = corr.shape[1:]
-    c = corr.reshape(45, -1).astype(np.float64)
+    c = corr.reshape(45, -1).astype(dtype)
     n = c[0]
     calib = exact and calibrated
     neff = n / max(area, 1.0)
@@ -457,7 +484,7 @@ def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, rid
     den = np.maximum(n, 1e-8)
     ma = np.stack([c[1 + i] / den for i in range(4)])
     mb = np.stack([c[5 + i] / den for i in range(4)])
-    C = np.zeros((4, 4, c.shape[1]))
+    C = np.zeros((4, 4, c.shape[1]), dtype)
     for i in range(nf):
         for j in range(nf):
             C[i, j] = c[9 + 4 * i + j] / den - ma[i] * mb[j]
@@ -490,7 +517,7 @@ def combine(corr, exact=True, calibrated=False, min_n=MIN_N, area=1.0, nf=4, rid
                 for k in range(i):
                     s -= LA[i, k] * X[k, j]
                 X[i, j] = s / LA[i, i]
-        acc = np.zeros(c.shape[1])
+        acc = np.zeros(c.shape[1], dtype)
         for r in range(nf):
             y = [None] * nf
             for i in range(nf):

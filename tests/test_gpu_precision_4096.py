@@ -1,0 +1,94 @@
+"""The precision study at 4096² (8192² FFT): the GPU map's score at 100 lags against float64
+direct sums with a float64 score, and what float32 centring and whitening would do to the same
+exact sums.
+
+The pair is the 1024² map workload's generator at 4× the size (blob field vs its 8-level
+segmented modality, seeded shift within ±800 px, seed 4). The lags: 0, the planted one, 68
+uniform within ±70 % of the image, 30 whose overlap is 2–10 % of the image. The GPU path is the
+shipped one: FP32 FFTs, float64 centring and Cholesky per shift. Checked: the map's argmax is the
+planted lag; at every lag where neither side floors the score, the GPU score is within 1e-4 of the
+map's peak, and within 1e-3 of its own value where the overlap is at least 20 %; both sides floor
+the same lags (the 8 %-of-zero-lag floor) except within 1 % of it. The float32-centring score of
+the exact sums is reported beside it (no bound: it is the alternative this build does not take).
+
+With ZCMIR_B200_STUDY_OUT set, the per-lag table is written there as JSON."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import zcmir_b200 as zc
+from oracle import smi_oracle as O
+from zcmir_b200 import synth
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+N = 4096
+
+
+def lags(rng, planted):
+    out = [(0, 0), planted]
+    while len(out) < 70:
+        out.append(tuple(int(v) for v in rng.integers(-int(0.7 * N), int(0.7 * N) + 1, 2)))
+    while len(out) < 100:
+        phi = rng.uniform(0.02, 0.10)
+        fx = phi ** rng.uniform(0.3, 0.7)
+        fy = phi / fx
+        lx, ly = int(round(N * (1 - fx))), int(round(N * (1 - fy)))
+        out.append((lx * int(rng.choice([-1, 1])), ly * int(rng.choice([-1, 1]))))
+    return out
+
+
+def test_precision_study_4096():
+    m, f, H = synth.pair_segmented(n=N, seed=4, max_shift=800)
+    planted = (int(-H[0, 2]), int(-H[1, 2]))
+    with zc.Registrar(half=False) as reg:
+        reg.set_images(m, f, preprocess=False)
+        sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=8192)
+        fa, fb = reg.features(0), reg.features(1)
+    assert (sm.n, sm.ny, sm.cw, sm.ch) == (8192, 8192, N, N)
+    assert (sm.dx, sm.dy) == planted
+    # at the identity pose of two equal images the canvas planes are the stacks themselves, at
+    # full resolution (the oracle's map plan stops at the reference's 2048-point lines)
+    ga = np.concatenate([np.ones((1, N, N), np.float32), fa])
+    gb = np.concatenate([np.ones((1, N, N), np.float32), fb])
+    ids, corrs = O.corr_plan(True, False)
+    rng = np.random.default_rng(4)
+    L = lags(rng, planted)
+    sums = np.stack([O.direct_sums_blocked(ga, gb, ids, corrs, tx, ty) for tx, ty in L], axis=1)
+    n00 = sums[0, 0]
+    s64 = O.combine(sums, exact=True, calibrated=False, n00=n00)
+    s32 = O.combine(sums, exact=True, calibrated=False, n00=n00, dtype=np.float32).astype(np.float64)
+    gpu = np.array([sm.map[ty % sm.ny, tx % sm.n] for tx, ty in L], np.float64)
+    overlap = sums[0] / (N * N)
+    peak = float(s64.max())
+    assert gpu[1] == pytest.approx(sm.peak) and s64[1] == pytest.approx(peak)
+    both = (gpu != 0) & (s64 != 0)
+    err_peak = np.abs(gpu - s64) / peak
+    err_own = np.where(both, np.abs(gpu - s64) / np.maximum(np.abs(s64), 1e-300), 0.0)
+    err32 = np.where(s64 != 0, np.abs(s32 - s64) / np.maximum(np.abs(s64), 1e-300), 0.0)
+    # the floor: 8 % of the zero-lag overlap; only lags at its edge may fall on different sides
+    floor = 0.08 * n00
+    flip = (gpu == 0) != (s64 == 0)
+    assert np.all(np.abs(sums[0][flip] - floor) <= 0.01 * floor)
+    assert err_peak[both].max() <= 1e-4, err_peak[both].max()
+    big = both & (overlap >= 0.2)
+    assert err_own[big].max() <= 1e-3, err_own[big].max()
+    out = os.environ.get("ZCMIR_B200_STUDY_OUT")
+    if out:
+        rows = [{"lag": [int(tx), int(ty)], "overlap": float(o), "fp64": float(a), "gpu": float(g), "fp32_centring": float(b),
+                 "gpu_err_of_peak": float(e), "gpu_err_rel": float(r), "fp32_centring_err_rel": float(q)}
+                for (tx, ty), o, a, g, b, e, r, q in zip(L, overlap, s64, gpu, s32, err_peak, err_own, err32)]
+        small = both & (overlap < 0.1)
+        summary = {
+            "image": N, "fft": sm.n, "lags": len(L), "peak": peak, "argmax_gpu": [sm.dx, sm.dy], "planted": list(planted),
+            "gpu_max_err_of_peak": float(err_peak[both].max()),
+            "gpu_max_err_rel_overlap_ge_20pct": float(err_own[big].max()),
+            "gpu_max_err_rel_overlap_lt_10pct": float(err_own[small].max()) if small.any() else None,
+            "fp32_centring_max_err_rel_overlap_ge_20pct": float(err32[big].max()),
+            "fp32_centring_max_err_rel_overlap_lt_10pct": float(err32[small].max()) if small.any() else None,
+            "floored_lags_gpu": int((gpu == 0).sum()), "floored_lags_fp64": int((s64 == 0).sum()),
+        }
+        with open(out, "w") as fh:
+            json.dump({"summary": summary, "rows": rows}, fh, indent=1)

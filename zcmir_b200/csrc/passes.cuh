@@ -85,7 +85,7 @@ __device__ __forceinline__ float real_plane_row(int r, const float* row, int cw,
 // The row's 5 stack values per cell are staged in shared memory once (after the line buffers).
 // Batched over blockIdx.y: item b reads grid + b·gbs and writes half + b·hbs.
 template <class F>
-__global__ void __launch_bounds__(256, 2) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int WP,
+__global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int WP,
                                                      CorrPlanDev plan, F f, int lpb, float2* __restrict__ half,
                                                      size_t pstride, size_t gbs, size_t hbs) {
     extern __shared__ float2 smem[];
@@ -479,6 +479,7 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
     const int tl = f.tl();
     if constexpr (P == Pass::FwdRows) {
         const int n_cplx = (plan.n_real + 1) / 2;
+        // up to 256 threads of lines (one line of more for the longest rows: 8192 points, 512 threads)
         const int lines = std::min(lines_per_block(tl, 256), n_cplx);
         const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)5 * g.cw * sizeof(float);
         cudaFuncSetAttribute(k_fwd_rows<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
