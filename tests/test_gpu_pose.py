@@ -123,3 +123,28 @@ def test_climb_ascends_to_a_stationary_point(pair):
         assert np.linalg.norm(step) < 5e-3
         # the climb's final score is the pair score at its pose
         assert abs(reg.score(c.H).mean - c.score) <= 1e-9 * abs(c.score)
+
+
+def test_climb_roto_scale_hop(golden):
+    """The roto-scale hop (hop_fm, src/gclimb.zig:417-435): from the landsat-b truth turned by 8°
+    and scaled by 1.1 about the moving image's centroid, the climb takes the roto-scale map's
+    peak as a step of the pose and ends within 1 px of the truth at the corners."""
+    d = np.load(golden / "landsat_b.npz")
+    m, f, H = d["moving"].astype(np.float32) / 255, d["fixed"].astype(np.float32) / 255, d["truth"]
+    mh, mw = m.shape
+    c = np.mean([(H @ [x, y, 1.0])[:2] for x, y in [(1, 1), (mw, 1), (mw, mh), (1, mh)]], axis=0)
+    a, s = np.deg2rad(8.0), 1.1
+    R = np.array([[s * np.cos(a), -s * np.sin(a), 0], [s * np.sin(a), s * np.cos(a), 0], [0, 0, 1]])
+    T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
+    start = T(*c) @ R @ T(*-c) @ H
+    assert corner_dist(start, H, mw, mh) > 30
+    with zc.Registrar(half=False, group="affine", hop_fm=True) as reg:
+        reg.set_images(m, f, preprocess=False)
+        reg.pose = start
+        r = reg.climb()
+        ev = reg.events()
+    labels = [e.get("label") for e in ev if e["kind"] == "trail"]
+    logs = [e.get("text", "") for e in ev if e["kind"] == "log"]
+    assert "roto-scale hop" in labels, labels
+    assert any("roto-scale hop+" in t for t in logs), logs
+    assert corner_dist(r.H, H, mw, mh) < 1.0, corner_dist(r.H, H, mw, mh)

@@ -50,7 +50,7 @@ __device__ __forceinline__ double lag0_units(const CombineParams& cp, double n00
 // to it is a compile-time constant. Each Cholesky pivot is inverted once (rsqrt) and the
 // substitutions multiply by it.
 template <int NF, bool EXACT, bool CALIB, class G>
-__device__ __forceinline__ float combine_t(G&& get, const CombineParams& p, double n00) {
+__device__ __forceinline__ float combine_smi(G&& get, const CombineParams& p, double n00) {
     constexpr bool THREE = NF == 3;
     auto S = [&](int c) -> double { return (double)get(corr_slot(c, THREE)) * p.inv_nn; };
     const double n = S(0);
@@ -158,6 +158,23 @@ __device__ __forceinline__ float combine_t(G&& get, const CombineParams& p, doub
         score = fmax(z, 0.0);
     }
     return (score == score) ? (float)score : 0.f;
+}
+
+// The NCC map's value at a lag (src/overlay.zig:256-258): the mean-free correlation over the
+// product of the planes' norms (den, carried in the n00 slot), clamped to ±1.5.
+template <class G>
+__device__ __forceinline__ float combine_ncc(G&& get, const CombineParams& p, double den) {
+    const double v = (double)get(0) * p.inv_nn / den;
+    return (float)fmin(1.5, fmax(-1.5, v));
+}
+
+// NF = 1 selects the NCC map, 3 or 4 the SMI score over that many features.
+template <int NF, bool EXACT, bool CALIB, class G>
+__device__ __forceinline__ float combine_t(G&& get, const CombineParams& p, double n00) {
+    if constexpr (NF == 1)
+        return combine_ncc(get, p, n00);
+    else
+        return combine_smi<NF, EXACT, CALIB>(get, p, n00);
 }
 
 }  // namespace zc

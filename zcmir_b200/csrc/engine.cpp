@@ -344,8 +344,7 @@ bool Engine::line_plan(int n, LinePlan& p) {
 
 bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap, double min_overlap, MapJob& job) {
     if (!need_images()) return false;
-    if (set.e("metric") != "smi")
-        return fail("shift_map: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    if (!metric_ok("shift_map")) return false;
     const bool ladder = set.e("fft_sizes") == "ladder";
     if (!ladder) return fail("shift_map: fft_sizes=\"compact\" is not supported by this build (use \"ladder\")");
     job.exact = exact;
@@ -528,6 +527,8 @@ void Engine::map_result(const MapJob& job, unsigned long long best, float zero, 
 }
 
 bool Engine::shift_map_settings(const Mat3& Hm, zc_shift_result* out, float* map, size_t map_len) {
+    if (!metric_ok("shift_map")) return false;
+    if (set.e("metric") == "ncc") return ncc_shift_map(Hm, out, map, map_len);
     // mapOpts (src/engine.zig:287-293)
     return shift_map(Hm, set.b("exact"), set.b("calibrated"), set.u("map_res"), set.f("min_overlap"), out, map, map_len);
 }

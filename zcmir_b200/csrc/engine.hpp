@@ -171,8 +171,22 @@ class Engine {
     // (len ≥ n²): the finished map, the raw forward and inverse maps.
     bool rs_map(const Mat3& H, const double* c, bool symmetric, zc_rs_result* out, float* map, float* fwd, float* inv,
                 size_t len);
+    // the one-sided roto-scale map's peak at H about c as the rotation (rad) and log scale
+    // that correct the pose (the climb's roto-scale hop)
+    bool rs_peak(const Mat3& H, const double c[2], double* dth, double* dsg);
+    // the moving image's centroid under H: the mean of its four mapped corners (src/lie.zig
+    // movingCentroid), the roto-scale map's default centre
+    void rs_center(const Mat3& H, double c[2]) const;
     bool rs_map_one(const Mat3& H, const double c[2], double r0, double r1, bool exact, bool calibrated, unsigned cap,
                     DevBuf& dst, RsPlan& p);
+    // the NCC overlay metric (engine_ncc.cpp): the zero-lag NCC of the pair's union canvas at H,
+    // and the NCC of every shift as a map; zc_score and zc_shift_map return these when the
+    // settings' metric is "ncc"
+    bool ncc_score(const Mat3& H, double* out);
+    bool ncc_shift_map(const Mat3& H, zc_shift_result* out, float* map, size_t map_len);
+    // fails unless the settings' metric is one this build has: "smi", or "ncc" (whose pose
+    // gradients, climb, sweep-free maps and roto-scale maps are SMI's, as in the reference)
+    bool metric_ok(const char* what);
     // maps along a stack (engine_stack.cpp): each slice's features once, then slice k (moving)
     // against slice k − 1 (fixed) at priors[k − 1] for k = 1..n−1; ms: device time of it all
     bool stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,

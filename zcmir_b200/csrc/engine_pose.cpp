@@ -51,8 +51,7 @@ void Engine::log_event(const std::string& text) { events.push_back("{\"kind\":\"
 bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::vector<PoseEval>& out,
                         bool forward_only) {
     if (!need_images()) return false;
-    if (set.e("metric") != "smi")
-        return fail("score: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    if (!metric_ok("score")) return false;
     const bool sym = set.b("symmetric") && !forward_only, homog = set.e("group") == "homography", exact = set.b("exact");
     const int n = (int)Hs.size(), nd = sym ? 2 : 1, nk = n_keys(homog);
     if (n == 0) return true;
@@ -177,6 +176,15 @@ bool Engine::moments(const Mat3& Hm, double* out45) {
 }
 
 bool Engine::score3(const Mat3& Hm, double* out3) {
+    if (!metric_ok("score")) return false;
+    if (set.e("metric") == "ncc") {
+        // the NCC metric's score is one-sided (src/engine.zig:752-758): mean = forward, no inverse
+        double s;
+        if (!ncc_score(Hm, &s)) return false;
+        out3[0] = out3[1] = s;
+        out3[2] = std::nan("");
+        return true;
+    }
     std::vector<PoseEval> r;
     if (!eval_poses({Hm}, false, false, r)) return false;
     out3[0] = r[0].mean;
@@ -210,11 +218,11 @@ bool Engine::gradient(const Mat3& Hm, bool hess, zc_grad_result* out) {
 bool Engine::climb(zc_climb_result* out) {
     if (!need_images()) return false;
     const bool sym = set.b("symmetric"), homog = set.e("group") == "homography", hop = set.b("hop");
+    const bool hop_fm = set.b("hop_fm"), hops = hop || hop_fm;
     const unsigned n_iters = std::max(1u, set.u("g_iters"));
     const int nk = n_keys(homog);
     const double rw = side[1].w, rh = side[1].h;
     if (set.b("ffd")) log_event("the spline stage is not part of this build; refining the homography only");
-    if (set.b("hop_fm")) log_event("the roto-scale hop is not part of this build; skipped");
     // a candidate beats the current score when higher by more than 1e-6 of it (pair.zig beats)
     auto beats = [](double nw, double old) { return nw > old + std::max(1e-6 * std::fabs(old), 1e-12); };
     std::vector<PoseEval> ev;
@@ -223,11 +231,12 @@ bool Engine::climb(zc_climb_result* out) {
     PoseEval cur = ev[0];
     const double s_start = cur.mean;
     char buf[256];
-    snprintf(buf, sizeof buf, "ascent %s score %.4f %s%sGauss–Newton (B200)", homog ? "homography" : "affine", s_start,
-             sym ? "mean " : "", hop ? "shift hop+" : "");
+    snprintf(buf, sizeof buf, "ascent %s score %.4f %s%s%sGauss–Newton (B200)", homog ? "homography" : "affine",
+             s_start, sym ? "mean " : "", hop ? "shift hop+" : "", hop_fm ? "roto-scale hop+" : "");
     log_event(buf);
     cancel = false;
     unsigned iter = 0, stall = 0, n_rec = 0;
+    double c[2] = {0, 0};
     // one stage: candidates and the current pose scored together; the best that beats the
     // current pose's fresh score becomes the pose, with its gradient (climb_select)
     auto stage = [&](const std::vector<Mat3>& cands, const char* label, const std::vector<double>& mus, bool& moved) {
@@ -272,12 +281,14 @@ bool Engine::climb(zc_climb_result* out) {
         if (hop) {
             // shift hop: the map's peak as a translation of the pose (hop_cand)
             zc_shift_result r;
-            if (!shift_map_settings(H, &r, nullptr, 0)) return false;
+            if (!shift_map(H, set.b("exact"), set.b("calibrated"), set.u("map_res"), set.f("min_overlap"), &r, nullptr, 0))
+                return false;
             bool moved = false;
             if (!stage({mul3(translate(-r.dx, -r.dy), H)}, "shift hop", {}, moved)) return false;
             moved_any |= moved;
         }
         // up to three Gauss–Newton steps; one that beats nothing ends the block (gn_cands)
+        auto gn_block = [&]() {
         for (int step = 0; step < 3; ++step) {
             double A[64], b[8], x[8] = {0};
             for (int i = 0; i < nk; ++i) {
@@ -303,6 +314,27 @@ bool Engine::climb(zc_climb_result* out) {
             moved_any |= moved;
             if (!moved) break;
         }
+        return true;
+        };
+        // the Gauss–Newton block follows the shift hop, and the roto-scale hop when it runs alone
+        if ((hop || !hop_fm) && !gn_block()) return false;
+        if (hop_fm) {
+            // roto-scale hop (rs_cand): the one-sided roto-scale map's peak about the moving
+            // image's centroid as a rotation and scale of the pose, then a fresh GN block; the
+            // centre is the one of the pose that each batch of 8 iterations starts from
+            if (iter % 8 == 0) rs_center(H, c);
+            double dth = 0, dsg = 0;
+            if (!rs_peak(H, c, &dth, &dsg)) return false;
+            if (!(std::fabs(dth) < 2e-4 && std::fabs(dsg) < 2e-4)) {
+                const double sc = std::exp(dsg), a = sc * std::cos(dth), b = -sc * std::sin(dth);
+                const double d = sc * std::sin(dth), e = sc * std::cos(dth);
+                const Mat3 S = {a, b, c[0] - a * c[0] - b * c[1], d, e, c[1] - d * c[0] - e * c[1], 0, 0, 1};
+                bool moved = false;
+                if (!stage({project_group(mul3(S, H), homog)}, "roto-scale hop", {}, moved)) return false;
+                moved_any |= moved;
+            }
+            if (!gn_block()) return false;
+        }
         // iter_end: a move resets the stall count; with the shift hop on, two iterations in a
         // row without a move end the climb (one without it), as does the iteration budget
         stall = moved_any ? 0 : stall + 1;
@@ -311,7 +343,7 @@ bool Engine::climb(zc_climb_result* out) {
         snprintf(buf, sizeof buf, "ascent %u/%u score %.4f  stall %u  (%u steps so far)", iter, n_iters, cur.mean, stall,
                  n_rec);
         log_event(buf);
-        if ((!moved_any && (!hop || stall >= 2)) || iter >= n_iters) break;
+        if ((!moved_any && (!hops || stall >= 2)) || iter >= n_iters) break;
         if (cancel) {
             snprintf(buf, sizeof buf, "ascent stopped  score %.4f", cur.mean);
             log_event(buf);

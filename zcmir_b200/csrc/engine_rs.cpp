@@ -121,11 +121,50 @@ bool Engine::rs_map_one(const Mat3& H, const double c[2], double r0_opt, double 
     return true;
 }
 
+void Engine::rs_center(const Mat3& H, double c[2]) const {
+    const double lw = side[0].w, lh = side[0].h;
+    const double q[4][2] = {{1, 1}, {lw, 1}, {lw, lh}, {1, lh}};
+    c[0] = c[1] = 0;
+    for (const auto& v : q) {
+        const auto m = map_pt(H, v[0], v[1]);
+        c[0] += 0.25 * m[0], c[1] += 0.25 * m[1];
+    }
+}
+
+bool Engine::rs_peak(const Mat3& H, const double c[2], double* dth, double* dsg) {
+    RsPlan p;
+    if (!rs_map_one(H, c, -1, 0, set.b("exact"), set.b("calibrated"), set.u("map_res"), rs_fwd_, p)) return false;
+    const bool mirror = H[0] * H[4] - H[1] * H[3] > 0;
+    const double smin = set.f("rs_smin"), smax = set.f("rs_smax");
+    const double lo = std::log(std::max(smin > 0 ? smin : 0.2, 1e-6));
+    const double hi = std::log(std::max(smax > 0 ? smax : 5.0, 1.000001));
+    const size_t nn = (size_t)p.n * p.n;
+    char* res = res_.as<char>();
+    unsigned long long key = 0;
+    if (!cuda_ok(rs_map_.ensure(nn * 4), "rs_map") ||
+        !cuda_ok(rs_finish(rs_fwd_.as<float>(), nullptr, mirror, p.n, (float)p.dlam, (float)lo, (float)hi,
+                           rs_map_.as<float>(), reinterpret_cast<unsigned long long*>(res),
+                           reinterpret_cast<float*>(res + 8), st),
+                 "rs_map") ||
+        !cuda_ok(cudaMemcpyAsync(&key, res, 8, cudaMemcpyDeviceToHost, st), "rs_map") ||
+        !cuda_ok(cudaStreamSynchronize(st), "rs_map"))
+        return false;
+    counts[0] += 1, counts[1]++, counts[2]++, counts[3]++;
+    *dth = *dsg = 0;
+    const uint32_t idx = 0xffffffffu - (uint32_t)(key & 0xffffffffu);
+    if (key != 0 && idx < nn) {
+        const int64_t py = idx / p.n, px = idx % p.n;
+        const int64_t lx = px <= p.n / 2 ? px : px - p.n, ly = py <= p.n / 2 ? py : py - p.n;
+        *dth = -((double)lx / (double)std::max(p.n_th, 1)) * 2 * M_PI;
+        *dsg = -(double)ly * p.dlam;
+    }
+    return true;
+}
+
 bool Engine::rs_map(const Mat3& H, const double* c_opt, bool symmetric, zc_rs_result* out, float* map, float* fwd,
                     float* inv, size_t len) {
     if (!need_images()) return false;
-    if (set.e("metric") != "smi")
-        return fail("rs_map: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    if (!metric_ok("rs_map")) return false;
     const bool exact = set.b("exact"), calibrated = set.b("calibrated");
     const unsigned cap = set.u("map_res");
     // the centre: given, else the moving image's centroid under H (src/lie.zig movingCentroid)
@@ -133,13 +172,7 @@ bool Engine::rs_map(const Mat3& H, const double* c_opt, bool symmetric, zc_rs_re
     if (c_opt) {
         c[0] = c_opt[0], c[1] = c_opt[1];
     } else {
-        const double lw = side[0].w, lh = side[0].h;
-        const double q[4][2] = {{1, 1}, {lw, 1}, {lw, lh}, {1, lh}};
-        c[0] = c[1] = 0;
-        for (const auto& v : q) {
-            const auto m = map_pt(H, v[0], v[1]);
-            c[0] += 0.25 * m[0], c[1] += 0.25 * m[1];
-        }
+        rs_center(H, c);
     }
     RsPlan p, pi;
     if (!rs_map_one(H, c, -1, 0, exact, calibrated, cap, rs_fwd_, p)) return false;

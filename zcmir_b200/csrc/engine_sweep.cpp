@@ -394,8 +394,8 @@ bool Engine::search_check() {
     if (!need_images()) return false;
     if (set.e("search_mode") != "sweep")
         return fail("search: search_mode \"" + set.e("search_mode") + "\" is not part of this build (search_mode=\"sweep\" is)");
-    if (set.e("metric") != "smi")
-        return fail("search: metric \"" + set.e("metric") + "\" is not part of this build's SMI path (metric=\"smi\")");
+    if (set.e("metric") == "ncc") return fail("search: SweepNeedsMomentScore (the sweep scores SMI moments; metric \"ncc\" has none)");
+    if (!metric_ok("search")) return false;
     return true;
 }
 

@@ -127,6 +127,23 @@ inline MapPlan linear_corr_plan_rect(int w, int h, unsigned max_n0, bool ladder)
     return {(int)max_n, (int)max_n, m, m};
 }
 
+// (n, cw, ch): one FFT length for both axes (src/fft.zig:70-91 linearCorrPlan, the NCC map's)
+inline MapPlan linear_corr_plan(int w, int h, unsigned max_n0, bool ladder) {
+    const unsigned max_n = largest_smooth(max_n0, ladder);
+    double s = std::min(1.0, (double)std::max(8u, max_n >> 1) / (double)std::max(std::max(w, h), 1));
+    unsigned n = 8, cw = 8, ch = 8;
+    for (int i = 0; i < 16; ++i) {
+        cw = std::max(8u, js_round(w * s));
+        ch = std::max(8u, js_round(h * s));
+        n = std::min(plan_size(std::max({cw + cw - 1, ch + ch - 1, 32u}), 1, ladder), max_n);
+        if (n >= cw + cw - 1 && n >= ch + ch - 1) return {(int)n, (int)n, (int)cw, (int)ch};
+        s *= 0.85;
+    }
+    cw = std::max(8u, std::min(cw, (n + 1) >> 1));
+    ch = std::max(8u, std::min(ch, (n + 1) >> 1));
+    return {(int)n, (int)n, (int)cw, (int)ch};
+}
+
 constexpr unsigned kMapAutoMin = 128, kMapAutoMax = 512, kMapCap = 1024;
 
 inline MapPlan auto_shift_plan(int w, int h) {

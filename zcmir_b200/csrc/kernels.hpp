@@ -37,7 +37,8 @@ struct MapGeom {
 struct CombineParams {
     int exact;       // per-overlap whitening
     int calib;       // Wilson–Hilferty z (exact only)
-    int nf;          // features the score runs over (3 or 4)
+    int nf;          // features the score runs over (3 or 4); 1: the NCC map (one correlation
+                     // over the norm product, which the n00 slot carries)
     float min_n;     // overlap floor (cells)
     double area;     // feature correlation area in cells (calibrated z)
     double ridge;
@@ -133,6 +134,18 @@ cudaError_t rs_logpolar(const float* canvas, int W, int Hh, float cx, float cy, 
 // symmetric average (inv may be null), scale mask, argmax key and lag-0 cell of an n × n map
 cudaError_t rs_finish(const float* fwd, const float* inv, bool mirror, int n, float dlam, float lo, float hi,
                       float* out, unsigned long long* best, float* zero, cudaStream_t st);
+
+// ── the NCC overlay metric (ncc.cu); the work images are f32, hi the canvas pose's inverse ──
+// both canvas planes of the pair: moving warped (rounded to f16 texels when half), fixed pasted
+cudaError_t ncc_canvas(const float* mv, int w, int h, const float hi[9], bool ok, const float* fx, int fw, int fh, int ox,
+                       int oy, bool half, int W, int Hh, float* ca, float* cb, cudaStream_t st);
+// Σa, Σb, Σa², Σb², Σab over the canvas (float64) into mom[5], the canvas not written
+cudaError_t ncc_moments(const float* mv, int w, int h, const float hi[9], bool ok, const float* fx, int fw, int fh,
+                        int ox, int oy, bool half, int W, int Hh, double* mom, cudaStream_t st);
+// the canvases resampled to cw × ch (plane 0 of ga, gb), made mean-free; sums[4] = Σa, Σb, Σa'²,
+// Σb'²; *den = max(‖a'‖‖b'‖, 1e-12)
+cudaError_t ncc_grid(const float* ca, const float* cb, int W, int Hh, int cw, int ch, float* ga, float* gb,
+                     double* sums, double* den, cudaStream_t st);
 
 // ── pose scores and gradients (pose.cu) ──
 struct PoseSide {

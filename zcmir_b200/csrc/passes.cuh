@@ -504,6 +504,7 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
         return cudaGetLastError();
     } else {
         const CombineParams& cp = *a.cp;
+        if (cp.nf == 1) return launch_rows<F, 1, false, false, SPLIT>(f, a, st);
         if (cp.nf == 4) {
             if (!cp.exact) return launch_rows<F, 4, false, false, SPLIT>(f, a, st);
             if (cp.calib) return launch_rows<F, 4, true, true, SPLIT>(f, a, st);
