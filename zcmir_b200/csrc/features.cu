@@ -205,12 +205,19 @@ __global__ void k_whiten(float* __restrict__ feat, int n, const float* __restric
     }
 }
 
-// Autocorrelation partial sums (smi.wgsl:935-975): one block per 32×32 tile (8-px halo in
-// shared memory), one thread per lag (17×17), f32 sums over the tile; partials [tile][289][4].
-constexpr int kAcfTile = 32, kAcfHalo = 8, kAcfSpan = kAcfTile + 2 * kAcfHalo;
+// Autocorrelation partial sums (smi.wgsl:935-975): one block per 32×32 tile with an 8-px halo in
+// shared memory (zero outside the image, so a pair with either pixel outside adds nothing and
+// every lag sums exactly the pairs inside the image). Register-blocked: thread (plane p, row lag
+// dy, row group g) takes the tile rows g, g + 4, …, and for each holds the row (32 values) and
+// its partner row at dy with the column halo (48 values) in registers, then accumulates all 17
+// column lags (544 FMAs per 20 vector shared loads). The four row groups' f32 sums are added in
+// shared memory; partials [tile][289][4].
+constexpr int kAcfTile = 32, kAcfHalo = 8, kAcfSpan = kAcfTile + 2 * kAcfHalo, kAcfGroups = 4;
+constexpr int kAcfThreads = 4 * 17 * kAcfGroups;  // 272
 
-__global__ void __launch_bounds__(320) k_acf(const float* __restrict__ feat, int w, int h, float* __restrict__ part) {
-    __shared__ float sh[4][kAcfSpan * kAcfSpan];
+__global__ void __launch_bounds__(kAcfThreads) k_acf(const float* __restrict__ feat, int w, int h,
+                                                     float* __restrict__ part) {
+    __shared__ __align__(16) float sh[4 * kAcfSpan * kAcfSpan];
     const int x0 = blockIdx.x * kAcfTile, y0 = blockIdx.y * kAcfTile;
     const size_t n = (size_t)w * h;
     for (int k = threadIdx.x; k < kAcfSpan * kAcfSpan; k += blockDim.x) {
@@ -218,28 +225,47 @@ __global__ void __launch_bounds__(320) k_acf(const float* __restrict__ feat, int
         const bool in = gx >= 0 && gy >= 0 && gx < w && gy < h;
         const size_t i = in ? (size_t)gy * w + gx : 0;
 #pragma unroll
-        for (int p = 0; p < 4; ++p) sh[p][k] = in ? feat[p * n + i] : 0.0f;
+        for (int p = 0; p < 4; ++p) sh[p * kAcfSpan * kAcfSpan + k] = in ? feat[p * n + i] : 0.0f;
     }
     __syncthreads();
-    const int lag = threadIdx.x;
-    if (lag >= 289) return;
-    const int dx = lag % 17 - 8, dy = lag / 17 - 8;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    // pixels t of the tile whose partner t + τ lies in the image: a rectangle
-    const int tx0 = max(0, -dx - x0), tx1 = min(min(kAcfTile, w - x0), w - dx - x0);
-    const int ty0 = max(0, -dy - y0), ty1 = min(min(kAcfTile, h - y0), h - dy - y0);
-    for (int ty = ty0; ty < ty1; ++ty) {
-        const int a0 = (ty + kAcfHalo) * kAcfSpan + kAcfHalo;
-        const int b0 = a0 + dy * kAcfSpan + dx;
-#pragma unroll 4
-        for (int tx = tx0; tx < tx1; ++tx) {
+    const int g = threadIdx.x % kAcfGroups, dy = (threadIdx.x / kAcfGroups) % 17, p = threadIdx.x / (kAcfGroups * 17);
+    const float* pl = sh + p * kAcfSpan * kAcfSpan;
+    float acc[17];
 #pragma unroll
-            for (int p = 0; p < 4; ++p) acc[p] = fmaf(sh[p][a0 + tx], sh[p][b0 + tx], acc[p]);
+    for (int d = 0; d < 17; ++d) acc[d] = 0.f;
+    for (int ty = g; ty < kAcfTile; ty += kAcfGroups) {
+        float a[32], b[48];
+        const float4* ar = reinterpret_cast<const float4*>(pl + (ty + kAcfHalo) * kAcfSpan + kAcfHalo);
+        const float4* br = reinterpret_cast<const float4*>(pl + (ty + dy) * kAcfSpan);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 v = ar[q];
+            a[4 * q] = v.x, a[4 * q + 1] = v.y, a[4 * q + 2] = v.z, a[4 * q + 3] = v.w;
         }
-    }
-    const size_t o = ((size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 289 + lag) * 4;
 #pragma unroll
-    for (int p = 0; p < 4; ++p) part[o + p] = acc[p];
+        for (int q = 0; q < 12; ++q) {
+            const float4 v = br[q];
+            b[4 * q] = v.x, b[4 * q + 1] = v.y, b[4 * q + 2] = v.z, b[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int d = 0; d < 17; ++d)
+#pragma unroll
+            for (int x = 0; x < 32; ++x) acc[d] = fmaf(a[x], b[x + d], acc[d]);
+    }
+    __syncthreads();
+    // the row groups' sums: red[g][p·289 + lag] in the (now free) staging array
+    float* red = sh;
+#pragma unroll
+    for (int d = 0; d < 17; ++d) red[g * 1156 + p * 289 + dy * 17 + d] = acc[d];
+    __syncthreads();
+    const size_t o = (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 1156;
+    for (int k = threadIdx.x; k < 1156; k += blockDim.x) {
+        const int lag = k >> 2, pp = k & 3;
+        float s = 0.f;
+#pragma unroll
+        for (int gg = 0; gg < kAcfGroups; ++gg) s += red[gg * 1156 + pp * 289 + lag];
+        part[o + k] = s;
+    }
 }
 
 // Σ over tiles (float64), ÷ the lag's pair count → acf[289][4] (not yet normalised)
@@ -291,7 +317,7 @@ cudaError_t build_features(float* gray, int w, int h, int mode, bool half, float
     dim3 ga((w + kAcfTile - 1) / kAcfTile, (h + kAcfTile - 1) / kAcfTile);
     const int ntiles = ga.x * ga.y;
     if ((size_t)ntiles * 1156 > s.acf_part_cap) return cudaErrorInvalidValue;
-    k_acf<<<ga, 320, 0, st>>>(feat, w, h, s.acf_part);
+    k_acf<<<ga, kAcfThreads, 0, st>>>(feat, w, h, s.acf_part);
     k_acf_finish<<<1156, kThreads, 0, st>>>(s.acf_part, ntiles, w, h, s.acf);
     k_stack<<<gb, kThreads, 0, st>>>(feat, n, stack);
     return cudaGetLastError();
