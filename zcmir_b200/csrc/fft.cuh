@@ -256,7 +256,94 @@ __device__ __forceinline__ void mix_fft(float2* __restrict__ buf, const float2* 
     }
 }
 
-// Line-FFT policies the map kernels are written against: n(), threads per line, run<INV>().
+// The stages after the first and before the last (S = 1 .. kStages − 2), through shared memory.
+template <int N, int TL, bool INV, int S, int NS>
+__device__ __forceinline__ void mix_mid(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
+    if constexpr (S < Mix<N>::kStages - 1) {
+        constexpr int R = Mix<N>::radix(S);
+        mix_stage<R, NS, N, TL, INV>(buf, tw, t, act);
+        mix_mid<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
+    }
+}
+
+// The whole line with its ends in registers: the first stage's butterflies take their inputs
+// straight from in(y) (point y of the line, typically a global load) and the last stage hands
+// its outputs to out(y, v), so the line is staged into and out of shared memory by neither the
+// caller nor this function (two shared-memory passes fewer than run()). Every thread of the
+// block calls it; buf is this thread's line buffer (padded_len(N) points). On return the
+// buffer may still be read by other threads of the line: synchronise before reusing it.
+template <int N, int TL, bool INV, class In, class Out>
+__device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
+                                           In&& in, Out&& out) {
+    using MX = Mix<N>;
+    static_assert(MX::kStages >= 2, "a line of one stage has no middle to run through shared memory");
+    constexpr int R0 = MX::radix(0), M0 = N / R0, BM0 = (M0 + TL - 1) / TL;
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BM0; ++b) {
+            const int j = t + b * TL;
+            if (M0 % TL == 0 || j < M0) {
+                float2 v[R0];
+#pragma unroll
+                for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
+                dft<R0, INV>(v);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) buf[pad_idx(j * R0 + r)] = v[r];
+            }
+        }
+    }
+    __syncthreads();
+    mix_mid<N, TL, INV, 1, R0>(buf, tw, t, act);
+    constexpr int RL = MX::radix(MX::kStages - 1), NSL = N / RL, ML = N / RL, BML = (ML + TL - 1) / TL;
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BML; ++b) {
+            const int j = t + b * TL;
+            if (ML % TL == 0 || j < ML) {
+                float2 v[RL];
+#pragma unroll
+                for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
+                // k = j mod NSL = j: twiddles w^{r·j} of the full length
+#pragma unroll
+                for (int r = 1; r < RL; ++r) {
+                    float2 w = __ldg(&tw[r * j]);
+                    if (INV) w.y = -w.y;
+                    v[r] = cmul(v[r], w);
+                }
+                dft<RL, INV>(v);
+#pragma unroll
+                for (int r = 0; r < RL; ++r) out(j + r * NSL, v[r]);
+            }
+        }
+    }
+}
+
+// The whole line with its first stage fed from in(y) (as mix_fft_io) and the result left in buf
+// in natural order, the block synchronised, as run() leaves it.
+template <int N, int TL, bool INV, class In>
+__device__ __forceinline__ void mix_fft_in(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
+                                           In&& in) {
+    constexpr int R0 = Mix<N>::radix(0), M0 = N / R0, BM0 = (M0 + TL - 1) / TL;
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BM0; ++b) {
+            const int j = t + b * TL;
+            if (M0 % TL == 0 || j < M0) {
+                float2 v[R0];
+#pragma unroll
+                for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
+                dft<R0, INV>(v);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) buf[pad_idx(j * R0 + r)] = v[r];
+            }
+        }
+    }
+    __syncthreads();
+    mix_fft<N, TL, INV, 1, R0>(buf, tw, t, act);
+}
+
+// Line-FFT policies the map kernels are written against: n(), threads per line, run<INV>(),
+// run_io<INV>(buf, t, act, in, out) (mix_fft_io's contract) and run_in<INV>(buf, t, act, in).
 struct GenericLine {
     LinePlan p;
     __host__ __device__ __forceinline__ int n() const { return p.n; }
@@ -264,6 +351,25 @@ struct GenericLine {
     template <bool INV>
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
         line_fft<INV>(buf, p, act ? t : (1 << 30));
+    }
+    // runtime lines stage through shared memory around the transform
+    template <bool INV, class In, class Out>
+    __device__ __forceinline__ void run_io(float2* buf, int t, bool act, In&& in, Out&& out) const {
+        const bool a = act && t < p.tl;
+        if (a)
+            for (int y = t; y < p.n; y += p.tl) buf[pad_idx(y)] = in(y);
+        __syncthreads();
+        line_fft<INV>(buf, p, a ? t : (1 << 30));
+        if (a)
+            for (int y = t; y < p.n; y += p.tl) out(y, buf[pad_idx(y)]);
+    }
+    template <bool INV, class In>
+    __device__ __forceinline__ void run_in(float2* buf, int t, bool act, In&& in) const {
+        const bool a = act && t < p.tl;
+        if (a)
+            for (int y = t; y < p.n; y += p.tl) buf[pad_idx(y)] = in(y);
+        __syncthreads();
+        line_fft<INV>(buf, p, a ? t : (1 << 30));
     }
 };
 
@@ -278,6 +384,14 @@ struct FixedLine {
     template <bool INV>
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
         mix_fft<N, TPL, INV>(buf, tw, t, act && t < TPL);
+    }
+    template <bool INV, class In, class Out>
+    __device__ __forceinline__ void run_io(float2* buf, int t, bool act, In&& in, Out&& out) const {
+        mix_fft_io<N, TPL, INV>(buf, tw, t, act && t < TPL, in, out);
+    }
+    template <bool INV, class In>
+    __device__ __forceinline__ void run_in(float2* buf, int t, bool act, In&& in) const {
+        mix_fft_in<N, TPL, INV>(buf, tw, t, act && t < TPL, in);
     }
 };
 

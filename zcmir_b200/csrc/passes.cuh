@@ -110,20 +110,17 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
     for (int z0 = 0; z0 < n_cplx; z0 += lpb) {
         const int z = z0 + line;
         const bool act = line < lpb && z < n_cplx;
-        if (act) {
-            const int ra = planes[2 * z];
-            const int rb = planes[2 * z + 1];
-            for (int x = t; x < nx; x += tl) {
-                float2 v = make_float2(0.f, 0.f);
-                if (x < cw) {
-                    v.x = real_plane_row(ra, row, cw, x);
-                    if (rb >= 0) v.y = real_plane_row(rb, row, cw, x);
-                }
-                buf[pad_idx(x)] = v;
+        const int ra = act ? planes[2 * z] : 0;
+        const int rb = act ? planes[2 * z + 1] : -1;
+        // the first butterflies read the staged row directly (real planes ra + i·rb, zero past cw)
+        f.template run_in<false>(buf, t, act, [&](int x) {
+            float2 v = make_float2(0.f, 0.f);
+            if (x < cw) {
+                v.x = real_plane_row(ra, row, cw, x);
+                if (rb >= 0) v.y = real_plane_row(rb, row, cw, x);
             }
-        }
-        __syncthreads();
-        f.template run<false>(buf, t, act);
+            return v;
+        });
         if (act) {
             const bool has_b = 2 * z + 1 < plan.n_real;
             float2* oa = half + (size_t)(2 * z) * pstride + (size_t)y * WP;
@@ -140,37 +137,25 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
 }
 
 // Column FFTs of the half spectra, in place: block = a tile of tx columns of one plane; rows
-// ≥ rows_in read as zero. Loads and stores go 8 per thread at a time (all in flight together).
+// ≥ rows_in read as zero. Thread (column c, line thread t), c fastest, so each load or store of
+// a warp covers 8 rows × 4 adjacent columns (whole 32-byte sectors); the first butterflies read
+// global memory and the last write it (run_io), with only the middle stages in shared memory.
 template <class F, bool INV>
 __global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size_t pstride, int WP, int ncols,
                                                  int rows_in, F f, int tx) {
     extern __shared__ float2 smem[];
     const int x0 = blockIdx.x * tx;
     float2* base = half + (size_t)blockIdx.y * pstride;
-    const int ny = f.n(), pl = line_pitch(ny), tl = f.tl();
-    const int total = tx * ny;
-    for (int e0 = 0; e0 < total; e0 += 8 * blockDim.x) {
-        float2 v[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int e = e0 + i * blockDim.x + threadIdx.x;
-            const int y = e / tx, c = e - y * tx;
-            v[i] = (e < total && y < rows_in && x0 + c < ncols) ? base[(size_t)y * WP + x0 + c] : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int e = e0 + i * blockDim.x + threadIdx.x;
-            const int y = e / tx, c = e - y * tx;
-            if (e < total) smem[c * pl + pad_idx(y)] = v[i];
-        }
-    }
-    __syncthreads();
-    const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
-    f.template run<INV>(smem + (line < tx ? line : 0) * pl, t, line < tx);
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int y = e / tx, c = e - y * tx;
-        if (x0 + c < ncols) base[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
-    }
+    const int pl = line_pitch(f.n());
+    const int c = threadIdx.x % tx, t = threadIdx.x / tx, col = x0 + c;
+    const bool okc = col < ncols;
+    float2* p = base + col;
+    f.template run_io<INV>(
+        smem + c * pl, t, true,
+        [&](int y) { return (okc && y < rows_in) ? p[(size_t)y * WP] : make_float2(0.f, 0.f); },
+        [&](int y, float2 v) {
+            if (okc) p[(size_t)y * WP] = v;
+        });
 }
 
 // ── inverse: products and column IFFTs ──────────────────────────────────────────────────────
@@ -185,36 +170,20 @@ __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ 
     const int k = blockIdx.x;
     const int x0 = blockIdx.y * tx;
     const size_t item = blockIdx.z;
-    const float2* A = ha + item * abs_ + (size_t)plan.ca[k] * pstride;
-    const float2* B = hb + item * bbs + (size_t)plan.cb[k] * pstride;
-    float2* O = Q + item * qbs + (size_t)k * pstride;
-    const int ny = f.n(), pl = line_pitch(ny), tl = f.tl();
-    const int total = tx * ny;
-    for (int e0 = 0; e0 < total; e0 += 4 * blockDim.x) {
-        float2 a[4], b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int e = e0 + i * blockDim.x + threadIdx.x;
-            const int y = e / tx, c = e - y * tx;
-            const bool ok = e < total && x0 + c < ncols;
-            const size_t ix = (size_t)y * WP + x0 + c;
-            a[i] = ok ? __ldg(&A[ix]) : make_float2(0.f, 0.f);
-            b[i] = ok ? __ldg(&B[ix]) : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int e = e0 + i * blockDim.x + threadIdx.x;
-            const int y = e / tx, c = e - y * tx;
-            if (e < total) smem[c * pl + pad_idx(y)] = cmulc(a[i], b[i]);
-        }
-    }
-    __syncthreads();
-    const int line = threadIdx.x / tl, t = threadIdx.x - line * tl;
-    f.template run<true>(smem + (line < tx ? line : 0) * pl, t, line < tx);
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int y = e / tx, c = e - y * tx;
-        if (x0 + c < ncols) O[(size_t)y * WP + x0 + c] = smem[c * pl + pad_idx(y)];
-    }
+    const int c = threadIdx.x % tx, t = threadIdx.x / tx, col = x0 + c;
+    const bool okc = col < ncols;
+    const float2* A = ha + item * abs_ + (size_t)plan.ca[k] * pstride + col;
+    const float2* B = hb + item * bbs + (size_t)plan.cb[k] * pstride + col;
+    float2* O = Q + item * qbs + (size_t)k * pstride + col;
+    const int pl = line_pitch(f.n());
+    f.template run_io<true>(
+        smem + c * pl, t, true,
+        [&](int y) {
+            return okc ? cmulc(__ldg(&A[(size_t)y * WP]), __ldg(&B[(size_t)y * WP])) : make_float2(0.f, 0.f);
+        },
+        [&](int y, float2 v) {
+            if (okc) O[(size_t)y * WP] = v;
+        });
 }
 
 // ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
@@ -359,43 +328,26 @@ __global__ void __launch_bounds__(512, 1) k_rows_multi(const float2* __restrict_
         const int r = act ? task / npairs : 0;
         const int pr = act ? task - r * npairs : 0;
         const int k1 = 2 * pr, k2 = (2 * pr + 1 < plan.n_corr) ? 2 * pr + 1 : -1;
-        if (act) {
-            const size_t row = (size_t)(y0 + r) * WP;
-            const float2* q1 = Q + (size_t)k1 * pstride + row;
-            const float2* q2 = (k2 >= 0) ? Q + (size_t)k2 * pstride + row : q1;
-            const bool has2 = k2 >= 0;
-            constexpr int B = 8;
-            const int per = (nx + tl - 1) / tl;
-            for (int b0 = 0; b0 < per; b0 += B) {
-                float2 ra[B], rb[B];
-#pragma unroll
-                for (int i = 0; i < B; ++i) {
-                    const int x = t + (b0 + i) * tl;
-                    const int ix = (x <= nx / 2) ? x : nx - x;
-                    const bool ok = x < nx;
-                    ra[i] = ok ? __ldg(&q1[ix]) : make_float2(0.f, 0.f);
-                    rb[i] = (ok && has2) ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
-                }
-#pragma unroll
-                for (int i = 0; i < B; ++i) {
-                    const int x = t + (b0 + i) * tl;
-                    if (x >= nx) continue;
-                    const float2 a = ra[i], bb = rb[i];
-                    // Z = Q1 + i·Q2 on the half row; conj(Q1) + i·conj(Q2) on the mirrored half
-                    buf[pad_idx(x)] = (x <= nx / 2) ? make_float2(a.x - bb.y, a.y + bb.x) : make_float2(a.x + bb.y, bb.x - a.y);
-                }
-            }
-        }
-        __syncthreads();
-        f.template run<true>(buf, t, act);
-        if (act) {
-            float* c = corr + (size_t)r * plan.n_corr * nx;
-            for (int m = t; m < nx; m += tl) {
-                const float2 z = buf[pad_idx(m)];
+        const size_t row = (size_t)(y0 + r) * WP;
+        const float2* q1 = Q + (size_t)k1 * pstride + row;
+        const float2* q2 = (k2 >= 0) ? Q + (size_t)k2 * pstride + row : q1;
+        const bool has2 = k2 >= 0;
+        float* c = corr + (size_t)r * plan.n_corr * nx;
+        // the first butterflies read the Hermitian row from the half spectra, the last write the
+        // row's sums straight to the correlation rows
+        f.template run_io<true>(
+            buf, t, act,
+            [&](int x) {
+                // Z = Q1 + i·Q2 on the half row; conj(Q1) + i·conj(Q2) on the mirrored half
+                const int ix = (x <= nx / 2) ? x : nx - x;
+                const float2 a = __ldg(&q1[ix]);
+                const float2 bb = has2 ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
+                return (x <= nx / 2) ? make_float2(a.x - bb.y, a.y + bb.x) : make_float2(a.x + bb.y, bb.x - a.y);
+            },
+            [&](int m, float2 z) {
                 c[(size_t)k1 * nx + m] = z.x;
-                if (k2 >= 0) c[(size_t)k2 * nx + m] = z.y;
-            }
-        }
+                if (has2) c[(size_t)k2 * nx + m] = z.y;
+            });
         __syncthreads();
     }
     const double n00 = lag0_units(cp, *n00p);

@@ -56,12 +56,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 
 constexpr int kTmemSlots = 32;
 
+// Lines of N ≥ 1024 run with 128 threads each and their ends in registers (run_io): the first
+// butterflies read the Hermitian row straight from the half spectra, and the last hand each
+// thread the outputs m ≡ t (mod 128) of its line thread t — exactly the TMEM lane that thread's
+// warp reaches — so the sums go from registers to TMEM with no pass through shared memory.
+template <int N>
+constexpr bool rows_io() { return N >= 1024; }
+template <int N>
+constexpr int rows_tl() { return rows_io<N>() ? 128 : N / 8; }
+
 template <int N, int NF, bool EXACT, bool CALIB>
 __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__ Q, size_t pstride, int WP, int n_corr,
                                                       const float2* __restrict__ tw, CombineParams cp,
                                                       const double* __restrict__ n00p, float* __restrict__ map,
                                                       unsigned long long* best, float* zero_out) {
-    constexpr int TL = N / 8;                  // threads per line
+    constexpr int TL = rows_tl<N>();           // threads per line
     constexpr int LINES = 512 / TL;            // lines per round
     constexpr int J = N / 128;                 // cells per TMEM lane
     constexpr int TCOLS = J * kTmemSlots;      // columns allocated (power of two ≥ 32)
@@ -89,6 +98,39 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
     float2* buf = lines + line * PL;
     const int npairs = (n_corr + 1) / 2;
     const Pow2Line<N, TL> fft{tw};
+
+    if constexpr (rows_io<N>()) {
+        static_assert(N / Mix<N>::radix(Mix<N>::kStages - 1) % 128 == 0, "last-stage outputs must fall in lane t");
+        for (int p0 = 0; p0 < npairs; p0 += LINES) {
+            const int pr = p0 + line;
+            const bool act = pr < npairs;
+            const int k1 = 2 * pr, k2 = 2 * pr + 1;
+            const bool h2 = k2 < n_corr;
+            const float2* q1 = Q + (size_t)(act ? k1 : 0) * pstride + (size_t)y * WP;
+            const float2* q2 = Q + (size_t)(act && h2 ? k2 : 0) * pstride + (size_t)y * WP;
+            fft.template run_io<true>(
+                buf, t, act,
+                [&](int x) {
+                    // Z = Q1 + i·Q2 on the half row, conj(Q1) + i·conj(Q2) mirrored above it
+                    const int ix = x <= N / 2 ? x : N - x;
+                    const float2 a = __ldg(&q1[ix]);
+                    const float2 b = h2 ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
+                    return x <= N / 2 ? make_float2(a.x - b.y, a.y + b.x) : make_float2(a.x + b.y, b.x - a.y);
+                },
+                [&](int m, float2 z) {
+                    // cell m lies in TMEM lane m mod 128 = t, this warp's quadrant; the warp's
+                    // lines all run, so each store is executed by the whole warp
+                    const uint32_t col = (uint32_t)(m >> 7) * kTmemSlots;
+                    if (k1 < kTmemSlots) tmem_st1(tq + col + (uint32_t)k1, z.x);
+                    else cs[(size_t)(k1 - kTmemSlots) * N + m] = z.x;
+                    if (h2) {
+                        if (k2 < kTmemSlots) tmem_st1(tq + col + (uint32_t)k2, z.y);
+                        else cs[(size_t)(k2 - kTmemSlots) * N + m] = z.y;
+                    }
+                });
+            __syncthreads();  // the line buffers are refilled next round
+        }
+    } else {
 
     float2 pa[PER], pb[PER], na = make_float2(0.f, 0.f), nb = make_float2(0.f, 0.f);
     auto fetch = [&](int pr) {
@@ -152,6 +194,7 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
         }
         __syncthreads();
     }
+    }
     tmem_wait_st();
     tc_fence_before();
     __syncthreads();
@@ -193,7 +236,7 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
 template <int N, int NF, bool EXACT, bool CALIB>
 cudaError_t launch_tmem(const float2* Q, const MapGeom& g, int n_corr, const float2* tw, const CombineParams& cp,
                         const double* n00, float* map, unsigned long long* best, float* zero, cudaStream_t st) {
-    constexpr int TL = N / 8, LINES = 512 / TL;
+    constexpr int TL = rows_tl<N>(), LINES = 512 / TL;
     const int extra = n_corr > kTmemSlots ? n_corr - kTmemSlots : 0;
     const size_t sm = (size_t)LINES * padded_len(N) * sizeof(float2) + (size_t)extra * N * sizeof(float);
     auto k = k_rows_tmem<N, NF, EXACT, CALIB>;
