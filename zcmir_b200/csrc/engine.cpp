@@ -295,15 +295,25 @@ bool Engine::work_image(int s, float* out, size_t len) {
 const float2* Engine::twiddles(int n) {
     auto it = tw_.find(n);
     if (it != tw_.end()) return it->second;
-    std::vector<float2> h(n);
+    // e^{−2πi t/n}, t < n, then the compile-time lines' per-stage tables (fft.cuh stage_tw_off)
+    const int ns = mix_stages(n), extra = stage_tw_off(n, ns);
+    std::vector<float2> h((size_t)n + extra);
     for (int t = 0; t < n; ++t) {
         const double a = -2.0 * M_PI * (double)t / (double)n;
         h[t] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
+    for (int s = 1, NS = mix_radix(n, 0); s < ns; NS *= mix_radix(n, s), ++s) {
+        const int R = mix_radix(n, s), off = n + stage_tw_off(n, s);
+        for (int r = 1; r < R; ++r)
+            for (int k = 0; k < NS; ++k) {
+                const double a = -2.0 * M_PI * (double)(r * k) / (double)(NS * R);
+                h[(size_t)off + (size_t)(r - 1) * NS + k] = make_float2((float)std::cos(a), (float)std::sin(a));
+            }
+    }
     float2* d = nullptr;
-    if (cudaMalloc(&d, (size_t)n * sizeof(float2)) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&d, h.size() * sizeof(float2)) != cudaSuccess) return nullptr;
     // stream-ordered before every kernel that reads it (pageable source: staged before return)
-    if (cudaMemcpyAsync(d, h.data(), (size_t)n * sizeof(float2), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    if (cudaMemcpyAsync(d, h.data(), h.size() * sizeof(float2), cudaMemcpyHostToDevice, st) != cudaSuccess) {
         cudaFree(d);
         return nullptr;
     }

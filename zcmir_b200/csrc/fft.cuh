@@ -197,20 +197,43 @@ constexpr int twos_of(int n) { return (n > 0 && n % 2 == 0) ? 1 + twos_of(n / 2)
 constexpr int threes_of(int n) { return (n > 0 && n % 3 == 0) ? 1 + threes_of(n / 3) : 0; }
 constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 
+// The schedule of a line of n = 2^a·3^b points (compile-time for the kernels, run-time for the
+// host building the twiddle tables): the number of stages and stage s's radix.
+__host__ __device__ constexpr int mix_stages(int n) { return (twos_of(n) + 3) / 4 + threes_of(n); }
+__host__ __device__ constexpr int mix_radix(int n, int s) {
+    return s < (twos_of(n) + 3) / 4
+               ? 1 << (twos_of(n) / ((twos_of(n) + 3) / 4) + (s < twos_of(n) % ((twos_of(n) + 3) / 4) ? 1 : 0))
+               : 3;
+}
+// Per-stage twiddle tables, after the n entries e^{−2πi t/n} of a line's table: stage s (radix R,
+// NS points transformed before it, NS > 1) holds w(r, k) = e^{−2πi r k/(NS·R)} at
+// (r − 1)·NS + k, r = 1..R−1, k < NS, so the threads of a stage (consecutive k) read consecutive
+// entries. stage_tw_off: where stage s's table starts (past the n entries); its value at
+// s = mix_stages(n) is the tables' total length.
+__host__ __device__ constexpr int stage_tw_off(int n, int s) {
+    int off = 0, ns = 1;
+    for (int i = 0; i < s; ++i) {
+        const int r = mix_radix(n, i);
+        if (ns > 1) off += (r - 1) * ns;
+        ns *= r;
+    }
+    return off;
+}
+
 template <int N>
 struct Mix {
     static constexpr int kA = twos_of(N), kB = threes_of(N);
     static_assert(ipow(2, twos_of(N)) * ipow(3, threes_of(N)) == N, "line length must be 2^a·3^b");
     static constexpr int kP2 = (kA + 3) / 4;
     static constexpr int kStages = kP2 + kB;
-    static constexpr int radix(int s) {
-        return s < kP2 ? 1 << (kA / kP2 + (s < kA % kP2 ? 1 : 0)) : 3;
-    }
+    static_assert(kStages == mix_stages(N), "stage count");
+    static constexpr int radix(int s) { return mix_radix(N, s); }
 };
 
-template <int R, int NS, int N, int TL, bool INV>
+// One stage of a compile-time line; OFF: this stage's twiddle table (stage_tw_off).
+template <int R, int NS, int N, int TL, bool INV, int OFF>
 __device__ __forceinline__ void mix_stage(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
-    constexpr int M = N / R, BM = (M + TL - 1) / TL, TWS = N / (NS * R);
+    constexpr int M = N / R, BM = (M + TL - 1) / TL;
     float2 v[BM][R];
     if (act) {
 #pragma unroll
@@ -232,7 +255,7 @@ __device__ __forceinline__ void mix_stage(float2* __restrict__ buf, const float2
                 if (NS > 1) {
 #pragma unroll
                     for (int r = 1; r < R; ++r) {
-                        float2 w = __ldg(&tw[r * k * TWS]);
+                        float2 w = __ldg(&tw[N + OFF + (r - 1) * NS + k]);
                         if (INV) w.y = -w.y;
                         v[b][r] = cmul(v[b][r], w);
                     }
@@ -251,7 +274,7 @@ template <int N, int TL, bool INV, int S = 0, int NS = 1>
 __device__ __forceinline__ void mix_fft(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
     if constexpr (S < Mix<N>::kStages) {
         constexpr int R = Mix<N>::radix(S);
-        mix_stage<R, NS, N, TL, INV>(buf, tw, t, act);
+        mix_stage<R, NS, N, TL, INV, stage_tw_off(N, S)>(buf, tw, t, act);
         mix_fft<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
     }
 }
@@ -261,7 +284,7 @@ template <int N, int TL, bool INV, int S, int NS>
 __device__ __forceinline__ void mix_mid(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act) {
     if constexpr (S < Mix<N>::kStages - 1) {
         constexpr int R = Mix<N>::radix(S);
-        mix_stage<R, NS, N, TL, INV>(buf, tw, t, act);
+        mix_stage<R, NS, N, TL, INV, stage_tw_off(N, S)>(buf, tw, t, act);
         mix_mid<N, TL, INV, S + 1, NS * R>(buf, tw, t, act);
     }
 }
@@ -303,10 +326,11 @@ __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float
                 float2 v[RL];
 #pragma unroll
                 for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
-                // k = j mod NSL = j: twiddles w^{r·j} of the full length
+                // k = j mod NSL = j
+                constexpr int OFFL = stage_tw_off(N, MX::kStages - 1);
 #pragma unroll
                 for (int r = 1; r < RL; ++r) {
-                    float2 w = __ldg(&tw[r * j]);
+                    float2 w = __ldg(&tw[N + OFFL + (r - 1) * NSL + j]);
                     if (INV) w.y = -w.y;
                     v[r] = cmul(v[r], w);
                 }
