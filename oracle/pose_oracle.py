@@ -9,6 +9,12 @@ Restates, in NumPy:
   2-px ramp inside the moving image's valid border;
 * ``scoreFromMoments`` (``src/moments.zig:91-172``): the score and its gradient coefficients;
 * the tangent gradient and Gauss–Newton matrix (``shaders/smi.wgsl:1123-1272``, tangent_grad);
+* the cubic B-spline free-form deformation on top of the pose (``shaders/smi.wgsl:198-240``
+  cubic_w / dest_half / ffd_disp; its use in overlap_moments 1003-1016 and tangent_grad
+  1168-1186: on the fixed image's lattice the displacement moves the fixed pixel before H⁻¹, on
+  the moving image's lattice it moves the sample after it) and the score's gradient over the
+  control points (``ffd_grad`` 1275-1417; ``src/pair.zig:387-410`` ffdGrad: symmetric
+  ½ (g_fwd − g_inv) with the inverse direction's spline negated on the other image);
 * the symmetric pair (``src/pair.zig:162-184, 241-268``) and the pose algebra
   (``src/lie.zig``: destN 27-35, inv3 85-117, hat 120-141, expm3 143-163, composeN 182-185,
   vee 187-204, generators 209-224, adjointGrad 227-241).
@@ -118,16 +124,57 @@ def _ramp(v, lo, hi):
     return ca * cb, da * cb + ca * db
 
 
-def sample(fa, H, bw, bh):
-    """Moving features at every fixed pixel under H: values, gradients, weight and its gradient,
-    the homogeneous sample position and the pixel grid (1-based)."""
+def cubic_w(t):
+    """The cubic B-spline's four basis weights at t ∈ [0, 1] (smi.wgsl cubic_w)."""
+    t2, t3 = t * t, t * t * t
+    return np.stack([(1 - t) ** 3 / 6, (3 * t3 - 6 * t2 + 4) / 6, (-3 * t3 + 3 * t2 + 3 * t + 1) / 6, t3 / 6])
+
+
+def _lattice(xf, yf, rw, rh, g):
+    """Per point: the lattice cell (iu, iv) and the 4 + 4 basis weights of a g × g lattice over
+    an rw × rh image; spacing (rw − 1)/(g − 1)."""
+    spx, spy = max(rw - 1.0, 1.0) / (g - 1), max(rh - 1.0, 1.0) / (g - 1)
+    su, sv = xf / spx, yf / spy
+    iu, iv = np.floor(su).astype(np.int64), np.floor(sv).astype(np.int64)
+    return iu, iv, cubic_w(np.clip(su - iu, 0, 1)), cubic_w(np.clip(sv - iv, 0, 1))
+
+
+def ffd_disp(xf, yf, rw, rh, ffd):
+    """Displacement in pixels at 0-based points (xf, yf) of the lattice's rw × rh image:
+    Σ B_i(u) B_j(v) c_ij · (rw/2, rh/2), clamped lattice indices, 0 outside the image."""
+    g, cps = int(ffd["g"]), np.asarray(ffd["cps"], np.float64)
+    out = np.zeros((2,) + np.shape(xf))
+    inside = ~((xf < 0) | (yf < 0) | (xf > rw - 1) | (yf > rh - 1))
+    iu, iv, bu, bv = _lattice(xf, yf, rw, rh, g)
+    hx, hy = max(rw, 1.0) * 0.5, max(rh, 1.0) * 0.5
+    for jj in range(4):
+        j = np.clip(iv - 1 + jj, 0, g - 1)
+        for ii in range(4):
+            i = np.clip(iu - 1 + ii, 0, g - 1)
+            w = bu[ii] * bv[jj]
+            o = (j * g + i) * 2
+            out[0] += w * cps[o] * hx
+            out[1] += w * cps[o + 1] * hy
+    return np.where(inside, out, 0.0)
+
+
+def sample(fa, H, bw, bh, ffd=None):
+    """Moving features at every fixed pixel under H (and the spline ffd = dict(g, cps, source),
+    or None): values, gradients, weight and its gradient, the homogeneous sample position H⁻¹X,
+    the pixel vector X (moved by a fixed-image lattice) and the pixel grid."""
     _, ah, aw = fa.shape
     y, x = np.mgrid[0:bh, 0:bw].astype(np.float64)
     X = np.stack([x + 1, y + 1, np.ones_like(x)])
+    if ffd is not None and not ffd["source"]:
+        d = ffd_disp(x, y, bw, bh, ffd)
+        X = np.stack([x + 1 + d[0], y + 1 + d[1], np.ones_like(x)])
     ph = np.tensordot(inv3(H), X, 1)
     okz = np.abs(ph[2]) >= 1e-8
     pz = np.where(okz, ph[2], 1.0)
     fx, fy = ph[0] / pz - 1, ph[1] / pz - 1
+    if ffd is not None and ffd["source"]:
+        d = ffd_disp(fx, fy, aw, ah, ffd)
+        fx, fy = fx + d[0], fy + d[1]
     ok = okz & (fx >= 2) & (fy >= 2) & (fx <= aw - 3) & (fy <= ah - 3)
     tx, dtx = _ramp(fx, 2, aw - 3)
     ty, dty = _ramp(fy, 2, ah - 3)
@@ -142,14 +189,14 @@ def sample(fa, H, bw, bh):
         "gy": (v01 - v00) * (1 - ax) + (v11 - v10) * ax,
         "w": np.where(ok, tx * ty, 0.0),
         "dw": np.where(ok, np.stack([dtx * ty, tx * dty]), 0.0),
-        "ph": ph, "X": X, "ok": ok,
+        "ph": ph, "X": X, "ok": ok, "xy": (x, y), "f0": (ph[0] / pz - 1, ph[1] / pz - 1),
     }
 
 
-def moments(fa, fb, H):
+def moments(fa, fb, H, ffd=None):
     """The 45 overlap sums of a (moving) onto b (fixed) at H (moments.zig layout)."""
     fb = fb.astype(np.float64)
-    S = sample(fa, H, fb.shape[2], fb.shape[1])
+    S = sample(fa, H, fb.shape[2], fb.shape[1], ffd)
     w, va, vb = S["w"], S["va"], fb
     s = [w.sum()] + [(w * va[i]).sum() for i in range(4)] + [(w * vb[j]).sum() for j in range(4)]
     s += [(w * va[i] * vb[j]).sum() for i in range(4) for j in range(4)]
@@ -224,20 +271,72 @@ def score_from_moments(st, exact=True, ridge=RIDGE):
     return score, coef
 
 
-def tangent(fa, fb, H, coef, homog=True, hess=True):
-    """(grad[8], GN[8×8]) of one direction at H from its coefficients (tangent_grad)."""
-    fb = fb.astype(np.float64)
-    bh, bw = fb.shape[1:]
-    S = sample(fa, H, bw, bh)
-    va, vb, gx, gy, wt = S["va"], fb, S["gx"], S["gy"], S["w"]
-    W, mb, Mh, ma, g, Q = (coef[0:16].reshape(4, 4), coef[16:20], coef[20:36].reshape(4, 4), coef[36:40],
-                           coef[40:85], coef[85:101].reshape(4, 4))
+def _dva(S, vb, coef):
+    """Per pixel ∂S/∂v_a (score_dva) and the taper's boundary value (boundary_value)."""
+    va = S["va"]
+    W, mb, Mh, ma, g = coef[0:16].reshape(4, 4), coef[16:20], coef[20:36].reshape(4, 4), coef[36:40], coef[40:85]
     tb = vb - mb[:, None, None]
     ta = va - ma[:, None, None]
     ra = 2 * (np.tensordot(W, tb, 1) - np.tensordot(Mh, ta, 1))
     bwv = g[0] + sum(g[1 + i] * va[i] + g[5 + i] * vb[i] for i in range(4))
     bwv = bwv + sum(g[9 + 4 * i + j] * va[i] * vb[j] for i in range(4) for j in range(4))
     bwv = bwv + sum(g[25 + k] * va[i] * va[j] + g[35 + k] * vb[i] * vb[j] for k, (i, j) in enumerate(TRI))
+    return ra, bwv
+
+
+def ffd_grad(fa, fb, H, coef, ffd):
+    """∂score/∂(control points) of one direction at H (2·g·g, x then y per point; ffd_grad):
+    every valid pixel's (∂S/∂v_a)·∇v_a and taper term, times the sample's motion per control
+    point (its basis weight × half the lattice image, through H⁻¹ on a fixed-image lattice)."""
+    fb = fb.astype(np.float64)
+    _, ah, aw = fa.shape
+    bh, bw = fb.shape[1:]
+    g = int(ffd["g"])
+    S = sample(fa, H, bw, bh, ffd)
+    ra, bwv = _dva(S, fb, coef)
+    ok, wt, gx, gy = S["ok"], S["w"], S["gx"], S["gy"]
+    tpx, tpy = S["dw"][0], S["dw"][1]
+    src = bool(ffd["source"])
+    lw, lh = (aw, ah) if src else (bw, bh)
+    hx, hy = max(lw, 1.0) * 0.5, max(lh, 1.0) * 0.5
+    px_, py_ = S["f0"] if src else S["xy"]
+    iu, iv, bu, bv = _lattice(px_, py_, lw, lh, g)
+    Hi, ph = inv3(H), S["ph"]
+    z = np.where(np.abs(ph[2]) >= 1e-8, ph[2], 1.0)
+    z2 = np.maximum(z * z, 1e-12)
+    ax_ = np.sum(ra * gx, 0)
+    ay_ = np.sum(ra * gy, 0)
+    grad = np.zeros(2 * g * g)
+    for jj in range(4):
+        j = np.clip(iv - 1 + jj, 0, g - 1)
+        for ii in range(4):
+            i = np.clip(iu - 1 + ii, 0, g - 1)
+            bk = bu[ii] * bv[jj]
+            if src:
+                dxx, dyx, dxy, dyy = bk * hx, 0.0 * bk, 0.0 * bk, bk * hy
+            else:
+                wx = Hi[:, 0][:, None, None] * (bk * hx)
+                wy = Hi[:, 1][:, None, None] * (bk * hy)
+                dxx = (wx[0] * z - ph[0] * wx[2]) / z2
+                dyx = (wx[1] * z - ph[1] * wx[2]) / z2
+                dxy = (wy[0] * z - ph[0] * wy[2]) / z2
+                dyy = (wy[1] * z - ph[1] * wy[2]) / z2
+            gxv = np.where(ok, wt * (ax_ * dxx + ay_ * dyx) + bwv * (tpx * dxx + tpy * dyx), 0.0)
+            gyv = np.where(ok, wt * (ax_ * dxy + ay_ * dyy) + bwv * (tpx * dxy + tpy * dyy), 0.0)
+            idx = (j * g + i).ravel()
+            np.add.at(grad, 2 * idx, gxv.ravel())
+            np.add.at(grad, 2 * idx + 1, gyv.ravel())
+    return grad
+
+
+def tangent(fa, fb, H, coef, homog=True, hess=True, ffd=None):
+    """(grad[8], GN[8×8]) of one direction at H from its coefficients (tangent_grad)."""
+    fb = fb.astype(np.float64)
+    bh, bw = fb.shape[1:]
+    S = sample(fa, H, bw, bh, ffd)
+    va, vb, gx, gy, wt = S["va"], fb, S["gx"], S["gy"], S["w"]
+    Q = coef[85:101].reshape(4, 4)
+    ra, bwv = _dva(S, vb, coef)
     ok = S["ok"]
     cx = np.where(ok, wt * np.sum(ra * gx, 0) + bwv * S["dw"][0], 0.0)
     cy = np.where(ok, wt * np.sum(ra * gy, 0) + bwv * S["dw"][1], 0.0)
@@ -265,29 +364,59 @@ def tangent(fa, fb, H, coef, homog=True, hess=True):
 
 # ── the pair ──────────────────────────────────────────────────────────────────────────────────
 
-def pair_eval(fa, fb, H, exact=True, symmetric=True, homog=True, grad=False, hess=False):
+def ffd_live(ffd):
+    """A spline that moves anything (src/pair.zig:32-36 live): on, some |c| > 1e-12."""
+    return ffd is not None and bool(np.any(np.abs(np.asarray(ffd["cps"], np.float64)) > 1e-12))
+
+
+def ffd_adjoint(ffd):
+    """The inverse direction's spline: negated, on the other image (pair.zig invCfg)."""
+    return None if ffd is None else dict(g=ffd["g"], cps=-np.asarray(ffd["cps"], np.float64), source=not ffd["source"])
+
+
+def pair_ffd_grad(fa, fb, H, ffd, exact=True, symmetric=True):
+    """(score, ∇ over the control points) at H (src/pair.zig:387-410 ffdGrad): the forward
+    direction with the spline as given; when symmetric and the spline is live, the mean with the
+    inverse direction, gradient ½ (g_fwd − g_inv)."""
+    H = np.asarray(H, np.float64).reshape(3, 3)
+    mf = moments(fa, fb, H, ffd)
+    sf, cf = score_from_moments(mf, exact)
+    gf = ffd_grad(fa, fb, H, cf, ffd) if mf[0] >= MIN_N else np.zeros(2 * ffd["g"] ** 2)
+    if not symmetric or not ffd_live(ffd):
+        return sf, gf
+    Hi = inv3(H)
+    adj = ffd_adjoint(ffd)
+    mi = moments(fb, fa, Hi, adj)
+    si, ci = score_from_moments(mi, exact)
+    gi = ffd_grad(fb, fa, Hi, ci, adj) if mi[0] >= MIN_N else np.zeros_like(gf)
+    return 0.5 * (sf + si), 0.5 * (gf - gi)
+
+
+def pair_eval(fa, fb, H, exact=True, symmetric=True, homog=True, grad=False, hess=False, ffd=None):
     """Scores (mean, fwd, inv) and, with grad, the symmetric gradient and GN matrix at H
-    (src/pair.zig parts / sym)."""
+    (src/pair.zig parts / sym); ffd: the engine's spline (used only when live)."""
     H = np.asarray(H, np.float64).reshape(3, 3)
     nk = n_keys(homog)
-    mf = moments(fa, fb, H)
+    fwd_ffd = ffd if ffd_live(ffd) else None
+    inv_ffd = ffd_adjoint(fwd_ffd)
+    mf = moments(fa, fb, H, fwd_ffd)
     sf, cf = score_from_moments(mf, exact)
     out = {"fwd": sf, "sums": mf, "n": mf[0]}
     if symmetric:
         Hi = inv3(H)
-        mi = moments(fb, fa, Hi)
+        mi = moments(fb, fa, Hi, inv_ffd)
         si, ci = score_from_moments(mi, exact)
         out.update(inv=si, mean=0.5 * (sf + si))
     else:
         out.update(inv=None, mean=sf)
     if not grad:
         return out
-    gf, Af = tangent(fa, fb, H, cf, homog, hess) if mf[0] >= MIN_N else (np.zeros(8), np.zeros((8, 8)))
+    gf, Af = tangent(fa, fb, H, cf, homog, hess, fwd_ffd) if mf[0] >= MIN_N else (np.zeros(8), np.zeros((8, 8)))
     gf, Af = gf[:nk], Af[:nk, :nk]
     if not symmetric:
         out.update(grad=gf, hess=Af)
         return out
-    gb, Ab = tangent(fb, fa, Hi, ci, homog, hess) if mi[0] >= MIN_N else (np.zeros(8), np.zeros((8, 8)))
+    gb, Ab = tangent(fb, fa, Hi, ci, homog, hess, inv_ffd) if mi[0] >= MIN_N else (np.zeros(8), np.zeros((8, 8)))
     gb, Ab = gb[:nk], Ab[:nk, :nk]
     _, ah, aw = fa.shape
     _, bh, bw = fb.shape

@@ -1,0 +1,180 @@
+"""GPU parity of the B-spline on top of the pose (settings ffd, ffd_grid, ffd_source; zc_set_ffd,
+zc_get_ffd, zc_ffd_gradient) against the CPU oracle, through the C ABI.
+
+Tolerances as for the spline-free pose path: scores within 1e-5 relative, the tangent gradient
+within 1e-3 in norm and the Gauss–Newton matrix within 1e-3 of its largest entry. The gradient
+over the control points: most entries within 1e-6 of the largest (median), and within 5e-3 in
+norm: each control point sums only its own support, where one pixel whose sample lies within
+float32 rounding of the taper's inner end (the taper is 0 there but its slope is not, so the
+pixel's boundary term jumps in or out) moves an entry by ~1e-3 of the norm."""
+import numpy as np
+import pytest
+
+import zcmir_b200 as zc
+from oracle import pose_oracle as P
+from zcmir_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pair():
+    m, f, H = synth.pair_remap(n=200, shift=(9, -6), seed=1)
+    return m, f[:180, :190], H
+
+
+def _close(got, ref):
+    d = np.abs(got - ref)
+    assert np.median(d) <= 1e-6 * np.abs(ref).max(), (np.median(d), np.abs(ref).max())
+    assert np.linalg.norm(d) <= 5e-3 * np.linalg.norm(ref), (np.linalg.norm(d), np.linalg.norm(ref))
+
+
+def _cps(g, seed, amp=0.01):
+    return (amp * np.random.default_rng(seed).standard_normal(2 * g * g)).astype(np.float32)
+
+
+@pytest.mark.parametrize("source,g", [(False, 4), (True, 5)])
+def test_scores_and_pose_gradient_with_a_live_spline(pair, source, g):
+    m, f, H = pair
+    cps = _cps(g, 7 + g)
+    with zc.Registrar(half=False, ffd=True, ffd_grid=g, ffd_source=source) as reg:
+        reg.set_images(m, f, preprocess=False)
+        A, B = reg.features(0), reg.features(1)
+        reg.ffd = cps
+        np.testing.assert_array_equal(reg.ffd, cps)
+        sc = reg.score(H)
+        gr = reg.gradient(H, hess=True)
+        mom = reg.moments(H)
+    ffd = dict(g=g, cps=cps.astype(np.float64), source=source)
+    ref = P.pair_eval(A, B, H, grad=True, hess=True, ffd=ffd)
+    assert abs(sc.fwd - ref["fwd"]) <= 1e-5 * abs(ref["fwd"])
+    assert abs(sc.inv - ref["inv"]) <= 1e-5 * abs(ref["inv"])
+    np.testing.assert_allclose(mom, ref["sums"], rtol=0, atol=1e-5 * np.abs(ref["sums"]).max())
+    assert np.linalg.norm(gr.grad - ref["grad"]) <= 1e-3 * np.linalg.norm(ref["grad"])
+    assert np.abs(gr.hess - ref["hess"]).max() <= 1e-3 * np.abs(ref["hess"]).max()
+    # the spline moves the score: the same pose without it scores differently
+    plain = P.pair_eval(A, B, H)
+    assert abs(plain["mean"] - ref["mean"]) > 1e-4 * abs(ref["mean"])
+
+
+@pytest.mark.parametrize("source,symmetric", [(False, True), (True, True), (False, False)])
+def test_control_point_gradient_matches_oracle(pair, source, symmetric):
+    m, f, H = pair
+    g = 4
+    cps = _cps(g, 3)
+    with zc.Registrar(half=False, ffd=True, ffd_grid=g, ffd_source=source, symmetric=symmetric) as reg:
+        reg.set_images(m, f, preprocess=False)
+        A, B = reg.features(0), reg.features(1)
+        reg.ffd = cps
+        s, gr = reg.ffd_gradient(H)
+    ref_s, ref_g = P.pair_ffd_grad(A, B, H, dict(g=g, cps=cps.astype(np.float64), source=source), symmetric=symmetric)
+    assert gr.shape == (2 * g * g,)
+    assert abs(s - ref_s) <= 1e-5 * abs(ref_s)
+    _close(gr, ref_g)
+
+
+def test_lattices_past_one_chunk_and_spline_rules(pair):
+    """A 7 × 7 lattice (98 parameters, four 16-point chunks) matches the oracle; the zero spline
+    is not live (scores equal the spline-free ones) but still has a gradient, forward only
+    (src/pair.zig:387-398); the spline off gives score 0 and a zero gradient; a wrong number of
+    control points is refused; a new lattice size zeroes them; the no-alloc scores refuse a live
+    spline."""
+    m, f, H = pair
+    with zc.Registrar(half=False, ffd=True, ffd_grid=7) as reg:
+        reg.set_images(m, f, preprocess=False)
+        A, B = reg.features(0), reg.features(1)
+        assert reg.ffd.shape == (98,) and not reg.ffd.any()
+        s0 = reg.score(H)
+        ref0 = P.pair_eval(A, B, H)
+        assert abs(s0.mean - ref0["mean"]) <= 1e-5 * abs(ref0["mean"])
+        sz, gz = reg.ffd_gradient(H)
+        rs, rg = P.pair_ffd_grad(A, B, H, dict(g=7, cps=np.zeros(98), source=False))
+        assert abs(sz - ref0["fwd"]) <= 1e-5 * abs(ref0["fwd"]) and abs(sz - rs) <= 1e-5 * abs(rs)
+        _close(gz, rg)
+        cps = _cps(7, 11, 0.006)
+        reg.ffd = cps
+        s7, g7 = reg.ffd_gradient(H)
+        r7s, r7g = P.pair_ffd_grad(A, B, H, dict(g=7, cps=cps.astype(np.float64), source=False))
+        assert abs(s7 - r7s) <= 1e-5 * abs(r7s)
+        _close(g7, r7g)
+        with pytest.raises(RuntimeError, match="BadControlPoints"):
+            reg.ffd = np.zeros(10, np.float32)
+        Hs = np.ascontiguousarray(H, np.float64).reshape(1, 9)
+        out = np.zeros(3)
+        rc = reg._lib.zcb_score_static(reg._e, Hs.ctypes.data_as(zc._native.f64p), 1, out.ctypes.data_as(zc._native.f64p))
+        with pytest.raises(RuntimeError, match="spline is live"):
+            reg._check(rc, "score_static")
+        reg.configure(ffd_grid=5)
+        assert reg.ffd.shape == (50,) and not reg.ffd.any()
+        reg.configure(ffd=False)
+        s, gv = reg.ffd_gradient(H)
+        assert s == 0.0 and gv.shape == (50,) and not gv.any()
+
+
+@pytest.mark.parametrize("source", [False, True])
+def test_displacement_field_with_the_spline(pair, source):
+    """zc_displacement (src/export.zig:64-106): the composed warp H then the spline over the fixed
+    image against the oracle's displacement, and H alone with the spline off."""
+    m, f, H = pair
+    g = 5
+    cps = _cps(g, 21, 0.02)
+    with zc.Registrar(half=False, ffd=True, ffd_grid=g, ffd_source=source) as reg:
+        reg.set_images(m, f, preprocess=False)
+        reg.pose = H
+        reg.ffd = cps
+        d = reg.displacement()
+        reg.configure(ffd=False)
+        d0 = reg.displacement()
+    fh, fw = f.shape
+    mh, mw = m.shape
+    y, x = np.mgrid[0:fh, 0:fw].astype(np.float64)
+    Hi = np.linalg.inv(H)
+    ffd = dict(g=g, cps=cps.astype(np.float64), source=source)
+    if source:
+        q = np.tensordot(Hi, np.stack([x + 1, y + 1, np.ones_like(x)]), 1)
+        sx, sy = q[0] / q[2] - 1, q[1] / q[2] - 1
+        dd = P.ffd_disp(sx, sy, mw, mh, ffd)
+        px, py = sx + dd[0], sy + dd[1]
+    else:
+        dd = P.ffd_disp(x, y, fw, fh, ffd)
+        q = np.tensordot(Hi, np.stack([x + 1 + dd[0], y + 1 + dd[1], np.ones_like(x)]), 1)
+        px, py = q[0] / q[2] - 1, q[1] / q[2] - 1
+    np.testing.assert_allclose(d[..., 0], px - x, atol=1e-4)
+    np.testing.assert_allclose(d[..., 1], py - y, atol=1e-4)
+    q = np.tensordot(Hi, np.stack([x + 1, y + 1, np.ones_like(x)]), 1)
+    np.testing.assert_allclose(d0[..., 0], q[0] / q[2] - 1 - x, atol=1e-4)
+
+
+def _bilinear(img, X, Y):
+    h, w = img.shape
+    x0 = np.clip(np.floor(X).astype(int), 0, w - 2)
+    y0 = np.clip(np.floor(Y).astype(int), 0, h - 2)
+    fx, fy = np.clip(X - x0, 0, 1), np.clip(Y - y0, 0, 1)
+    return ((img[y0, x0] * (1 - fx) + img[y0, x0 + 1] * fx) * (1 - fy)
+            + (img[y0 + 1, x0] * (1 - fx) + img[y0 + 1, x0 + 1] * fx) * fy)
+
+
+def test_register_with_spline_recovers_a_smooth_warp():
+    """register(spline=True) (python/zcmir/api.py:291-325): a 256² blob field against itself under
+    a smooth non-rigid warp (amplitude 3 px) and a small shift; the spline stage moves the control
+    points, raises the score over the homography-only result and brings the displacement field
+    closer to the true one."""
+    rng = np.random.default_rng(8)
+    n = 256
+    fixed = synth.blob_field(n, n, rng).astype(np.float32)
+    Y, X = np.mgrid[0:n, 0:n].astype(np.float64)
+    vx = 3.0 * np.sin(2 * np.pi * Y / n) * np.cos(np.pi * X / n) + 1.5
+    vy = 3.0 * np.cos(2 * np.pi * X / n) * np.sin(np.pi * Y / n) - 1.0
+    moving = _bilinear(fixed.astype(np.float64), X + vx, Y + vy).astype(np.float32)
+    true_d = -np.stack([vx, vy], -1)   # fixed x ↔ moving x − v(x), to first order
+    r0 = zc.register(moving, fixed, init=np.eye(3), preprocess=False, half=False)
+    r1 = zc.register(moving, fixed, init=np.eye(3), spline=True, preprocess=False, half=False)
+    assert r1.spline is not None and r1.spline.shape == (32,) and np.abs(r1.spline).max() > 0
+    assert r1.lattice == 4 and "spline 4×4" in repr(r1)
+    assert r1.score > r0.score
+    inner = (slice(24, n - 24), slice(24, n - 24))
+    e0 = np.linalg.norm(r0.displacement()[inner] - true_d[inner], axis=-1).mean()
+    e1 = np.linalg.norm(r1.displacement()[inner] - true_d[inner], axis=-1).mean()
+    assert e1 < 0.8 * e0, (e0, e1)
+    w = r1.warp(moving)
+    assert w.shape == fixed.shape and w.dtype == moving.dtype

@@ -86,3 +86,44 @@ def test_pose_algebra():
     # adjointGrad pulls a moving-frame increment back: the identity pose of equal frames negates
     g = np.arange(1.0, 9.0)
     np.testing.assert_allclose(P.adjoint_grad(g, np.eye(3), True, 64, 64, 64, 64), -g, atol=1e-12)
+
+
+@pytest.mark.parametrize("source", [False, True])
+def test_ffd_gradient_matches_finite_differences(landsat, source):
+    """The control-point gradient of the oracle (smi.wgsl ffd_grad restated) against central
+    differences of the pair score over the control points, both lattice placements, symmetric
+    (src/pair.zig:387-410). A 4 × 4 lattice with a small random warp on the landsat-b truth."""
+    A, B, truth = landsat
+    # a 240² window of the fixed image against the whole moving one (the CPU suite stays quick)
+    T = np.array([[1, 0, -200.0], [0, 1, -180.0], [0, 0, 1]])
+    Bw = B[:, 180:420, 200:440]
+    H = T @ truth
+    rng = np.random.default_rng(3 if source else 4)
+    ffd = dict(g=4, cps=0.004 * rng.standard_normal(32), source=source)
+    s0, g_an = P.pair_ffd_grad(A, Bw, H, ffd)
+    assert np.isfinite(s0) and np.linalg.norm(g_an) > 0
+    h = 2e-5
+    ks = np.argsort(-np.abs(g_an))[:8]   # the eight largest components
+    g_fd = np.zeros(len(ks))
+    for n, k in enumerate(ks):
+        for sgn in (1, -1):
+            c = ffd["cps"].copy()
+            c[k] += sgn * h
+            s, _ = P.pair_ffd_grad(A, Bw, H, dict(ffd, cps=c))
+            g_fd[n] += sgn * s / (2 * h)
+    # bilinear sampling makes the score piecewise smooth: agreement to a few per cent
+    assert np.linalg.norm(g_fd - g_an[ks]) < 0.05 * np.linalg.norm(g_fd), (g_fd, g_an[ks])
+
+
+def test_ffd_off_or_zero_leaves_the_pose_path():
+    """A spline with all-zero control points moves nothing: the moments equal the spline-free
+    ones (both placements), and the pair scores ignore a spline that is not live."""
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((4, 40, 48))
+    B = rng.standard_normal((4, 44, 40))
+    H = np.array([[1.0, 0.02, 1.5], [-0.01, 0.99, -2.0], [0, 0, 1]])
+    for source in (False, True):
+        z = dict(g=5, cps=np.zeros(50), source=source)
+        np.testing.assert_array_equal(P.moments(A, B, H, z), P.moments(A, B, H))
+        assert not P.ffd_live(z)
+        assert P.pair_eval(A, B, H, ffd=z)["mean"] == P.pair_eval(A, B, H)["mean"]

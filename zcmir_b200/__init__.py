@@ -297,6 +297,19 @@ class Registrar:
         a, p = _mat(H)
         self._lib.zc_set_pose(self._e, p)
 
+    @property
+    def ffd(self):
+        """The B-spline's control points: 2·g·g float32 (x, y per point, row by row), in half-image
+        units of the lattice's image; g = settings["ffd_grid"]."""
+        buf = np.zeros(512, np.float32)
+        n = self._lib.zc_get_ffd(self._e, _fp(buf), buf.size)
+        return buf[:n].copy()
+
+    @ffd.setter
+    def ffd(self, cps):
+        a = np.ascontiguousarray(cps, dtype=np.float32).ravel()
+        self._check(self._lib.zc_set_ffd(self._e, _fp(a), a.size), "set_ffd")
+
     def _Hp(self, H):
         return _mat(self.pose if H is None else H)
 
@@ -315,6 +328,25 @@ class Registrar:
         g = np.array(r.grad[:nk])
         Hm = np.array(r.hess[: nk * nk]).reshape(nk, nk) if r.has_hess else None
         return Gradient(r.score, r.fwd, None if math.isnan(r.inv) else r.inv, r.n, g, Hm)
+
+    def displacement(self):
+        """The composed warp at the engine's pose (and spline, when on) over the fixed image as
+        (h, w, 2) float32: x_moving − x_fixed, 0-based pixels."""
+        w, h = self.image_size(1)
+        out = np.empty((h, w, 2), np.float32)
+        self._check(self._lib.zc_displacement(self._e, _fp(out), out.size), "displacement")
+        return out
+
+    def ffd_gradient(self, H=None):
+        """(score, gradient over the spline's 2·g·g control points) at H; with the spline off
+        (settings["ffd"] False) the score is 0 and the gradient zero."""
+        a, p = self._Hp(H)
+        s = ctypes.c_double()
+        g = np.zeros(512, np.float64)
+        self._check(self._lib.zc_ffd_gradient(self._e, p, ctypes.byref(s), g.ctypes.data_as(_native.f64p), g.size),
+                    "ffd_gradient")
+        n = 2 * min(max(int(self.settings["ffd_grid"]), 2), 16) ** 2
+        return s.value, g[:n].copy()
 
     def shift_map(self, H=None, *, exact=None, calibrated=None, resolution=1024, return_map=True, out=None):
         """Score every translation of the moving image about pose H. Without exact / calibrated the

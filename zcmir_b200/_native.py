@@ -85,6 +85,10 @@ SIGS = {
     "zc_shift_map_set": ([P, f64p, ctypes.POINTER(ShiftResult), f32p, SZ], I32),
     "zc_rs_map": ([P, f64p, f64p, U32, ctypes.POINTER(RsResult), f32p, f32p, f32p, SZ], I32),
     "zc_canvas": ([P, f64p, U32, ctypes.POINTER(Canvas)], I32),
+    "zc_set_ffd": ([P, f32p, SZ], I32),
+    "zc_get_ffd": ([P, f32p, SZ], SZ),
+    "zc_ffd_gradient": ([P, f64p, f64p, f64p, SZ], I32),
+    "zc_displacement": ([P, f32p, SZ], I32),
     "zc_result_sizes": ([u32p], None),
     "zcb_bench_maps": ([P, f64p, U32, U32, U32, U32, f64p, SZ], I32),
     "zcb_score_static": ([P, f64p, U32, f64p], I32),

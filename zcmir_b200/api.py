@@ -47,14 +47,31 @@ def settings():
 _SPELL = {"model": "group", "spline_lattice": "ffd_grid", "spline_stiffness": "ffd_stiffness"}
 
 
-def _resolve(model="homography", **kw):
+def _lattice(spline):
+    """spline= → the lattice size: True 4, False/0 none, else 2–16 (python/zcmir/api.py:87-95)."""
+    if spline is True:
+        return 4
+    if not spline:
+        return 0
+    g = int(spline)
+    if not 2 <= g <= 16:
+        raise ValueError("spline: True (a 4×4 lattice) or the lattice size 2–16")
+    return g
+
+
+def _resolve(model="homography", spline=False, **kw):
     """Keyword arguments → engine settings (defaults + these), with the names checked
-    (python/zcmir/api.py:65-84)."""
+    (python/zcmir/api.py:65-84). The spline stays off: register() turns it on for its second
+    stage."""
     _engine()
     s = dict(_DEFAULTS)
     if model not in ("affine", "homography"):
         raise ValueError(f'model: "affine" or "homography", not {model!r}')
     s["group"] = model
+    lattice = _lattice(spline)
+    s["ffd"] = False
+    if lattice:
+        s["ffd_grid"] = lattice
     for k, v in kw.items():
         k = _SPELL.get(k, k)
         if k not in s:
@@ -92,10 +109,50 @@ def _prepare(moving, fixed, preprocess, kw):
     return reg, s, m, f
 
 
+def _field_from_H(H, fixed_shape):
+    """x_moving − x_fixed (0-based) over the fixed grid for a pose H (moving → fixed, 1-based)."""
+    h, w = fixed_shape[:2]
+    Hi = np.linalg.inv(np.asarray(H, np.float64))
+    Y, X = np.mgrid[1:h + 1, 1:w + 1].astype(np.float64)
+    d = Hi[2, 0] * X + Hi[2, 1] * Y + Hi[2, 2]
+    out = np.empty((h, w, 2), np.float32)
+    out[..., 0] = (Hi[0, 0] * X + Hi[0, 1] * Y + Hi[0, 2]) / d - X
+    out[..., 1] = (Hi[1, 0] * X + Hi[1, 1] * Y + Hi[1, 2]) / d - Y
+    return out
+
+
+def warp_image(image, field, fill=0):
+    """Resample image (gray or with channels, any dtype) on a displacement field (h, w, 2:
+    x_moving − x_fixed, 0-based), bilinear. Returns (warped, mask of fixed pixels inside)."""
+    img = np.asarray(image)
+    sh, sw = img.shape[:2]
+    h, w = field.shape[:2]
+    Y, X = np.mgrid[0:h, 0:w].astype(np.float64)
+    mx, my = X + field[..., 0], Y + field[..., 1]
+    inside = (mx >= 0) & (my >= 0) & (mx <= sw - 1) & (my <= sh - 1)
+    x0 = np.clip(np.floor(mx).astype(np.int64), 0, max(sw - 2, 0))
+    y0 = np.clip(np.floor(my).astype(np.int64), 0, max(sh - 2, 0))
+    fx, fy = np.clip(mx - x0, 0, 1), np.clip(my - y0, 0, 1)
+    x1, y1 = np.minimum(x0 + 1, sw - 1), np.minimum(y0 + 1, sh - 1)
+    src = img.astype(np.float64)
+    if src.ndim == 3:
+        fx, fy, inside_c = fx[..., None], fy[..., None], inside[..., None]
+    else:
+        inside_c = inside
+    v = (src[y0, x0] * (1 - fx) + src[y0, x1] * fx) * (1 - fy) + (src[y1, x0] * (1 - fx) + src[y1, x1] * fx) * fy
+    v = np.where(inside_c, v, fill)
+    if np.issubdtype(img.dtype, np.integer):
+        info = np.iinfo(img.dtype)
+        v = np.clip(np.rint(v), info.min, info.max)
+    return v.astype(img.dtype), inside
+
+
 @dataclass
 class Registration:
-    """A registered pair (python/zcmir/api.py:205-222, without the spline and keypoint fields):
-    H maps moving pixel coordinates to fixed ones (row-major 3×3, 1-based)."""
+    """A registered pair (python/zcmir/api.py:205-290, without the keypoint fields): H maps moving
+    pixel coordinates to fixed ones (row-major 3×3, 1-based); with a spline, the full warp is H
+    followed by the B-spline (spline: its 2·lattice² control points), which displacement(),
+    fixed_to_moving() and warp() include."""
     H: np.ndarray
     score: float
     model: str
@@ -104,20 +161,50 @@ class Registration:
     method: str = "refine"
     iterations: int = 0
     redetected: bool = False
+    spline: np.ndarray | None = None
+    lattice: int = 0
+    _field: np.ndarray | None = None
 
     def __repr__(self):
-        return f"Registration({self.model}, score {self.score:.4g}, {self.method})"
+        sp = f", spline {self.lattice}×{self.lattice}" if self.spline is not None else ""
+        return f"Registration({self.model}{sp}, score {self.score:.4g}, {self.method})"
 
     def map_points(self, points):
-        """Moving (x, y) points (1-based, (n, 2)) to fixed coordinates by H."""
+        """Moving (x, y) points (1-based, (n, 2)) to fixed coordinates by H (the global model; a
+        spline's local correction is not included — fixed_to_moving() includes it)."""
         p = np.asarray(points, np.float64).reshape(-1, 2)
         q = np.c_[p, np.ones(len(p))] @ self.H.T
         return q[:, :2] / q[:, 2:]
 
+    def displacement(self):
+        """The full warp over the fixed image, (h, w, 2) float32: x_moving − x_fixed, 0-based."""
+        if self._field is not None:
+            return self._field
+        return _field_from_H(self.H, self.fixed_shape)
+
+    def fixed_to_moving(self, points):
+        """Fixed (x, y) points (1-based) to moving coordinates through the full warp."""
+        d = self.displacement()
+        p = np.asarray(points, np.float64).reshape(-1, 2) - 1
+        h, w = d.shape[:2]
+        x, y = np.clip(p[:, 0], 0, w - 1), np.clip(p[:, 1], 0, h - 1)
+        x0, y0 = np.minimum(np.floor(x).astype(int), w - 2), np.minimum(np.floor(y).astype(int), h - 2)
+        fx, fy = (x - x0)[:, None], (y - y0)[:, None]
+        v = (d[y0, x0] * (1 - fx) + d[y0, x0 + 1] * fx) * (1 - fy) + (d[y0 + 1, x0] * (1 - fx) + d[y0 + 1, x0 + 1] * fx) * fy
+        return p + v + 1
+
+    def warp(self, moving, fill=0, mask=False):
+        """The moving image resampled into the fixed frame through the full warp (bilinear, fill
+        outside); mask=True also returns the fixed pixels the moving image covers."""
+        out, m = warp_image(moving, self.displacement(), fill)
+        return (out, m) if mask else out
+
     def to_dict(self):
         return {"H": np.asarray(self.H).tolist(), "score": float(self.score), "model": self.model,
                 "moving_shape": list(self.moving_shape), "fixed_shape": list(self.fixed_shape), "method": self.method,
-                "iterations": int(self.iterations), "redetected": bool(self.redetected)}
+                "iterations": int(self.iterations), "redetected": bool(self.redetected),
+                "spline": None if self.spline is None else {"lattice": int(self.lattice),
+                                                            "coefficients": np.asarray(self.spline).tolist()}}
 
 
 def shift_map(moving, fixed, H=None, *, preprocess=True, **settings):
@@ -142,17 +229,34 @@ def score(moving, fixed, H, *, preprocess=True, **settings):
         return reg.score(np.asarray(H, np.float64)).mean
 
 
-def register(moving, fixed, *, init=None, model="homography", preprocess=True, **settings):
+def register(moving, fixed, *, init=None, model="homography", spline=False, preprocess=True, **settings):
     """Refine from ``init`` (keypoint detection is not part of this build, so ``init`` is
-    required): the climb from H, then the score at the result."""
+    required): the climb over the model from H; with spline (True: a 4×4 lattice, or the lattice
+    size 2–16; spline_stiffness, default 0.15, the bending penalty's wavelength in fractions of
+    the lattice's size), then a second climb of the B-spline together with the model
+    (python/zcmir/api.py:291-325)."""
     if init is None:
         raise ValueError("register: keypoint detection is not part of this build; pass init=H (or use search())")
+    lattice = _lattice(spline)
     with _LOCK:
-        reg, s, m, f = _prepare(moving, fixed, preprocess, dict(model=model, **settings))
+        reg, s, m, f = _prepare(moving, fixed, preprocess, dict(model=model, spline=spline, **settings))
         reg.pose = np.asarray(init, np.float64).reshape(3, 3)
         c = reg.climb()
-        return Registration(H=reg.pose, score=reg.score(reg.pose).mean, model=s["group"], moving_shape=m.shape,
-                            fixed_shape=f.shape, method="refine", iterations=c.iterations)
+        iters = c.iterations
+        cps = fld = None
+        if lattice:
+            reg.configure(ffd=True, ffd_grid=lattice)
+            reg.ffd = np.zeros(2 * lattice * lattice, np.float32)
+            c = reg.climb()
+            iters += c.iterations
+            cps = reg.ffd
+            fld = reg.displacement()
+        H = reg.pose
+        out = Registration(H=H, score=reg.score(H).mean, model=s["group"], moving_shape=m.shape, fixed_shape=f.shape,
+                           method="refine", iterations=iters, spline=cps, lattice=lattice, _field=fld)
+        if lattice:
+            reg.configure(ffd=False)
+        return out
 
 
 def refine(moving, fixed, H, **kw):

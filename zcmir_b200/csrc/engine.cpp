@@ -94,7 +94,9 @@ Engine::~Engine() {
     for (auto& s : stack_)
         for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack}) b->release();
     stack_res_.release();
-    for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_}) b->release();
+    for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_, &ffd_dev_, &ffd_out_,
+                      &ffd_pk_, &ffd_cells_, &ffd_coef_})
+        b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     cudaStreamDestroy(st);
 }

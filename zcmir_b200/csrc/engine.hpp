@@ -196,14 +196,38 @@ class Engine {
                     size_t out_len);
 
     // poses (engine_pose.cpp): both directions (or the forward one) of many poses in one pass
+    // pose_cps: one spline per pose (n × 2·g·g, the engine's lattice; the inverse direction
+    // negated on the other image) instead of the engine's live one
     bool eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::vector<PoseEval>& out,
-                    bool forward_only = false);
+                    bool forward_only = false, const float* pose_cps = nullptr);
     bool moments(const Mat3& H, double* out45);
     bool score3(const Mat3& H, double* out3);
     // scores of n ≤ 64 poses with every device buffer in a file-scope array (score_static.cu)
     bool score_static(const double* Hs, int n, double* out3);
     bool gradient(const Mat3& H, bool hess, zc_grad_result* out);
     bool climb(zc_climb_result* out);
+
+    // the B-spline on top of the pose (engine_ffd.cpp; src/pair.zig:17-37 Ffd): g = ffd_grid
+    // clamped to 2..16 (a new g zeroes the control points), 2·g·g control points in half-image
+    // units of the lattice's image (the fixed one, or the moving one with ffd_source)
+    unsigned ffd_grid();
+    bool ffd_live();
+    bool set_ffd(const float* cps, size_t n);
+    size_t get_ffd(float* cps, size_t cap);
+    // score and ∇ over the control points at H (src/pair.zig:387-410 ffdGrad)
+    bool ffd_gradient(const Mat3& H, double* score, double* grad, size_t len);
+    // the composed warp at the engine's pose (and spline, when on) over the fixed image: per
+    // 0-based fixed pixel x_moving − x_fixed (src/export.zig:64-106), rw × rh × 2 floats
+    bool displacement(float* out, size_t len);
+    // the forward and inverse directions' device splines for the pose passes (none unless live)
+    bool ffd_dirs(PoseFfd& fwd, PoseFfd& inv);
+    // per-pose splines for n poses (n × 2·g·g floats) as the two directions' device packs
+    bool ffd_pose_dirs(const float* cps, int n, PoseFfd& fwd, PoseFfd& inv);
+    // the climb's spline stage (src/gclimb.zig:206-246 splineStage): both directions' per-cell
+    // Gauss–Newton terms at H, the banded step under the bending energy, the candidates along it
+    // picked by score less bending penalty; lam: the penalty weight, set at the climb's first
+    // spline step (< 0 until then)
+    bool spline_stage(const Mat3& H, double& lam, bool& moved, double& score);
     void log_event(const std::string& text);
 
     // the rotation × scale sweep (engine_sweep.cpp): every candidate's map reduced to n_peak
@@ -246,6 +270,9 @@ class Engine {
     DevBuf stack_res_;
     DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;
     std::vector<float> pose_host_;
+    std::vector<float> ffd_cps_ = std::vector<float>(2 * 16 * 16, 0.f);
+    unsigned ffd_g_ = 4;
+    DevBuf ffd_dev_, ffd_out_, ffd_pk_, ffd_cells_, ffd_coef_;
     std::map<int, float2*> tw_;
 };
 

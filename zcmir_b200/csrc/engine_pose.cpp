@@ -49,7 +49,7 @@ std::string json_str(const std::string& t) {
 void Engine::log_event(const std::string& text) { events.push_back("{\"kind\":\"log\",\"text\":" + json_str(text) + "}"); }
 
 bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::vector<PoseEval>& out,
-                        bool forward_only) {
+                        bool forward_only, const float* pose_cps) {
     if (!need_images()) return false;
     if (!metric_ok("score")) return false;
     const bool sym = set.b("symmetric") && !forward_only, homog = set.e("group") == "homography", exact = set.b("exact");
@@ -88,15 +88,18 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
     double* sums = pose_sums_.as<double>();
     double* tsum = pose_tsum_.as<double>();
     float* coef = pose_coef_.as<float>();
-    if (!cuda_ok(pose_moments(pa, pb, dh, n, sums, st), "moments")) return false;
-    if (sym && !cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st), "moments"))
+    // a live spline moves the samples of both directions (src/pair.zig:127-150)
+    PoseFfd ff, fi;
+    if (!(pose_cps ? ffd_pose_dirs(pose_cps, n, ff, fi) : ffd_dirs(ff, fi))) return false;
+    if (!cuda_ok(pose_moments(pa, pb, dh, n, sums, st, ff), "moments")) return false;
+    if (sym && !cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, fi), "moments"))
         return false;
     if (!cuda_ok(pose_coefs(sums, (int)m, exact, coef, pose_score_.as<double>(), st), "score")) return false;
     counts[0] += nd + 1;
     if (grad) {
-        if (!cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, hess, tsum, st), "gradient")) return false;
+        if (!cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, hess, tsum, st, ff), "gradient")) return false;
         if (sym && !cuda_ok(pose_tangent(pb, pa, dh + (size_t)n * 9, coef + (size_t)n * kCoef, dg + 72, n, hess,
-                                         tsum + (size_t)n * kGrad, st),
+                                         tsum + (size_t)n * kGrad, st, fi),
                             "gradient"))
             return false;
         counts[0] += nd;
@@ -218,11 +221,11 @@ bool Engine::gradient(const Mat3& Hm, bool hess, zc_grad_result* out) {
 bool Engine::climb(zc_climb_result* out) {
     if (!need_images()) return false;
     const bool sym = set.b("symmetric"), homog = set.e("group") == "homography", hop = set.b("hop");
-    const bool hop_fm = set.b("hop_fm"), hops = hop || hop_fm;
+    const bool hop_fm = set.b("hop_fm"), hops = hop || hop_fm, spline = set.b("ffd");
+    double lam = -1;  // the spline's bending weight, set at its first step
     const unsigned n_iters = std::max(1u, set.u("g_iters"));
     const int nk = n_keys(homog);
     const double rw = side[1].w, rh = side[1].h;
-    if (set.b("ffd")) log_event("the spline stage is not part of this build; refining the homography only");
     // a candidate beats the current score when higher by more than 1e-6 of it (pair.zig beats)
     auto beats = [](double nw, double old) { return nw > old + std::max(1e-6 * std::fabs(old), 1e-12); };
     std::vector<PoseEval> ev;
@@ -231,8 +234,9 @@ bool Engine::climb(zc_climb_result* out) {
     PoseEval cur = ev[0];
     const double s_start = cur.mean;
     char buf[256];
-    snprintf(buf, sizeof buf, "ascent %s score %.4f %s%s%sGauss–Newton (B200)", homog ? "homography" : "affine",
-             s_start, sym ? "mean " : "", hop ? "shift hop+" : "", hop_fm ? "roto-scale hop+" : "");
+    snprintf(buf, sizeof buf, "ascent %s score %.4f %s%s%sGauss–Newton%s (B200)", homog ? "homography" : "affine",
+             s_start, sym ? "mean " : "", hop ? "shift hop+" : "", hop_fm ? "roto-scale hop+" : "",
+             spline ? "+spline" : "");
     log_event(buf);
     cancel = false;
     unsigned iter = 0, stall = 0, n_rec = 0;
@@ -335,11 +339,41 @@ bool Engine::climb(zc_climb_result* out) {
             }
             if (!gn_block()) return false;
         }
+        if (spline) {
+            // the spline stage (src/gclimb.zig:206-246): a Gauss–Newton step of the control
+            // points under the bending penalty; a win moves the spline, then the current pose's
+            // gradient is taken again with it
+            bool moved = false;
+            double sc_now = 0;
+            if (!spline_stage(H, lam, moved, sc_now)) return false;
+            if (moved) {
+                std::vector<PoseEval> g;
+                if (!eval_poses({H}, true, true, g)) return false;
+                cur = g[0];
+                ++n_rec;
+                std::string cj = "[";
+                const unsigned gg = ffd_grid();
+                for (size_t i = 0; i < 2 * (size_t)gg * gg; ++i) cj += (i ? "," : "") + json_num(ffd_cps_[i]);
+                events.push_back("{\"kind\":\"trail\",\"label\":\"spline\",\"score\":" + json_num(cur.mean) +
+                                 ",\"fwd\":" + json_num(cur.fwd) + ",\"inv\":" + (sym ? json_num(cur.inv) : "null") +
+                                 ",\"H\":" + fmt_mat(H) + ",\"cps\":" + cj + "]}");
+            } else {
+                cur.mean = sc_now;
+            }
+            moved_any |= moved;
+        }
         // iter_end: a move resets the stall count; with the shift hop on, two iterations in a
         // row without a move end the climb (one without it), as does the iteration budget
         stall = moved_any ? 0 : stall + 1;
         ++iter;
-        events.push_back("{\"kind\":\"pose\",\"H\":" + fmt_mat(H) + ",\"cps\":null}");
+        std::string pj = "null";
+        if (spline) {
+            pj = "[";
+            const unsigned gg = ffd_grid();
+            for (size_t i = 0; i < 2 * (size_t)gg * gg; ++i) pj += (i ? "," : "") + json_num(ffd_cps_[i]);
+            pj += "]";
+        }
+        events.push_back("{\"kind\":\"pose\",\"H\":" + fmt_mat(H) + ",\"cps\":" + pj + "}");
         snprintf(buf, sizeof buf, "ascent %u/%u score %.4f  stall %u  (%u steps so far)", iter, n_iters, cur.mean, stall,
                  n_rec);
         log_event(buf);

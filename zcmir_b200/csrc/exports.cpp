@@ -285,19 +285,13 @@ int32_t zc_keypoints(zc_engine* e, uint32_t, float*, size_t) { return unsupporte
 int32_t zc_keypoint_frames(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "keypoint_frames"); }
 int32_t zc_matches(zc_engine* e, uint32_t*, size_t) { return unsupported(e, "matches"); }
 
-int32_t zc_set_ffd(zc_engine* e, const float*, size_t n) {
-    // the spline stays off in this build; all-zero control points are accepted
-    (void)n;
-    if (e) e->err.clear();
-    return 0;
+int32_t zc_set_ffd(zc_engine* e, const float* cps, size_t n) {
+    return guarded(e, "set_ffd", [&] { return e->set_ffd(cps, n); });
 }
 
 size_t zc_get_ffd(zc_engine* e, float* cps, size_t cap) {
     if (!e) return 0;
-    const unsigned g = std::min(std::max(e->set.u("ffd_grid"), 2u), 16u);
-    const size_t n = 2 * (size_t)g * g;
-    for (size_t i = 0; i < std::min(n, cap); ++i) cps[i] = 0.f;
-    return n;
+    return e->get_ffd(cps, cap);
 }
 
 uint32_t zc_fit_check(zc_engine* e, const double*) {
@@ -305,8 +299,8 @@ uint32_t zc_fit_check(zc_engine* e, const double*) {
     return 7;  // "it fails the sanity check" (python/zcmir/__init__.py:178-181)
 }
 
-int32_t zc_ffd_gradient(zc_engine* e, const double*, double*, double*, size_t) {
-    return unsupported(e, "ffd_gradient");
+int32_t zc_ffd_gradient(zc_engine* e, const double* H, double* score, double* grad, size_t len) {
+    return guarded(e, "ffd_gradient", [&] { return e->ffd_gradient(mat(H), score, grad, len); });
 }
 
 int32_t zc_canvas(zc_engine* e, const double H[9], uint32_t inverse, zc_canvas_info* out) {
@@ -334,7 +328,9 @@ int32_t zc_tile_heat(zc_engine* e, const double*, uint32_t, uint32_t, double*, f
     return unsupported(e, "tile_heat");
 }
 int64_t zc_export_warp(zc_engine* e, const char*, size_t, void*, size_t) { return unsupported(e, "export_warp"); }
-int32_t zc_displacement(zc_engine* e, float*, size_t) { return unsupported(e, "displacement"); }
+int32_t zc_displacement(zc_engine* e, float* out, size_t len) {
+    return guarded(e, "displacement", [&] { return e->displacement(out, len); });
+}
 
 void zc_result_sizes(uint32_t out[4]) {
     out[0] = sizeof(zc_shift_result);

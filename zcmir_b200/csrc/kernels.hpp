@@ -152,14 +152,34 @@ struct PoseSide {
     const float* feat;  // 4 whitened planes, plane-major
     int w, h;
 };
+// A cubic B-spline on top of the pose: g × g control points (x, y per point, in half-image units
+// of the lattice's image), on b (the destination: it moves b's pixel before H⁻¹) or, source, on a
+// (it moves the sample after H⁻¹). cps null: no spline.
+struct PoseFfd {
+    const float* cps = nullptr;
+    int g = 0;
+    int source = 0;
+    int stride = 0;  // floats between poses' control points (0: one set for every pose)
+};
 // the 45 sums of n poses of one direction (a sampled at H⁻¹x for every b pixel x); hinv: n
 // inverse poses (f32, row-major); sums: n × 45 float64 (zeroed here)
-cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st);
+cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
+                         const PoseFfd& ffd = {});
 // score (float64) and the 102 gradient coefficients (f32) of each pose's sums
 cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, double* score, cudaStream_t st);
 // tangent sums per pose: 8 gradient + 36 Gauss–Newton (upper triangle) float64 (zeroed here);
 // gens: 8 generators (9 f32 each) in b's pixel coordinates
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
-                         int n, bool hess, double* out, cudaStream_t st);
+                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd = {});
+// ∂score/∂(control points cp0 .. cp0 + 15) of pose 0 of one direction from its coefficients:
+// out[32] float64 (x then y per point; zeroed here)
+cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef,
+                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st);
+// the spline's Gauss–Newton terms per lattice cell of pose 0 of one direction (its coefficients
+// with a positive semi-definite Q): per cell and chunk 332 float32 sums (100 symmetric basis
+// pairs × K_xx, K_xy, K_yy, then 16 taps × ∇_x, ∇_y); nch chunks per cell
+constexpr int kFfdCell = 332;
+cudaError_t pose_ffd_cells(const PoseSide& a, const PoseSide& b, const float* hinv, const float* hpose,
+                           const float* coef, const PoseFfd& ffd, int nch, float* out, cudaStream_t st);
 
 }  // namespace zc

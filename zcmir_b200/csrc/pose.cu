@@ -42,31 +42,98 @@ __device__ __forceinline__ void taper(float fx, float fy, float w, float h, floa
     ty = vx * dy;
 }
 
-struct Hinv {
-    float m[9];
+// ── the B-spline (smi.wgsl:198-240 cubic_w, dest_half, ffd_disp) ──
+
+constexpr int kFfdMax = 16;  // lattice side (src/pose.zig:17 FFD_MAX)
+
+__device__ __forceinline__ float4 cubic_w(float t) {
+    const float t2 = t * t, t3 = t2 * t;
+    return make_float4((1.f - t) * (1.f - t) * (1.f - t) / 6.f, (3.f * t3 - 6.f * t2 + 4.f) / 6.f,
+                       (-3.f * t3 + 3.f * t2 + 3.f * t + 1.f) / 6.f, t3 / 6.f);
+}
+__device__ __forceinline__ float comp4(const float4& v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+
+// A block's view of a spline: its control points staged in shared memory (c null: none).
+struct FfdView {
+    const float* c;
+    int g, source;
 };
 
-// pose sample position of b pixel (x, y): false when outside a's valid interior
-__device__ __forceinline__ bool sample_pos(const float* Hi, int x, int y, int aw, int ah, float& fx, float& fy, float3& ph) {
-    const float X = (float)x + 1.f, Y = (float)y + 1.f;
-    ph.x = Hi[0] * X + Hi[1] * Y + Hi[2];
-    ph.y = Hi[3] * X + Hi[4] * Y + Hi[5];
-    ph.z = Hi[6] * X + Hi[7] * Y + Hi[8];
+// stage pose `pose`'s control points (all threads call it; a __syncthreads must follow)
+__device__ __forceinline__ FfdView ffd_view(const PoseFfd& f, float* sh, int pose = 0) {
+    if (!f.cps || f.g < 2) return FfdView{nullptr, 0, 0};
+    const float* c = f.cps + (size_t)pose * f.stride;
+    for (int i = threadIdx.x; i < 2 * f.g * f.g; i += blockDim.x) sh[i] = c[i];
+    return FfdView{sh, f.g, f.source};
+}
+
+// the displacement (pixels) at the 0-based point (xf, yf) of the lattice's rw × rh image: 0
+// outside it; half-image units scaled by (rw/2, rh/2); clamped lattice indices
+__device__ __forceinline__ float2 ffd_disp(const FfdView& f, float xf, float yf, float rw, float rh) {
+    if (xf < 0.f || yf < 0.f || xf > rw - 1.f || yf > rh - 1.f) return make_float2(0.f, 0.f);
+    const int g = f.g;
+    const float hx = fmaxf(rw, 1.f) * 0.5f, hy = fmaxf(rh, 1.f) * 0.5f;
+    const float spx = fmaxf(rw - 1.f, 1.f) / (float)(g - 1), spy = fmaxf(rh - 1.f, 1.f) / (float)(g - 1);
+    const float su = xf / spx, sv = yf / spy;
+    const int iu = (int)floorf(su), iv = (int)floorf(sv);
+    const float4 bu = cubic_w(fminf(fmaxf(su - (float)iu, 0.f), 1.f));
+    const float4 bv = cubic_w(fminf(fmaxf(sv - (float)iv, 0.f), 1.f));
+    float dx = 0.f, dy = 0.f;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+        const int j = min(max(iv - 1 + jj, 0), g - 1);
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+            const int i = min(max(iu - 1 + ii, 0), g - 1);
+            const float w = comp4(bu, ii) * comp4(bv, jj);
+            const int o = (j * g + i) * 2;
+            dx = dx + w * (f.c[o] * hx);
+            dy = dy + w * (f.c[o + 1] * hy);
+        }
+    }
+    return make_float2(dx, dy);
+}
+
+// pose sample position of b pixel (x, y) (smi.wgsl overlap_moments 1003-1016): with a spline on
+// b the pixel moves first, X = (x + 1 + dx, y + 1 + dy); on a the sample H⁻¹X − 1 moves after.
+// ph = H⁻¹X, (Xx, Xy) = X. False when outside a's valid interior.
+template <bool FFD>
+__device__ __forceinline__ bool sample_pos(const float* Hi, const FfdView& f, int x, int y, int aw, int ah, int bw,
+                                           int bh, float& fx, float& fy, float3& ph, float& Xx, float& Xy) {
+    Xx = (float)x + 1.f;
+    Xy = (float)y + 1.f;
+    if (FFD && !f.source) {
+        const float2 d = ffd_disp(f, (float)x, (float)y, (float)bw, (float)bh);
+        Xx = (float)x + 1.f + d.x;
+        Xy = (float)y + 1.f + d.y;
+    }
+    ph.x = Hi[0] * Xx + Hi[1] * Xy + Hi[2];
+    ph.y = Hi[3] * Xx + Hi[4] * Xy + Hi[5];
+    ph.z = Hi[6] * Xx + Hi[7] * Xy + Hi[8];
     if (fabsf(ph.z) < 1e-8f) return false;
     fx = ph.x / ph.z - 1.f;
     fy = ph.y / ph.z - 1.f;
+    if (FFD && f.source) {
+        const float2 d = ffd_disp(f, fx, fy, (float)aw, (float)ah);
+        fx = fx + d.x;
+        fy = fy + d.y;
+    }
     return !(fx < 2.f || fy < 2.f || fx > (float)aw - 3.f || fy > (float)ah - 3.f);
 }
 
 // The 45 sums: 0 Σw, 1–4 Σw a, 5–8 Σw b, 9–24 Σw a_i b_j, 25–34 / 35–44 upper triangles of
 // Σw a aᵀ and Σw b bᵀ.
+template <bool FFD>
 __global__ void __launch_bounds__(256) k_pose_moments(const float* __restrict__ fa, int aw, int ah,
                                                       const float* __restrict__ fb, int bw, int bh,
-                                                      const float* __restrict__ hinv, double* __restrict__ sums) {
+                                                      const float* __restrict__ hinv, double* __restrict__ sums,
+                                                      PoseFfd ffd) {
     __shared__ float Hs[9];
     __shared__ float red[8][kMom];
+    __shared__ float cps[2 * kFfdMax * kFfdMax];
     const int pose = blockIdx.y;
     if (threadIdx.x < 9) Hs[threadIdx.x] = hinv[pose * 9 + threadIdx.x];
+    const FfdView fv = ffd_view(ffd, cps, pose);
     __syncthreads();
     float Hi[9];
 #pragma unroll
@@ -77,9 +144,9 @@ __global__ void __launch_bounds__(256) k_pose_moments(const float* __restrict__ 
     const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
         const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
-        float fx, fy;
+        float fx, fy, Xx, Xy;
         float3 ph;
-        if (!sample_pos(Hi, x, y, aw, ah, fx, fy, ph)) continue;
+        if (!sample_pos<FFD>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, Xx, Xy)) continue;
         float wt, d1, d2;
         taper(fx, fy, (float)aw, (float)ah, wt, d1, d2);
         if (wt <= 0.f) continue;
@@ -273,15 +340,19 @@ __global__ void k_pose_coefs(const double* __restrict__ sums, int n, int exact, 
 // per pose 44 sums (8 gradient, then the 8×8 upper triangle row by row). Per pixel the gradient
 // needs the two scalars cx, cy = (∂S/∂v_a)·∇v_a plus the taper's boundary term, times each
 // tangent's flow ∂(sample)/∂ξ_k = ((M_k X)·ph.z − ph·(M_k X).z)/ph.z², M_k = −H⁻¹ G_k.
+template <bool FFD>
 __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ fa, int aw, int ah,
                                                       const float* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, const float* __restrict__ coef,
-                                                      const float* __restrict__ gens, int hess, double* __restrict__ out) {
+                                                      const float* __restrict__ gens, int hess, double* __restrict__ out,
+                                                      PoseFfd ffd) {
     __shared__ float Hs[9], Mk[8][9], cf[kCoef];
     __shared__ float red[8][kGrad];
+    __shared__ float cps[2 * kFfdMax * kFfdMax];
     const int pose = blockIdx.y;
     if (threadIdx.x < 9) Hs[threadIdx.x] = hinv[pose * 9 + threadIdx.x];
     for (int k = threadIdx.x; k < kCoef; k += blockDim.x) cf[k] = coef[pose * kCoef + k];
+    const FfdView fv = ffd_view(ffd, cps, pose);
     __syncthreads();
     if (threadIdx.x < 72) {
         const int k = threadIdx.x / 9, e = threadIdx.x % 9, r = e / 3, c = e % 3;
@@ -299,9 +370,9 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
     const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
         const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
-        float fx, fy;
+        float fx, fy, X, Y;
         float3 ph;
-        if (!sample_pos(Hi, x, y, aw, ah, fx, fy, ph)) continue;
+        if (!sample_pos<FFD>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, X, Y)) continue;
         float wt, tpx, tpy;
         taper(fx, fy, (float)aw, (float)ah, wt, tpx, tpy);
         const float flx = floorf(fx), fly = floorf(fy);
@@ -350,7 +421,6 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
         }
         const float cx = wt * dga + bwv * tpx, cy = wt * dgb + bwv * tpy;
         const float iz2 = 1.f / fmaxf(ph.z * ph.z, 1e-12f);
-        const float X = (float)x + 1.f, Y = (float)y + 1.f;
         float px[8], py[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -412,6 +482,350 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
     }
 }
 
+// ∂score/∂(control points cp0 .. cp0 + 15) of pose 0 (smi.wgsl ffd_grad 1275-1417): per valid
+// pixel the two scalars Gx, Gy — (∂S/∂v_a)·∇v_a and the taper's boundary term along the sample's
+// motion under a unit x or y displacement of one control point (through H⁻¹ on a b lattice,
+// directly on an a lattice), per unit basis weight — then each control point of the chunk takes
+// its basis weight B_i(u) B_j(v) (clamped lattice indices summed) times them.
+__global__ void __launch_bounds__(256) k_pose_ffd_grad(const float* __restrict__ fa, int aw, int ah,
+                                                       const float* __restrict__ fb, int bw, int bh,
+                                                       const float* __restrict__ hinv, const float* __restrict__ coef,
+                                                       PoseFfd ffd, int cp0, double* __restrict__ out) {
+    __shared__ float Hs[9], cf[kCoef];
+    __shared__ float red[8][32];
+    __shared__ float cps[2 * kFfdMax * kFfdMax];
+    if (threadIdx.x < 9) Hs[threadIdx.x] = hinv[threadIdx.x];
+    for (int k = threadIdx.x; k < kCoef; k += blockDim.x) cf[k] = coef[k];
+    const FfdView fv = ffd_view(ffd, cps);
+    __syncthreads();
+    float Hi[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Hi[i] = Hs[i];
+    const int g = fv.g;
+    const bool src = fv.source != 0;
+    const float lw = src ? (float)aw : (float)bw, lh = src ? (float)ah : (float)bh;
+    const float hx = fmaxf(lw, 1.f) * 0.5f, hy = fmaxf(lh, 1.f) * 0.5f;
+    const float spx = fmaxf(lw - 1.f, 1.f) / (float)(g - 1), spy = fmaxf(lh - 1.f, 1.f) / (float)(g - 1);
+    float acc[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) acc[k] = 0.f;
+    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
+        float fx, fy, X, Y;
+        float3 ph;
+        if (!sample_pos<true>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, X, Y)) continue;
+        float wt, tpx, tpy;
+        taper(fx, fy, (float)aw, (float)ah, wt, tpx, tpy);
+        const float flx = floorf(fx), fly = floorf(fy);
+        const float ax = fx - flx, ay = fy - fly;
+        const size_t i00 = (size_t)fly * aw + (size_t)flx;
+        float va[4], gx[4], gy[4], vb[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const float* P = fa + p * na;
+            const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
+            const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+            va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
+            gx[p] = (v10 - v00) * (1.f - ay) + (v11 - v01) * ay;
+            gy[p] = (v01 - v00) * (1.f - ax) + (v11 - v10) * ax;
+            vb[p] = __ldg(&fb[p * nb + t]);
+        }
+        float dga = 0.f, dgb = 0.f;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            float s = 0.f;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) s += cf[a * 4 + b] * (vb[b] - cf[16 + b]) - cf[20 + a * 4 + b] * (va[b] - cf[36 + b]);
+            dga += 2.f * s * gx[a];
+            dgb += 2.f * s * gy[a];
+        }
+        float bwv = 0.f;
+        if (tpx != 0.f || tpy != 0.f) {
+            const float* gg = cf + kG0;
+            float s = gg[0];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                s += gg[1 + i] * va[i] + gg[5 + i] * vb[i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) s += gg[9 + i * 4 + j] * va[i] * vb[j];
+#pragma unroll
+                for (int j = i; j < 4; ++j) s += gg[25 + tri4(i, j)] * va[i] * va[j] + gg[35 + tri4(i, j)] * vb[i] * vb[j];
+            }
+            bwv = s;
+        }
+        // the sample's motion per unit basis weight of a control point's x / y displacement
+        float uxx, uxy, uyx, uyy;
+        float su, sv;
+        if (src) {
+            uxx = hx, uxy = 0.f, uyx = 0.f, uyy = hy;
+            su = (ph.x / ph.z - 1.f) / spx;
+            sv = (ph.y / ph.z - 1.f) / spy;
+        } else {
+            const float z = ph.z, z2 = fmaxf(z * z, 1e-12f);
+            uxx = hx * (Hi[0] * z - ph.x * Hi[6]) / z2;
+            uxy = hx * (Hi[3] * z - ph.y * Hi[6]) / z2;
+            uyx = hy * (Hi[1] * z - ph.x * Hi[7]) / z2;
+            uyy = hy * (Hi[4] * z - ph.y * Hi[7]) / z2;
+            su = (float)x / spx;
+            sv = (float)y / spy;
+        }
+        const float Gx = wt * (dga * uxx + dgb * uxy) + bwv * (tpx * uxx + tpy * uxy);
+        const float Gy = wt * (dga * uyx + dgb * uyy) + bwv * (tpx * uyx + tpy * uyy);
+        if (!(Gx == Gx) || !(Gy == Gy)) continue;
+        const int iu = (int)floorf(su), iv = (int)floorf(sv);
+        const float4 bu = cubic_w(fminf(fmaxf(su - (float)iu, 0.f), 1.f));
+        const float4 bv = cubic_w(fminf(fmaxf(sv - (float)iv, 0.f), 1.f));
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int cp = cp0 + k;
+            if (cp >= g * g) break;
+            const int ci = cp % g, cj = cp / g;
+            float wu = 0.f, wv = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (min(max(iu - 1 + q, 0), g - 1) == ci) wu += comp4(bu, q);
+                if (min(max(iv - 1 + q, 0), g - 1) == cj) wv += comp4(bv, q);
+            }
+            const float bk = wu * wv;
+            acc[2 * k] += bk * Gx;
+            acc[2 * k + 1] += bk * Gy;
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        const float v = warp_sumf(acc[k]);
+        if (lane == 0) red[w][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += (double)red[i][threadIdx.x];
+        atomicAdd(&out[threadIdx.x], s);
+    }
+}
+
+// The spline's Gauss–Newton terms of one lattice cell (smi.wgsl ffd_cells 2065-2264): block =
+// (cell, chunk of its pixel tiles). The cell's fixed pixels (the cell itself on a fixed-image
+// lattice; the bounding box of the moving cell's corners under H, one pixel wider, on a
+// moving-image lattice) in tiles of 256: each thread stages one pixel that samples inside the
+// moving image and whose lattice point lies in this cell — its basis weights, K = wt·Jdᵀ S Jd
+// (S = ∇vᵀ Q ∇v, Jd the sample's motion per unit control-point displacement) and the
+// gradient Jdᵀ (wt ∇S + the taper term) — then thread (task, half) adds its share of the tile:
+// tasks 0–99 a pair of symmetric basis products × (K_xx, K_xy, K_yy), 100–115 a tap × ∇.
+constexpr int kFcTasks = 116;
+__device__ __forceinline__ int tri_i(int k) { return k < 4 ? 0 : k < 7 ? 1 : k < 9 ? 2 : 3; }
+__device__ __forceinline__ int tri_j(int k) { return k < 4 ? k : k < 7 ? k - 3 : k < 9 ? k - 5 : 3; }
+
+__global__ void __launch_bounds__(256) k_pose_ffd_cells(const float* __restrict__ fa, int aw, int ah,
+                                                        const float* __restrict__ fb, int bw, int bh,
+                                                        const float* __restrict__ hinv, const float* __restrict__ hpose,
+                                                        const float* __restrict__ coef, PoseFfd ffd, int nch,
+                                                        float* __restrict__ out) {
+    __shared__ float Hs[9], Hp[9], cf[kCoef];
+    __shared__ float cps[2 * kFfdMax * kFfdMax];
+    __shared__ float4 s_bu[256], s_bv[256], s_k[256];
+    __shared__ float s_gy[256];
+    __shared__ float3 s_acc[256];
+    if (threadIdx.x < 9) {
+        Hs[threadIdx.x] = hinv[threadIdx.x];
+        Hp[threadIdx.x] = hpose[threadIdx.x];
+    }
+    for (int k = threadIdx.x; k < kCoef; k += blockDim.x) cf[k] = coef[k];
+    const FfdView fv = ffd_view(ffd, cps);
+    __syncthreads();
+    float Hi[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Hi[i] = Hs[i];
+    const int g = fv.g;
+    const int cell = blockIdx.x / nch, chunk = blockIdx.x % nch;
+    const int iu = cell % g, iv = cell / g;
+    const bool src = fv.source != 0;
+    const float rw = (float)bw, rh = (float)bh, sw = (float)aw, shh = (float)ah;
+    const float lw = src ? sw : rw, lh = src ? shh : rh;
+    const float hx = fmaxf(lw, 1.f) * 0.5f, hy = fmaxf(lh, 1.f) * 0.5f;
+    const float spx = fmaxf(lw - 1.f, 1.f) / (float)(g - 1), spy = fmaxf(lh - 1.f, 1.f) / (float)(g - 1);
+    float x0 = 0.f, x1 = rw - 1.f, y0 = 0.f, y1 = rh - 1.f;
+    if (!src) {
+        x0 = fmaxf(0.f, floorf((float)iu * spx) - 1.f);
+        x1 = fminf(rw - 1.f, ceilf((float)(iu + 1) * spx) + 1.f);
+        y0 = fmaxf(0.f, floorf((float)iv * spy) - 1.f);
+        y1 = fminf(rh - 1.f, ceilf((float)(iv + 1) * spy) + 1.f);
+    } else {
+        float bx0 = 3.0e38f, bx1 = -3.0e38f, by0 = 3.0e38f, by1 = -3.0e38f;
+        for (int c = 0; c < 4; ++c) {
+            const float mx = (float)(iu + (c & 1)) * spx + 1.f, my = (float)(iv + (c >> 1)) * spy + 1.f;
+            const float qx = Hp[0] * mx + Hp[1] * my + Hp[2], qy = Hp[3] * mx + Hp[4] * my + Hp[5];
+            const float qz = Hp[6] * mx + Hp[7] * my + Hp[8];
+            if (fabsf(qz) < 1e-8f) continue;
+            bx0 = fminf(bx0, qx / qz - 1.f);
+            bx1 = fmaxf(bx1, qx / qz - 1.f);
+            by0 = fminf(by0, qy / qz - 1.f);
+            by1 = fmaxf(by1, qy / qz - 1.f);
+        }
+        x0 = fmaxf(0.f, floorf(bx0) - 1.f);
+        x1 = fminf(rw - 1.f, ceilf(bx1) + 1.f);
+        y0 = fmaxf(0.f, floorf(by0) - 1.f);
+        y1 = fminf(rh - 1.f, ceilf(by1) + 1.f);
+    }
+    const int bwx = (int)fmaxf(x1 - x0 + 1.f, 0.f), bhy = (int)fmaxf(y1 - y0 + 1.f, 0.f);
+    const int total = bwx * bhy;
+    const int half = threadIdx.x / kFcTasks, task = threadIdx.x % kFcTasks;
+    int bi = 0, bi2 = 0, bj = 0, bj2 = 0;
+    if (task < 100) {
+        bi = tri_i(task / 10), bi2 = tri_j(task / 10), bj = tri_i(task % 10), bj2 = tri_j(task % 10);
+    } else {
+        bi = (task - 100) % 4, bj = (task - 100) / 4;
+    }
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
+    const int ntile = (total + 255) / 256;
+    for (int tile = chunk * ntile / nch; tile < (chunk + 1) * ntile / nch; ++tile) {
+        const int base = tile * 256, pidx = base + threadIdx.x;
+        bool ok = false;
+        float4 bu = make_float4(0.f, 0.f, 0.f, 0.f), bv = bu, kk = bu;
+        float gyv = 0.f;
+        if (pidx < total) {
+            const int xi = (int)x0 + pidx % bwx, yi = (int)y0 + pidx / bwx;
+            float fx, fy, X, Y, su, sv;
+            float3 ph;
+            ok = sample_pos<true>(Hi, fv, xi, yi, aw, ah, bw, bh, fx, fy, ph, X, Y);
+            if (fabsf(ph.z) >= 1e-8f) {
+                if (src) {
+                    su = (ph.x / ph.z - 1.f) / spx;
+                    sv = (ph.y / ph.z - 1.f) / spy;
+                } else {
+                    su = (float)xi / spx;
+                    sv = (float)yi / spy;
+                }
+                // this cell's pixels only (each pixel belongs to exactly one cell)
+                if ((int)floorf(su) != iu || (int)floorf(sv) != iv) ok = false;
+                if (su < 0.f || sv < 0.f || su > (float)(g - 1) || sv > (float)(g - 1)) ok = false;
+            } else {
+                ok = false;
+                su = sv = 0.f;
+            }
+            if (ok) {
+                const size_t t = (size_t)yi * bw + xi;
+                float wt, tpx, tpy;
+                taper(fx, fy, sw, shh, wt, tpx, tpy);
+                const float flx = floorf(fx), fly = floorf(fy);
+                const float ax = fx - flx, ay = fy - fly;
+                const size_t i00 = (size_t)fly * aw + (size_t)flx;
+                float va[4], gx[4], gy[4], vb[4];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const float* P = fa + p * na;
+                    const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
+                    const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+                    va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
+                    gx[p] = (v10 - v00) * (1.f - ay) + (v11 - v01) * ay;
+                    gy[p] = (v01 - v00) * (1.f - ax) + (v11 - v10) * ax;
+                    vb[p] = __ldg(&fb[p * nb + t]);
+                }
+                float rx = 0.f, ry = 0.f;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    float s = 0.f;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) s += cf[a * 4 + b] * (vb[b] - cf[16 + b]) - cf[20 + a * 4 + b] * (va[b] - cf[36 + b]);
+                    rx += 2.f * s * gx[a];
+                    ry += 2.f * s * gy[a];
+                }
+                float bwb = 0.f;
+                if (tpx != 0.f || tpy != 0.f) {
+                    const float* gg = cf + kG0;
+                    float s = gg[0];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        s += gg[1 + i] * va[i] + gg[5 + i] * vb[i];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) s += gg[9 + i * 4 + j] * va[i] * vb[j];
+#pragma unroll
+                        for (int j = i; j < 4; ++j) s += gg[25 + tri4(i, j)] * va[i] * va[j] + gg[35 + tri4(i, j)] * vb[i] * vb[j];
+                    }
+                    bwb = s;
+                }
+                float j00, j10, j01, j11;
+                if (src) {
+                    j00 = hx, j10 = 0.f, j01 = 0.f, j11 = hy;
+                } else {
+                    const float z = ph.z, z2 = fmaxf(z * z, 1e-12f);
+                    j00 = hx * (Hi[0] * z - ph.x * Hi[6]) / z2;
+                    j10 = hx * (Hi[3] * z - ph.y * Hi[6]) / z2;
+                    j01 = hy * (Hi[1] * z - ph.x * Hi[7]) / z2;
+                    j11 = hy * (Hi[4] * z - ph.y * Hi[7]) / z2;
+                }
+                float sxx = 0.f, sxy = 0.f, syy = 0.f;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    float qx = 0.f, qy = 0.f;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        qx += cf[kQ0 + a * 4 + b] * gx[b];
+                        qy += cf[kQ0 + a * 4 + b] * gy[b];
+                    }
+                    sxx += gx[a] * qx;
+                    sxy += gx[a] * qy;
+                    syy += gy[a] * qy;
+                }
+                const float px = wt * rx + bwb * tpx, py = wt * ry + bwb * tpy;
+                const float gxv = j00 * px + j10 * py;
+                gyv = j01 * px + j11 * py;
+                const float a0 = sxx * j00 + sxy * j10, a1 = sxy * j00 + syy * j10;
+                const float b0 = sxx * j01 + sxy * j11, b1 = sxy * j01 + syy * j11;
+                kk = make_float4(wt * (j00 * a0 + j10 * a1), wt * (j00 * b0 + j10 * b1), wt * (j01 * b0 + j11 * b1), gxv);
+                bu = cubic_w(fminf(fmaxf(su - floorf(su), 0.f), 1.f));
+                bv = cubic_w(fminf(fmaxf(sv - floorf(sv), 0.f), 1.f));
+                if (!(fabsf(kk.x) + fabsf(kk.y) + fabsf(kk.z) + fabsf(kk.w) + fabsf(gyv) < 1e30f)) ok = false;
+            }
+        }
+        if (!ok) {
+            bu = bv = kk = make_float4(0.f, 0.f, 0.f, 0.f);
+            gyv = 0.f;
+        }
+        s_bu[threadIdx.x] = bu;
+        s_bv[threadIdx.x] = bv;
+        s_k[threadIdx.x] = kk;
+        s_gy[threadIdx.x] = gyv;
+        __syncthreads();
+        const int m = min(256, total - base);
+        if (half < 2) {
+            const int e1 = min(m, (half + 1) * 128);
+            if (task < 100) {
+                for (int e = half * 128; e < e1; ++e) {
+                    const float pr = comp4(s_bu[e], bi) * comp4(s_bu[e], bi2) * comp4(s_bv[e], bj) * comp4(s_bv[e], bj2);
+                    acc.x += pr * s_k[e].x;
+                    acc.y += pr * s_k[e].y;
+                    acc.z += pr * s_k[e].z;
+                }
+            } else {
+                for (int e = half * 128; e < e1; ++e) {
+                    const float b = comp4(s_bu[e], bi) * comp4(s_bv[e], bj);
+                    acc.x += s_k[e].w * b;
+                    acc.y += s_gy[e] * b;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    s_acc[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < kFcTasks) {
+        const float3 u = s_acc[threadIdx.x], v = s_acc[threadIdx.x + kFcTasks];
+        float* o = out + (size_t)blockIdx.x * kFfdCell;
+        if (threadIdx.x < 100) {
+            o[threadIdx.x * 3] = u.x + v.x;
+            o[threadIdx.x * 3 + 1] = u.y + v.y;
+            o[threadIdx.x * 3 + 2] = u.z + v.z;
+        } else {
+            o[300 + (threadIdx.x - 100) * 2] = u.x + v.x;
+            o[300 + (threadIdx.x - 100) * 2 + 1] = u.y + v.y;
+        }
+    }
+}
+
 int pose_blocks(size_t pixels, int n) {
     const size_t by_work = (pixels + 256 * 16 - 1) / (256 * 16);  // ≥ 16 pixels per thread
     const size_t by_fill = (1184 + (size_t)n - 1) / (size_t)n;
@@ -421,10 +835,32 @@ int pose_blocks(size_t pixels, int n) {
 
 }  // namespace
 
-cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st) {
+cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
+                         const PoseFfd& ffd) {
+    if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(sums, 0, (size_t)n * kMom * sizeof(double), st);
     dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
-    k_pose_moments<<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, sums);
+    if (ffd.cps)
+        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, sums, ffd);
+    else
+        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, sums, ffd);
+    return cudaGetLastError();
+}
+
+cudaError_t pose_ffd_cells(const PoseSide& a, const PoseSide& b, const float* hinv, const float* hpose,
+                           const float* coef, const PoseFfd& ffd, int nch, float* out, cudaStream_t st) {
+    if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax || nch < 1) return cudaErrorInvalidValue;
+    k_pose_ffd_cells<<<ffd.g * ffd.g * nch, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, hpose, coef, ffd,
+                                                          nch, out);
+    return cudaGetLastError();
+}
+
+cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef,
+                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st) {
+    if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax) return cudaErrorInvalidValue;
+    cudaMemsetAsync(out, 0, 32 * sizeof(double), st);
+    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, 1), 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef,
+                                                                       ffd, cp0, out);
     return cudaGetLastError();
 }
 
@@ -434,10 +870,14 @@ cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, doubl
 }
 
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
-                         int n, bool hess, double* out, cudaStream_t st) {
+                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd) {
+    if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, (size_t)n * kGrad * sizeof(double), st);
     dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
-    k_pose_tangent<<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out);
+    if (ffd.cps)
+        k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
+    else
+        k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
     return cudaGetLastError();
 }
 

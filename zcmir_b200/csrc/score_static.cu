@@ -86,6 +86,7 @@ bool Engine::score_static(const double* Hs, int n, double* out3) {
     if (!side[0].has || !side[1].has) return fail("NoImages");
     if (set.e("metric") != "smi")
         return fail("score_static: metric \"" + set.e("metric") + "\" is not part of this build's SMI path");
+    if (ffd_live()) return fail("score_static: the spline is live; its scores come from zc_score");
     const std::string& fm = set.e("smi_features");
     const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
     for (const Side& sd : side)
