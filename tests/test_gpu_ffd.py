@@ -178,3 +178,17 @@ def test_register_with_spline_recovers_a_smooth_warp():
     assert e1 < 0.8 * e0, (e0, e1)
     w = r1.warp(moving)
     assert w.shape == fixed.shape and w.dtype == moving.dtype
+
+
+def test_search_runs_without_the_spline_and_resets_it():
+    """The sweep search scores the current pose with the live spline, climbs its peaks without it
+    and, when it moves the pose, zeroes the control points (src/search.zig:703-705, 806-815)."""
+    m, f, _ = synth.pair_similarity(n=160, seed=5, deg=25.0, scale=1.05, shift=(4.0, -3.0))
+    with zc.Registrar(half=False, ffd=True, ffd_grid=4, sw_nth=72, sw_ns=3) as reg:
+        reg.set_images(m, f, preprocess=False)
+        reg.ffd = _cps(4, 2, 0.01)
+        r = reg.search()
+        logs = [e.get("text", "") for e in reg.events() if e["kind"] == "log"]
+        assert r.improved
+        assert not reg.ffd.any()
+        assert any("spline reset" in t for t in logs), logs

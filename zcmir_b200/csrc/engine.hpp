@@ -272,6 +272,7 @@ class Engine {
     std::vector<float> pose_host_;
     std::vector<float> ffd_cps_ = std::vector<float>(2 * 16 * 16, 0.f);
     unsigned ffd_g_ = 4;
+    bool ffd_suspended_ = false;  // the search's climbs run without the spline
     DevBuf ffd_dev_, ffd_out_, ffd_pk_, ffd_cells_, ffd_coef_;
     std::map<int, float2*> tw_;
 };

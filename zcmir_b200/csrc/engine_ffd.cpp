@@ -27,7 +27,7 @@ unsigned Engine::ffd_grid() {
 }
 
 bool Engine::ffd_live() {
-    if (!set.b("ffd")) return false;
+    if (!set.b("ffd") || ffd_suspended_) return false;
     const unsigned g = ffd_grid();
     for (size_t i = 0; i < 2 * (size_t)g * g; ++i)
         if (std::fabs(ffd_cps_[i]) > 1e-12) return true;

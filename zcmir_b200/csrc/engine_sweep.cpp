@@ -431,7 +431,6 @@ bool Engine::search_lanes(const float* scores, const uint32_t* idx, size_t n, zc
 
 bool Engine::search_finish(const SweepOut& res, const SweepGrid& gv, const Mat3& H0, zc_search_result* out) {
     cancel = false;
-    if (set.b("ffd")) log_event("the spline stage is not part of this build; searching the homography only");
     const int G = res.G;
     const unsigned kk = set.u("sw_k");
     const unsigned K = (kk == 8 || kk == 16 || kk == 32) ? kk : 32;
@@ -439,8 +438,15 @@ bool Engine::search_finish(const SweepOut& res, const SweepGrid& gv, const Mat3&
     const Mat3 Hcur = H;
     const double c_mov[2] = {(side[0].w + 1) / 2.0, (side[0].h + 1) / 2.0};
     std::vector<PoseEval> e0;
-    if (!eval_poses({Hcur}, false, false, e0)) return false;
+    if (!eval_poses({Hcur}, false, false, e0)) return false;  // with the live spline
     const double s_cur = e0[0].mean;
+    // the spline is off while the sweep's peaks climb (src/search.zig:703-705, 806-810)
+    const bool ffd_was = set.b("ffd");
+    struct Suspend {
+        bool& f;
+        explicit Suspend(bool& x) : f(x) { f = true; }
+        ~Suspend() { f = false; }
+    } suspend(ffd_suspended_);
     const bool exact = set.b("exact");
     const std::vector<SweepPeak> top = nms4(res.peaks, (unsigned)gv.thetas.size(), K, gv.wrap);
     char buf[320];
@@ -492,8 +498,9 @@ bool Engine::search_finish(const SweepOut& res, const SweepGrid& gv, const Mat3&
         std::memcpy(r.H, best.H.data(), sizeof r.H);
         r.score = best.score;
         r.improved = 1;
-        snprintf(buf, sizeof buf, "search done  nS %.1f (was %.1f)  θ %.1f° σ %.3f", best.score, s_cur,
-                 rs[0] * 180 / M_PI, rs[1]);
+        if (ffd_was) std::fill(ffd_cps_.begin(), ffd_cps_.end(), 0.f);  // the spline starts over at the new pose
+        snprintf(buf, sizeof buf, "search done  nS %.1f (was %.1f)  θ %.1f° σ %.3f%s", best.score, s_cur,
+                 rs[0] * 180 / M_PI, rs[1], ffd_was ? "  spline reset" : "");
     } else {
         snprintf(buf, sizeof buf, "search done  kept the current pose (nS %.1f ≥ %.1f)", s_cur, best.score);
     }
