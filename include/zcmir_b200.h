@@ -69,6 +69,30 @@ int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, con
  * settings (by zc_set_image_gray, zc_score or zc_features); otherwise -1 with zc_error. 0 / -1. */
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out);
 
+/* Gauss–Newton from each of n poses (Hs, row-major 3×3 each) at once for `iters` steps of the
+ * search's batched screen (src/search.zig gnBatch: a step only where it raises the pair score),
+ * the final poses into Hout and their scores into scores: the seeds of a search that starts from
+ * poses of its own (the learned proposal's). 0 / −1. */
+int32_t zcb_refine_poses(zc_engine* e, const double* Hs, uint32_t n, uint32_t iters, double* Hout, double* scores);
+
+/* The learned pose proposal's network (no counterpart in the reference): a circular 1-D CNN over
+ * a coarse sweep landscape x [n][6][36] (per rotation 10·i° from −180°, for each of 3 scales: the
+ * best and second-best map peak over the landscape's maximum), logits [n][3240] over the plain
+ * sweep's 360 × 9 rotation × scale grid (index 90·i + 9·dθ + s: rotation 10·i − 5 + dθ degrees
+ * from −180°, scale s). params: zcb_prop_nparams() float32 (conv 6→32 k5, conv 32→32 k5, conv
+ * 32→90 k3, each weights then bias). The calls allocate and free their own device memory; 0 / −1
+ * with the message from zcb_prop_error. */
+size_t zcb_prop_nparams(void);
+size_t zcb_prop_error(char* buf, size_t cap);
+int32_t zcb_prop_forward(const float* params, size_t np, const float* x, uint32_t n, float* logits);
+/* per-sample softmax cross-entropy loss[n] over labels (0..3239) and the mean loss's gradient */
+int32_t zcb_prop_grad(const float* params, size_t np, const float* x, const int32_t* labels, uint32_t n, float* loss,
+                      float* grad);
+/* Adam (β 0.9 / 0.999) over seeded shuffled minibatches of `batch` for `epochs`; params in/out;
+ * epoch_loss[epochs] (nullable) the mean training loss of each epoch */
+int32_t zcb_prop_train(float* params, size_t np, const float* x, const int32_t* labels, uint32_t n, uint32_t batch,
+                       uint32_t epochs, float lr, uint32_t seed, float* epoch_loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,61 @@
+"""The learned proposal's network on the GPU (zcb_prop_forward / zcb_prop_grad / zcb_prop_train)
+against the CPU oracle, and its training.
+
+Tolerances: logits within 1e-4 of the largest (float32 sums of at most 160 products per layer
+against float64); the per-sample loss within 1e-4 relative; the parameter gradient within 1e-4
+of the oracle's in norm."""
+import numpy as np
+import pytest
+
+from oracle import proposal_oracle as N
+from zcmir_b200 import proposal as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(seed, n=9):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, 1, (n, 6, 36)).astype(np.float32)
+    lab = rng.integers(0, 3240, n).astype(np.int32)
+    return x, lab
+
+
+def test_forward_and_gradient_match_oracle():
+    net = P.Network(seed=3)
+    x, lab = _data(1)
+    z = net.logits(x)
+    zr, _ = N.forward(net.params.astype(np.float64), x)
+    assert z.shape == (9, 3240)
+    assert np.abs(z - zr).max() <= 1e-4 * np.abs(zr).max()
+    loss, g = net.loss_grad(x, lab)
+    lr, gr = N.loss_grad(net.params.astype(np.float64), x, lab)
+    np.testing.assert_allclose(loss, lr, rtol=1e-4, atol=1e-5)
+    assert np.linalg.norm(g - gr) <= 1e-4 * np.linalg.norm(gr)
+
+
+def test_training_fits_a_learnable_map():
+    """Inputs whose label is the cell of their brightest entry (a circular peak to locate): the
+    GPU's Adam training takes the loss from about ln 3240 well down and locates the peaks."""
+    rng = np.random.default_rng(2)
+    n = 512
+    x = rng.uniform(0, 0.2, (n, 6, 36)).astype(np.float32)
+    pos = rng.integers(0, 36, n)
+    ch = rng.integers(0, 3, n)
+    x[np.arange(n), 2 * ch, pos] = 1.0
+    lab = (90 * pos + 9 * 5 + 4 * ch).astype(np.int32)
+    net = P.Network(seed=0)
+    hist = net.train(x, lab, epochs=60, batch=64, lr=3e-3, seed=1)
+    assert hist[0] > 6.0 and hist[-1] < 0.5 * hist[0], hist
+    assert np.mean(np.argmax(net.logits(x), axis=1) == lab) > 0.9
+
+
+def test_bins_round_trip_and_refusals():
+    for th in (-180.0, -3.0, 0.0, 47.0, 179.0):
+        for s in (0.8, 1.0, 1.25):
+            t2, s2 = P.bin_pose(P.fine_bin(th, s))
+            assert abs((t2 - th + 180) % 360 - 180) < 1e-9 and abs(s2 - s) < 1e-9
+    net = P.Network(seed=0)
+    x, lab = _data(0, 2)
+    lab[1] = 3240
+    with pytest.raises(RuntimeError, match="label outside"):
+        net.loss_grad(x, lab)

@@ -468,6 +468,17 @@ class Registrar:
             raise RuntimeError(f"sweep: {int(d['candidates'])} candidates, expected {nc}")
         return Sweep(sc, ix, d)
 
+    def refine_poses(self, Hs, iters=25):
+        """Gauss–Newton from each pose at once (zcb_refine_poses): (poses (n, 3, 3), scores (n,))."""
+        a = np.ascontiguousarray(np.asarray(Hs, np.float64).reshape(-1, 9))
+        n = len(a)
+        out = np.zeros_like(a)
+        sc = np.zeros(n)
+        self._check(self._lib.zcb_refine_poses(self._e, a.ctypes.data_as(_native.f64p), n, iters,
+                                               out.ctypes.data_as(_native.f64p), sc.ctypes.data_as(_native.f64p)),
+                    "refine_poses")
+        return out.reshape(n, 3, 3), sc
+
     def search_lanes(self, scores, index):
         """search() from every candidate's 4 lane maxima gathered from sharded sweeps."""
         sc = np.ascontiguousarray(scores, np.float32).reshape(-1)

@@ -95,6 +95,12 @@ SIGS = {
     "zcb_stack_maps": ([P, U32, ctypes.POINTER(f32p), u32p, u32p, f64p, U32, U32, ctypes.POINTER(ShiftResult), f64p], I32),
     "zcb_sweep": ([P, f64p, U32, U32, U32, U32, f32p, u32p, SZ, f64p, SZ], I32),
     "zcb_search_lanes": ([P, f32p, u32p, SZ, ctypes.POINTER(SearchResult)], I32),
+    "zcb_refine_poses": ([P, f64p, U32, U32, f64p, f64p], I32),
+    "zcb_prop_nparams": ([], SZ),
+    "zcb_prop_error": ([ctypes.c_char_p, SZ], SZ),
+    "zcb_prop_forward": ([f32p, SZ, f32p, U32, f32p], I32),
+    "zcb_prop_grad": ([f32p, SZ, f32p, ctypes.POINTER(ctypes.c_int32), U32, f32p, f32p], I32),
+    "zcb_prop_train": ([f32p, SZ, f32p, ctypes.POINTER(ctypes.c_int32), U32, U32, U32, ctypes.c_float, U32, f32p], I32),
     "zcb_settings_apply": ([ctypes.c_char_p, SZ, ctypes.c_char_p, SZ, ctypes.POINTER(SZ), ctypes.c_char_p, SZ, ctypes.POINTER(SZ)], I32),
 }
 

@@ -361,6 +361,24 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
     return 0;
 }
 
+int32_t zcb_refine_poses(zc_engine* e, const double* Hs, uint32_t n, uint32_t iters, double* Hout, double* scores) {
+    return guarded(e, "refine_poses", [&] {
+        if (n > 0 && (!Hs || !Hout || !scores)) return e->fail("refine_poses: null poses or outputs");
+        if (!e->search_check()) return false;
+        std::vector<zc::Mat3> in(n);
+        for (uint32_t i = 0; i < n; ++i) in[i] = mat(Hs + 9 * (size_t)i);
+        const std::vector<double> amps = zc::geo_amps(e->set.f("g_a0"), e->set.f("g_decay"),
+                                                      e->set.u("g_steps") > 0 ? e->set.u("g_steps") : 7);
+        std::vector<zc::ScoredPose> out;
+        if (!e->gn_batch(in, iters, amps, out)) return false;
+        for (uint32_t i = 0; i < n; ++i) {
+            std::memcpy(Hout + 9 * (size_t)i, out[i].H.data(), 9 * sizeof(double));
+            scores[i] = out[i].score;
+        }
+        return true;
+    });
+}
+
 int32_t zcb_search_lanes(zc_engine* e, const float* scores, const uint32_t* idx, size_t n, zc_search_result* out) {
     return guarded(e, "search_lanes", [&] { return e->search_lanes(scores, idx, n, out); });
 }

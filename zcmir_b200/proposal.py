@@ -1,0 +1,353 @@
+"""The learned pose proposal: a small network that reads a coarse sweep and proposes where the
+plain sweep's answer lies on its full rotation × scale grid.
+
+The plain search maps every candidate of a 360 × 9 grid (1° rotations × 9 scales in
+[0.8, 1.25]: 3240 shift maps) and refines the best peaks. The proposal maps only a 36 × 3 grid
+(10° × 3 scales: 108 maps); the coarse landscape — per coarse rotation and scale, its best and
+second-best map peaks — is what the network reads (an input that carries the answer: the
+images' per-pixel features themselves do not, being rotation-invariant). The network puts a
+distribution over the 3240 fine cells; the top k become poses (each placed by one shift map)
+that Gauss–Newton refines beside the coarse search's own best. The coarse search alone is the
+method without the network; the plain full search remains the reference of pose error.
+
+The network's forward, backward and Adam run on the GPU (zcb_prop_forward / zcb_prop_grad /
+zcb_prop_train in libzcmir.so). Trained weights ship as ``data/proposal_params.npy``, written by
+``python -m zcmir_b200.proposal train``; ``python -m zcmir_b200.proposal eval`` measures the
+three searches on held-out pairs.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _native
+
+FINE_NTH, FINE_NS = 360, 9
+COARSE_NTH, COARSE_NS = 36, 3
+S_MIN, S_MAX = 0.8, 1.25
+N_OUT = FINE_NTH * FINE_NS
+PARAMS_PATH = Path(__file__).resolve().parent / "data" / "proposal_params.npy"
+LAYERS = ((6, 32, 5), (32, 32, 5), (32, 90, 3))
+
+
+def _lib():
+    return _native.load()
+
+
+def _err(lib):
+    buf = ctypes.create_string_buffer(512)
+    lib.zcb_prop_error(buf, len(buf))
+    return buf.value.decode()
+
+
+# ── the grids ──
+
+def fine_theta(k):
+    """Rotation (degrees) of the plain sweep's k-th rotation (360 over the full turn, from −180°)."""
+    return -180.0 + 360.0 * k / FINE_NTH
+
+
+def fine_sigma(s):
+    return math.exp(math.log(S_MIN) + (math.log(S_MAX) - math.log(S_MIN)) * s / (FINE_NS - 1))
+
+
+def fine_bin(theta_deg, sigma):
+    """The network's output cell nearest to a rotation and scale: 90·i + 9·dθ + s, i the coarse
+    rotation (−180° + 10·i°), dθ the 1° offset in [−5, +4] stored as 0..9, s the scale."""
+    k = int(round((theta_deg + 180.0) * FINE_NTH / 360.0)) % FINE_NTH
+    s = int(round((math.log(sigma) - math.log(S_MIN)) / (math.log(S_MAX) - math.log(S_MIN)) * (FINE_NS - 1)))
+    s = min(max(s, 0), FINE_NS - 1)
+    i = int(round(k / 10.0)) % COARSE_NTH
+    dth = (k - 10 * i + 5) % FINE_NTH
+    return 90 * i + 9 * dth + s
+
+
+def bin_pose(b):
+    """(rotation degrees, scale) of an output cell (fine_bin's inverse)."""
+    i, o = divmod(int(b), 90)
+    dth, s = divmod(o, 9)
+    k = (10 * i - 5 + dth) % FINE_NTH
+    return fine_theta(k), fine_sigma(s)
+
+
+def coarse_settings():
+    return dict(sw_nth=COARSE_NTH, sw_ns=COARSE_NS, sw_smin=S_MIN, sw_smax=S_MAX)
+
+
+def fine_settings():
+    return dict(sw_nth=FINE_NTH, sw_ns=FINE_NS, sw_smin=S_MIN, sw_smax=S_MAX)
+
+
+def features(scores):
+    """The network's input [6][36] from a coarse sweep's lane maxima [108][lanes] (θ-major, then
+    σ): per scale j, channel 2j the candidate's best peak and 2j + 1 its second, both over the
+    landscape's maximum."""
+    sc = np.asarray(scores, np.float64).reshape(COARSE_NTH, COARSE_NS, -1)
+    srt = -np.sort(-sc, axis=2)
+    m = max(float(srt[..., 0].max()), 1e-30)
+    x = np.zeros((6, COARSE_NTH), np.float32)
+    for j in range(COARSE_NS):
+        x[2 * j] = srt[:, j, 0] / m
+        x[2 * j + 1] = (srt[:, j, 1] if srt.shape[2] > 1 else 0.0) / m
+    return x
+
+
+# ── the network ──
+
+class Network:
+    """The proposal network's parameters (float32) and its GPU passes."""
+
+    def __init__(self, params=None, seed=0):
+        n = int(_lib().zcb_prop_nparams())
+        if params is None:
+            rng = np.random.default_rng(seed)
+            parts = []
+            for ci, co, k in LAYERS:
+                parts += [rng.standard_normal(co * ci * k) * math.sqrt(2.0 / (ci * k)), np.zeros(co)]
+            params = np.concatenate(parts)
+        self.params = np.ascontiguousarray(params, np.float32)
+        if self.params.size != n:
+            raise ValueError(f"proposal network: {self.params.size} parameters, the library's network has {n}")
+
+    @classmethod
+    def load(cls, path=PARAMS_PATH):
+        return cls(np.load(path))
+
+    def save(self, path=PARAMS_PATH):
+        Path(path).parent.mkdir(parents=True, exist_ok=True)
+        np.save(path, self.params)
+
+    def logits(self, x):
+        lib = _lib()
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6, COARSE_NTH)
+        out = np.zeros((len(x), N_OUT), np.float32)
+        p = self.params
+        if lib.zcb_prop_forward(p.ctypes.data_as(_native.f32p), p.size, x.ctypes.data_as(_native.f32p), len(x),
+                                out.ctypes.data_as(_native.f32p)) != 0:
+            raise RuntimeError(_err(lib))
+        return out
+
+    def loss_grad(self, x, labels):
+        lib = _lib()
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6, COARSE_NTH)
+        lab = np.ascontiguousarray(labels, np.int32)
+        loss = np.zeros(len(x), np.float32)
+        g = np.zeros_like(self.params)
+        p = self.params
+        if lib.zcb_prop_grad(p.ctypes.data_as(_native.f32p), p.size, x.ctypes.data_as(_native.f32p),
+                             lab.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(x), loss.ctypes.data_as(_native.f32p),
+                             g.ctypes.data_as(_native.f32p)) != 0:
+            raise RuntimeError(_err(lib))
+        return loss, g
+
+    def train(self, x, labels, epochs=40, batch=128, lr=3e-3, seed=0):
+        """Adam on the GPU; the parameters in place; returns the mean training loss per epoch."""
+        lib = _lib()
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6, COARSE_NTH)
+        lab = np.ascontiguousarray(labels, np.int32)
+        hist = np.zeros(epochs, np.float32)
+        p = self.params
+        if lib.zcb_prop_train(p.ctypes.data_as(_native.f32p), p.size, x.ctypes.data_as(_native.f32p),
+                              lab.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(x), min(batch, len(x)), epochs,
+                              ctypes.c_float(lr), seed, hist.ctypes.data_as(_native.f32p)) != 0:
+            raise RuntimeError(_err(lib))
+        return hist
+
+    def top(self, x, k=8):
+        """The k most likely output cells of one landscape, best first."""
+        z = self.logits(x)[0]
+        return [int(b) for b in np.argsort(-z)[:k]]
+
+
+# ── the search ──
+
+def _prior(reg):
+    """The plain search's prior (the images' centres aligned) and the moving centre under it,
+    the point the candidates turn and scale about."""
+    (mw, mh), (fw, fh) = reg.image_size(0), reg.image_size(1)
+    H0 = np.array([[1, 0, (fw - mw) / 2], [0, 1, (fh - mh) / 2], [0, 0, 1.0]])
+    c = H0 @ [(mw + 1) / 2, (mh + 1) / 2, 1.0]
+    return H0, c[:2]
+
+
+def candidate_pose(reg, theta_deg, sigma):
+    """The sweep candidate's pose at a rotation and scale (about the moving centre, after the prior)."""
+    H0, c = _prior(reg)
+    a = math.radians(theta_deg)
+    L = sigma * np.array([[math.cos(a), -math.sin(a)], [math.sin(a), math.cos(a)]])
+    A = np.eye(3)
+    A[:2, :2] = L
+    A[:2, 2] = c - L @ c
+    return A @ H0
+
+
+def _with(reg, settings, fn):
+    keep = {k: reg.settings[k] for k in settings}
+    reg.configure(**settings)
+    try:
+        return fn()
+    finally:
+        reg.configure(**keep)
+
+
+def landscape(reg):
+    """(network input, coarse sweep) of the pair loaded in reg."""
+    sw = _with(reg, coarse_settings(), reg.sweep)
+    return features(sw.scores), sw
+
+
+def search(reg, net, k=8, with_network=True, iters=25):
+    """The proposal search on the pair loaded in reg from its current pose: the coarse search
+    (coarse sweep, its peaks screened and climbed) and, with the network, its top-k cells placed
+    by one shift map each and refined by Gauss–Newton; the best pose of both becomes the pose when
+    it beats the current one. Returns dict(H, score, maps, coarse_score)."""
+    def coarse_run():
+        sw = reg.sweep()
+        return sw, reg.search_lanes(sw.scores, sw.index)
+
+    sw, coarse = _with(reg, coarse_settings(), coarse_run)
+    best_H, best_s = coarse.H, coarse.score
+    maps = COARSE_NTH * COARSE_NS
+    if with_network:
+        seeds = []
+        for b in net.top(features(sw.scores), k):
+            H = candidate_pose(reg, *bin_pose(b))
+            sm = reg.shift_map(H, return_map=False)
+            seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
+        maps += len(seeds)
+        Hs, sc = reg.refine_poses(np.array(seeds), iters)
+        i = int(np.argmax(sc))
+        if sc[i] > best_s + max(1e-6 * abs(best_s), 1e-12):
+            best_H, best_s = Hs[i], float(sc[i])
+    if best_s > coarse.prev + max(1e-6 * abs(coarse.prev), 1e-12):
+        reg.pose = best_H
+    return dict(H=np.asarray(best_H), score=best_s, maps=maps, coarse_score=coarse.score)
+
+
+def corner_rms(H, Ht, w, h):
+    """RMS distance (px) of the moving image's four corners under two poses."""
+    d = []
+    for x, y in ((1, 1), (w, 1), (w, h), (1, h)):
+        a, b = H @ [x, y, 1.0], Ht @ [x, y, 1.0]
+        d.append(np.hypot(*(a[:2] / a[2] - b[:2] / b[2])))
+    return float(np.sqrt(np.mean(np.square(d))))
+
+
+# ── training data and training ──
+
+def truth_bin(H):
+    """The output cell of a similarity pose's rotation and scale (moving → fixed)."""
+    th = math.degrees(math.atan2(H[1, 0], H[0, 0]))
+    s = math.sqrt(abs(np.linalg.det(H[:2, :2])))
+    return fine_bin(th, s)
+
+
+def make_pair(seed, n=256):
+    """A seeded synthetic pair of the sweep workload's generator (blob field vs its 8-level
+    segmented modality under a random similarity: any rotation, a scale in [0.8, 1.25], a shift
+    of up to n/16 px)."""
+    from . import synth
+    rng = np.random.default_rng(10_000 + seed)
+    deg = float(rng.uniform(-180, 180))
+    scale = float(math.exp(rng.uniform(math.log(S_MIN), math.log(S_MAX))))
+    shift = tuple(float(v) for v in rng.uniform(-n / 16, n / 16, 2))
+    return synth.pair_similarity(n=n, seed=seed, deg=deg, scale=scale, shift=shift)
+
+
+def dataset(reg, seeds, n=256):
+    """(inputs [m][6][36], labels [m]) of the pairs of these seeds; the label is the planted
+    rotation and scale's cell of the plain sweep's grid (which the plain sweep recovers on this
+    generator)."""
+    xs, ys = [], []
+    for sd in seeds:
+        m, f, H = make_pair(sd, n)
+        reg.set_images(m, f, preprocess=False)
+        xs.append(landscape(reg)[0])
+        ys.append(truth_bin(H))
+    return np.stack(xs), np.array(ys, np.int32)
+
+
+def _train_main(a):
+    from . import Registrar
+    t0 = time.perf_counter()
+    with Registrar(half=False) as reg:
+        x, y = dataset(reg, range(a.train), a.n)
+        xv, yv = dataset(reg, range(a.train, a.train + a.val), a.n)
+    t_data = time.perf_counter() - t0
+    net = Network(seed=a.seed)
+    t0 = time.perf_counter()
+    hist = net.train(x, y, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
+    t_train = time.perf_counter() - t0
+    top = np.argsort(-net.logits(xv), axis=1)
+    acc = {k: float(np.mean([yv[i] in top[i, :k] for i in range(len(yv))])) for k in (1, 8)}
+    net.save(a.out)
+    print(json.dumps({"train_pairs": a.train, "val_pairs": a.val, "epochs": a.epochs, "loss_first": float(hist[0]),
+                      "loss_last": float(hist[-1]), "val_top1": acc[1], "val_top8": acc[8], "data_s": t_data,
+                      "train_s": t_train, "params": str(a.out)}))
+
+
+def _eval_main(a):
+    """Held-out pairs: the plain full search (the reference of pose error), the coarse search
+    alone and the coarse search with the network; success = corner RMS error ≤ 0.5 px against
+    the planted pose; the wall time of each search with the images already loaded."""
+    from . import Registrar
+    net = Network.load(a.params)
+    rows = []
+    with Registrar(half=False) as reg:
+        for sd in range(a.first, a.first + a.pairs):
+            m, f, Ht = make_pair(sd, a.n)
+            reg.set_images(m, f, preprocess=False)
+            mh, mw = m.shape
+            r = {}
+            for name in ("plain", "coarse", "proposal"):
+                reg.pose = np.eye(3)
+                t0 = time.perf_counter()
+                if name == "plain":
+                    H, maps = _with(reg, fine_settings(), reg.search).H, FINE_NTH * FINE_NS
+                else:
+                    out = search(reg, net, k=a.k, with_network=name == "proposal")
+                    H, maps = out["H"], out["maps"]
+                r[name] = dict(err=corner_rms(H, Ht, mw, mh), s=time.perf_counter() - t0, maps=maps)
+            rows.append(r)
+    summ = {}
+    for name in ("plain", "coarse", "proposal"):
+        e = np.array([r[name]["err"] for r in rows])
+        summ[name] = dict(success=float(np.mean(e <= 0.5)), median_err=float(np.median(e)),
+                          s_per_search=float(np.mean([r[name]["s"] for r in rows])), maps=rows[0][name]["maps"])
+    print(json.dumps({"pairs": a.pairs, "first_seed": a.first, "k": a.k, "summary": summ,
+                      "errors": {n: [round(r[n]["err"], 3) for r in rows] for n in ("plain", "coarse", "proposal")}}))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train", help="generate pairs, train on the GPU, write the weights")
+    t.add_argument("--train", type=int, default=3000)
+    t.add_argument("--val", type=int, default=300)
+    t.add_argument("--n", type=int, default=256)
+    t.add_argument("--epochs", type=int, default=40)
+    t.add_argument("--batch", type=int, default=128)
+    t.add_argument("--lr", type=float, default=3e-3)
+    t.add_argument("--seed", type=int, default=0)
+    t.add_argument("--out", type=Path, default=PARAMS_PATH)
+    e = sub.add_parser("eval", help="held-out pairs: plain, coarse and proposal searches")
+    e.add_argument("--pairs", type=int, default=32)
+    e.add_argument("--first", type=int, default=100_000)
+    e.add_argument("--n", type=int, default=256)
+    e.add_argument("--k", type=int, default=8)
+    e.add_argument("--params", type=Path, default=PARAMS_PATH)
+    a = ap.parse_args()
+    if a.cmd == "train":
+        _train_main(a)
+    else:
+        _eval_main(a)
+
+
+if __name__ == "__main__":
+    main()
