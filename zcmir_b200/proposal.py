@@ -146,7 +146,7 @@ class Network:
             raise RuntimeError(_err(lib))
         return loss, g
 
-    def train(self, x, labels, epochs=40, batch=128, lr=3e-3, seed=0):
+    def train(self, x, labels, epochs=60, batch=128, lr=1e-2, seed=0):
         """Adam on the GPU; the parameters in place; returns the mean training loss per epoch."""
         lib = _lib()
         x = np.ascontiguousarray(x, np.float32).reshape(-1, 6, COARSE_NTH)
@@ -331,9 +331,9 @@ def main():
     t.add_argument("--train", type=int, default=3000)
     t.add_argument("--val", type=int, default=300)
     t.add_argument("--n", type=int, default=256)
-    t.add_argument("--epochs", type=int, default=40)
+    t.add_argument("--epochs", type=int, default=60)
     t.add_argument("--batch", type=int, default=128)
-    t.add_argument("--lr", type=float, default=3e-3)
+    t.add_argument("--lr", type=float, default=1e-2)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--out", type=Path, default=PARAMS_PATH)
     e = sub.add_parser("eval", help="held-out pairs: plain, coarse and proposal searches")
