@@ -225,7 +225,7 @@ def search(reg, net, k=8, with_network=True, iters=25):
         i = int(np.argmax(sc))
         if sc[i] > best_s + max(1e-6 * abs(best_s), 1e-12):
             best_H, best_s = Hs[i], float(sc[i])
-    if best_s > coarse.prev + max(1e-6 * abs(coarse.prev), 1e-12):
+    if best_s > coarse.previous + max(1e-6 * abs(coarse.previous), 1e-12):
         reg.pose = best_H
     return dict(H=np.asarray(best_H), score=best_s, maps=maps, coarse_score=coarse.score)
 
@@ -280,6 +280,8 @@ def _train_main(a):
         x, y = dataset(reg, range(a.train), a.n)
         xv, yv = dataset(reg, range(a.train, a.train + a.val), a.n)
     t_data = time.perf_counter() - t0
+    if a.data:
+        np.savez_compressed(a.data, x=x, y=y, xv=xv, yv=yv)
     net = Network(seed=a.seed)
     t0 = time.perf_counter()
     hist = net.train(x, y, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
@@ -336,6 +338,7 @@ def main():
     t.add_argument("--lr", type=float, default=1e-2)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--out", type=Path, default=PARAMS_PATH)
+    t.add_argument("--data", type=Path, default=None, help="also write the landscapes and labels here (.npz)")
     e = sub.add_parser("eval", help="held-out pairs: plain, coarse and proposal searches")
     e.add_argument("--pairs", type=int, default=32)
     e.add_argument("--first", type=int, default=100_000)
