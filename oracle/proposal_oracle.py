@@ -4,8 +4,8 @@ TEST INFRASTRUCTURE ONLY: imported by ``tests/`` as the checker, never by the pr
 
 The network has no counterpart in the reference (it is this build's learned stage in front of
 the sweep): a circular 1-D CNN over the coarse sweep landscape, x [n][6][36] → conv 6→32 (k 5),
-ReLU, conv 32→32 (k 5), ReLU, conv 32→90 (k 3) → logits [n][90·36], the softmax cross-entropy
-over the 3240 logits. Each convolution is circular over the 36 positions:
+ReLU, conv 32→32 (k 5), ReLU, conv 32→90 (k 3) → [n][90][36], read position-major as 3240
+logits (index 90·i + o, position i, channel o), the softmax cross-entropy over them. Each convolution is circular over the 36 positions:
 y[c][l] = b[c] + Σ_j Σ_k w[c][j][k] x[j][(l + k − K//2) mod 36]. The parameter vector holds each
 layer's weights [co][ci][k] then its bias, layer by layer.
 """
@@ -49,7 +49,7 @@ def forward(p, x):
         z = np.einsum("cjk,njkl->ncl", w, xs) + b[None, :, None]
         cache.append((a, xs, z))
         a = np.maximum(z, 0.0) if li < len(layers) - 1 else z
-    return a.reshape(len(x), -1), cache
+    return a.transpose(0, 2, 1).reshape(len(x), -1), cache
 
 
 def loss_grad(p, x, labels):
@@ -63,7 +63,7 @@ def loss_grad(p, x, labels):
     dz = e / se
     dz[np.arange(n), labels] -= 1.0
     dz /= n
-    d = dz.reshape(n, LAYERS[-1][1], L)
+    d = dz.reshape(n, L, LAYERS[-1][1]).transpose(0, 2, 1)
     grads = []
     layers = unpack(p)
     for li in range(len(layers) - 1, -1, -1):

@@ -4,8 +4,9 @@
 //
 // Layers (parameters in this order, float32): conv 6 → 32 (k 5), ReLU, conv 32 → 32 (k 5), ReLU,
 // conv 32 → 90 (k 3); every convolution circular over the 36 rotations (the landscape wraps at
-// 360°), with a bias. Output [n][90][36] = 3240 logits per sample: position i (the coarse
-// rotation 10·i°), channel o = 9·dθ + s (fine rotation 10·i − 5 + dθ degrees, fine scale s of 9).
+// 360°), with a bias. The last layer's [n][90][36] is read position-major as 3240 logits per
+// sample, index 90·i + o: position i (the coarse rotation −180° + 10·i°), channel o = 9·dθ + s
+// (fine rotation −180° + 10·i − 5 + dθ degrees, fine scale s of 9).
 // The loss is the softmax cross-entropy over the 3240 logits.
 //
 // The network is 15 k parameters and a batch is 128 × 36 positions: every kernel is a plain
@@ -87,6 +88,15 @@ __global__ void k_conv_bwd_w(const float* __restrict__ dy, const float* __restri
     }
 }
 
+// [n][a][b] → [n][b][a]: the last layer's channel-major output as position-major logits (index
+// 90·i + o), and the logits' gradient back
+__global__ void k_transpose(const float* __restrict__ in, int n, int a, int b, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * a * b) return;
+    const int s = i / (a * b), r = i - s * a * b, u = r / b, w = r - u * b;
+    out[(size_t)s * a * b + (size_t)w * a + u] = in[i];
+}
+
 // the ReLU's gradient in place: dy = 0 where the layer's output was clipped
 __global__ void k_relu_bwd(float* __restrict__ dy, const float* __restrict__ y, int m) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -152,11 +162,12 @@ int blocks(int m) { return (m + 255) / 256; }
 // gradients (zeroed on the stream that uses them).
 struct Net {
     float *base = nullptr, *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
-    float *x = nullptr, *a1 = nullptr, *a2 = nullptr, *z = nullptr, *d1 = nullptr, *d2 = nullptr, *dz = nullptr;
+    float *x = nullptr, *a1 = nullptr, *a2 = nullptr, *a3 = nullptr, *z = nullptr, *d1 = nullptr, *d2 = nullptr,
+          *d3 = nullptr, *dz = nullptr;
     float* loss = nullptr;
     int* lab = nullptr;
     bool alloc(int n, cudaStream_t st) {
-        const size_t f = (size_t)4 * kNParams + (size_t)n * (kC0 + 2 * kC1 + 2 * kC2) * kL + 2 * (size_t)n * kOut + n;
+        const size_t f = (size_t)4 * kNParams + (size_t)n * (kC0 + 2 * kC1 + 2 * kC2) * kL + 4 * (size_t)n * kOut + n;
         if (cudaMalloc(&base, f * sizeof(float)) != cudaSuccess) return false;
         if (cudaMalloc(&lab, (size_t)n * sizeof(int)) != cudaSuccess) {
             cudaFree(base);
@@ -173,7 +184,8 @@ struct Net {
         p = take(kNParams), g = take(kNParams), m = take(kNParams), v = take(kNParams);
         x = take((size_t)n * kC0 * kL), a1 = take((size_t)n * kC1 * kL), d1 = take((size_t)n * kC1 * kL);
         a2 = take((size_t)n * kC2 * kL), d2 = take((size_t)n * kC2 * kL);
-        z = take((size_t)n * kOut), dz = take((size_t)n * kOut), loss = take(n);
+        a3 = take((size_t)n * kOut), z = take((size_t)n * kOut), d3 = take((size_t)n * kOut), dz = take((size_t)n * kOut);
+        loss = take(n);
         return true;
     }
     void release() {
@@ -195,13 +207,15 @@ struct Net {
     void forward(int n, cudaStream_t st) const {
         k_conv_fwd<<<blocks(n * kC1 * kL), 256, 0, st>>>(x, w1(), b1(), n, kC0, kC1, kK1, 1, a1);
         k_conv_fwd<<<blocks(n * kC2 * kL), 256, 0, st>>>(a1, w2(), b2(), n, kC1, kC2, kK2, 1, a2);
-        k_conv_fwd<<<blocks(n * kOut), 256, 0, st>>>(a2, w3(), b3(), n, kC2, kC3, kK3, 0, z);
+        k_conv_fwd<<<blocks(n * kOut), 256, 0, st>>>(a2, w3(), b3(), n, kC2, kC3, kK3, 0, a3);
+        k_transpose<<<blocks(n * kOut), 256, 0, st>>>(a3, n, kC3, kL, z);
     }
     // the loss per sample into `loss`, the mean loss's gradient into g
     void backward(int n, cudaStream_t st) const {
         k_softmax_xent<<<n, 256, 0, st>>>(z, lab, n, loss, dz);
-        k_conv_bwd_w<<<blocks(kNW3 + kC3), 256, 0, st>>>(dz, a2, n, kC2, kC3, kK3, gw(2), gb(2));
-        k_conv_bwd_data<<<blocks(n * kC2 * kL), 256, 0, st>>>(dz, w3(), n, kC2, kC3, kK3, d2);
+        k_transpose<<<blocks(n * kOut), 256, 0, st>>>(dz, n, kL, kC3, d3);
+        k_conv_bwd_w<<<blocks(kNW3 + kC3), 256, 0, st>>>(d3, a2, n, kC2, kC3, kK3, gw(2), gb(2));
+        k_conv_bwd_data<<<blocks(n * kC2 * kL), 256, 0, st>>>(d3, w3(), n, kC2, kC3, kK3, d2);
         k_relu_bwd<<<blocks(n * kC2 * kL), 256, 0, st>>>(d2, a2, n * kC2 * kL);
         k_conv_bwd_w<<<blocks(kNW2 + kC2), 256, 0, st>>>(d2, a1, n, kC1, kC2, kK2, gw(1), gb(1));
         k_conv_bwd_data<<<blocks(n * kC1 * kL), 256, 0, st>>>(d2, w2(), n, kC1, kC2, kK2, d1);

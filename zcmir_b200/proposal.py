@@ -7,8 +7,9 @@ The plain search maps every candidate of a 360 × 9 grid (1° rotations × 9 sca
 second-best map peaks — is what the network reads (an input that carries the answer: the
 images' per-pixel features themselves do not, being rotation-invariant). The network puts a
 distribution over the 3240 fine cells; the top k become poses (each placed by one shift map)
-that Gauss–Newton refines beside the coarse search's own best. The coarse search alone is the
-method without the network; the plain full search remains the reference of pose error.
+that Gauss–Newton refines together. The coarse search (the coarse sweep's peaks screened and
+climbed, the plain search's own steps) is the method without the network; the plain full search
+remains the reference of pose error.
 
 The network's forward, backward and Adam run on the GPU (zcb_prop_forward / zcb_prop_grad /
 zcb_prop_train in libzcmir.so). Trained weights ship as ``data/proposal_params.npy``, written by
@@ -202,32 +203,33 @@ def landscape(reg):
     return features(sw.scores), sw
 
 
-def search(reg, net, k=8, with_network=True, iters=25):
-    """The proposal search on the pair loaded in reg from its current pose: the coarse search
-    (coarse sweep, its peaks screened and climbed) and, with the network, its top-k cells placed
-    by one shift map each and refined by Gauss–Newton; the best pose of both becomes the pose when
-    it beats the current one. Returns dict(H, score, maps, coarse_score)."""
-    def coarse_run():
-        sw = reg.sweep()
-        return sw, reg.search_lanes(sw.scores, sw.index)
-
-    sw, coarse = _with(reg, coarse_settings(), coarse_run)
-    best_H, best_s = coarse.H, coarse.score
-    maps = COARSE_NTH * COARSE_NS
-    if with_network:
-        seeds = []
-        for b in net.top(features(sw.scores), k):
-            H = candidate_pose(reg, *bin_pose(b))
-            sm = reg.shift_map(H, return_map=False)
-            seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
-        maps += len(seeds)
-        Hs, sc = reg.refine_poses(np.array(seeds), iters)
-        i = int(np.argmax(sc))
-        if sc[i] > best_s + max(1e-6 * abs(best_s), 1e-12):
-            best_H, best_s = Hs[i], float(sc[i])
-    if best_s > coarse.previous + max(1e-6 * abs(coarse.previous), 1e-12):
+def search(reg, net, k=4, with_network=True, iters=25):
+    """The proposal search on the pair loaded in reg from its current pose. Both forms map the
+    coarse 36 × 3 grid. Without the network, the coarse search: the coarse sweep's peaks screened
+    and climbed (the plain search's own steps on the coarse grid). With it, the network's top-k
+    cells of the plain sweep's fine grid, each placed by one shift map and refined by
+    Gauss–Newton together. The result becomes the pose when it beats the current one. Returns
+    dict(H, score, maps)."""
+    cur = reg.score().mean
+    if not with_network:
+        r = _with(reg, coarse_settings(), lambda: reg.search_lanes(*_lanes(reg.sweep())))
+        return dict(H=np.asarray(r.H), score=r.score, maps=COARSE_NTH * COARSE_NS)
+    sw = _with(reg, coarse_settings(), reg.sweep)
+    seeds = []
+    for b in net.top(features(sw.scores), k):
+        H = candidate_pose(reg, *bin_pose(b))
+        sm = reg.shift_map(H, return_map=False)
+        seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
+    Hs, sc = reg.refine_poses(np.array(seeds), iters)
+    i = int(np.argmax(sc))
+    best_H, best_s = np.asarray(Hs[i]), float(sc[i])
+    if best_s > cur + max(1e-6 * abs(cur), 1e-12):
         reg.pose = best_H
-    return dict(H=np.asarray(best_H), score=best_s, maps=maps, coarse_score=coarse.score)
+    return dict(H=best_H, score=best_s, maps=COARSE_NTH * COARSE_NS + len(seeds))
+
+
+def _lanes(sw):
+    return sw.scores, sw.index
 
 
 def corner_rms(H, Ht, w, h):
@@ -343,7 +345,7 @@ def main():
     e.add_argument("--pairs", type=int, default=32)
     e.add_argument("--first", type=int, default=100_000)
     e.add_argument("--n", type=int, default=256)
-    e.add_argument("--k", type=int, default=8)
+    e.add_argument("--k", type=int, default=4)
     e.add_argument("--params", type=Path, default=PARAMS_PATH)
     a = ap.parse_args()
     if a.cmd == "train":
