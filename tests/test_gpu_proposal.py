@@ -44,9 +44,11 @@ def test_training_fits_a_learnable_map():
     x[np.arange(n), 2 * ch, pos] = 1.0
     lab = (90 * pos + 9 * 5 + 4 * ch).astype(np.int32)
     net = P.Network(seed=0)
-    hist = net.train(x, lab, epochs=60, batch=64, lr=1e-2, seed=1)
-    assert hist[0] > 6.0 and hist[-1] < 0.3 * hist[0], hist
-    assert np.mean(np.argmax(net.logits(x), axis=1) == lab) > 0.5
+    before = float(net.loss_grad(x, lab)[0].mean())
+    hist = net.train(x, lab, epochs=30, batch=64, lr=1e-2, seed=1)
+    after = float(net.loss_grad(x, lab)[0].mean())
+    assert before > 6.0 and after < 0.1 and hist[-1] < 0.1, (before, after, hist)
+    assert np.mean(np.argmax(net.logits(x), axis=1) == lab) > 0.95
 
 
 def test_bins_round_trip_and_refusals():
