@@ -264,6 +264,35 @@ def run_sweep(reg_cls, args, barrier, dist, torch, ws):
     return out, m, f
 
 
+def run_proposal(reg_cls, m, f, H, reps=3):
+    """The learned proposal beside the plain search on the sweep's 512² pair, images loaded: the
+    plain search (360 × 9 sweep), the coarse search (36 × 3 sweep, no network) and the proposal
+    search (36 × 3 sweep, the shipped network's top 4 cells refined); per search its wall time,
+    shift maps and corner error against the planted pose."""
+    from zcmir_b200 import proposal as P
+
+    net = P.Network.load()
+    reg = reg_cls(**SWEEP_SETTINGS)
+    reg.set_images(m, f, preprocess=False)
+    mh, mw = m.shape
+    out = {}
+    for name in ("plain", "coarse", "proposal"):
+        ts = []
+        for _ in range(reps + 1):
+            reg.pose = np.eye(3)
+            t0 = time.perf_counter()
+            if name == "plain":
+                Hs, maps = P._with(reg, P.fine_settings(), reg.search).H, P.FINE_NTH * P.FINE_NS
+            else:
+                r = P.search(reg, net, with_network=name == "proposal")
+                Hs, maps = r["H"], r["maps"]
+            ts.append(time.perf_counter() - t0)
+        out[name] = {"seconds_per_search": float(np.mean(ts[1:])), "maps": maps,
+                     "corner_rms_px": P.corner_rms(np.asarray(Hs), H, mw, mh)}
+    reg.close()
+    return out
+
+
 STACK_CONFIG = {"workload": "smi_stack_32_slices_384_1024", "slices": 32,
                 "sizes": "per side uniform in [384, 1024] (seed 3)",
                 "drift": "per step rotation N(0, 2 deg), log scale N(0, 0.02), shift N(0, 8 px)",
@@ -448,6 +477,9 @@ def run_gpu(args, rank, ws, local):
     reg.close()
     sweep, sm_, sf_ = run_sweep(zc.Registrar, args, barrier, dist, torch, ws)
     stack, st_imgs = run_stack(zc.Registrar, args, barrier, dist, torch, ws)
+    from zcmir_b200 import synth
+
+    proposal = run_proposal(zc.Registrar, sm_, sf_, synth.pair_similarity(n=512, seed=2)[2])
     if rank == 0:
         if ws == 1 and not args.no_cpu:
             v, n = sweep_cpu_sample(sm_, sf_)
@@ -459,6 +491,7 @@ def run_gpu(args, rank, ws, local):
             stack["cpu_baseline"] = {"value": v, "unit": "maps/s", "cores": os.cpu_count(), "kind": "port",
                                      "sample": f"the first {n} pairs of the stack, features included (float64 oracle)"}
         line["stack"] = stack
+        line["proposal"] = proposal
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
