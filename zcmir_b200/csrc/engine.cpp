@@ -98,6 +98,9 @@ Engine::~Engine() {
                       &ffd_pk_, &ffd_cells_, &ffd_coef_})
         b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
+    for (cudaEvent_t e : chunk_ev_)
+        if (e) cudaEventDestroy(e);
+    if (copy_st_) cudaStreamDestroy(copy_st_);
     cudaStreamDestroy(st);
 }
 
@@ -402,7 +405,7 @@ bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap,
     return true;
 }
 
-bool Engine::run_map(MapJob& job, cudaEvent_t* ev) {
+bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
     const MapGeom& g = job.g;
     const size_t cn = (size_t)g.W * g.Hh, gn = (size_t)g.cw * g.ch;
     const size_t hs = (size_t)job.plan.n_real * g.ny * g.WP * sizeof(float2);
@@ -457,7 +460,35 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev) {
         return false;
     rec(4);
     const bool tmem = row_pass != "split" && rows_tmem_supported(g.nx, job.plan.n_corr);
-    if (tmem) {
+    if (tmem && host_map) {
+        // the map's rows in chunks of whole waves (one block per SM per row), each chunk copied to
+        // the host on the copy stream while the next chunk runs; the last chunk is the smallest,
+        // so little copy is left after the last kernel
+        if (!copy_st_ && !cuda_ok(cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking), "shift_map")) return false;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int big = 4 * sms;
+        int y0 = 0, c = 0;
+        while (y0 < g.ny) {
+            const int rows = (g.ny - y0 > big + sms) ? big : g.ny - y0;
+            if (!cuda_ok(inverse_rows_score_tmem(q_.as<float2>(), g, job.plan, twiddles(g.nx), job.cp, n00,
+                                                 map_.as<float>(), best, zero, st, y0, rows),
+                         "inverse rows (tensor memory)"))
+                return false;
+            if (!chunk_ev_[c] && !cuda_ok(cudaEventCreateWithFlags(&chunk_ev_[c], cudaEventDisableTiming), "shift_map"))
+                return false;
+            const size_t off = (size_t)y0 * g.nx;
+            if (!cuda_ok(cudaEventRecord(chunk_ev_[c], st), "shift_map") ||
+                !cuda_ok(cudaStreamWaitEvent(copy_st_, chunk_ev_[c], 0), "shift_map") ||
+                !cuda_ok(cudaMemcpyAsync(host_map + off, map_.as<float>() + off, (size_t)rows * g.nx * 4,
+                                         cudaMemcpyDeviceToHost, copy_st_),
+                         "shift_map"))
+                return false;
+            y0 += rows;
+            c = (c + 1) % kChunkEvents;
+        }
+        counts[2]++;
+    } else if (tmem) {
         if (!cuda_ok(inverse_rows_score_tmem(q_.as<float2>(), g, job.plan, twiddles(g.nx), job.cp, n00, map_.as<float>(),
                                              best, zero, st),
                      "inverse rows (tensor memory)"))
@@ -480,15 +511,19 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     cudaEvent_t ev[kNumStages + 1];
     if (profiling)
         for (auto& e : ev) cudaEventCreate(&e);
-    if (!run_map(job, profiling ? ev : nullptr)) return false;
+    // with the tensor-memory row pass the map leaves in row chunks during the pass (copy_st_)
+    const bool chunked = map && row_pass != "split" && rows_tmem_supported(job.g.nx, job.plan.n_corr);
+    if (!run_map(job, profiling ? ev : nullptr, chunked ? map : nullptr)) return false;
     unsigned char host[24];
     if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 24, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
     counts[2]++;
-    if (map) {
+    if (map && !chunked) {
         if (!cuda_ok(cudaMemcpyAsync(map, map_.p, nn * 4, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
         counts[2]++;
     }
-    if (!cuda_ok(cudaStreamSynchronize(st), "shift_map")) return false;
+    if (!cuda_ok(cudaStreamSynchronize(st), "shift_map") ||
+        (chunked && !cuda_ok(cudaStreamSynchronize(copy_st_), "shift_map")))
+        return false;
     counts[1]++;
     counts[3]++;
     if (profiling) {

@@ -136,6 +136,9 @@ class Engine {
     int device = 0;
     cudaDeviceProp prop{};
     cudaStream_t st = nullptr;
+    cudaStream_t copy_st_ = nullptr;  // device → host copies that overlap the row pass
+    static constexpr int kChunkEvents = 16;
+    cudaEvent_t chunk_ev_[kChunkEvents] = {};
 
     // counters since the last zc_gpu_counts: launches, submits, reads, waits
     uint32_t counts[4] = {0, 0, 0, 0};
@@ -159,7 +162,9 @@ class Engine {
 
     // maps
     bool plan_map(const Mat3& H, bool exact, bool calibrated, unsigned cap, double min_overlap, MapJob& job);
-    bool run_map(MapJob& job, cudaEvent_t* ev /* kNumStages+1 events or null */);
+    // host_map (nullable): with the tensor-memory row pass, the map is copied there in row
+    // chunks on the copy stream during the pass (the caller synchronises copy_st_)
+    bool run_map(MapJob& job, cudaEvent_t* ev /* kNumStages+1 events or null */, float* host_map = nullptr);
     bool shift_map(const Mat3& H, bool exact, bool calibrated, unsigned cap, double min_overlap, zc_shift_result* out,
                    float* map, size_t map_len);
     bool shift_map_settings(const Mat3& H, zc_shift_result* out, float* map, size_t map_len);

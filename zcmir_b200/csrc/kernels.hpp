@@ -88,9 +88,11 @@ cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlan
                                size_t q_stride = 0, size_t map_stride = 0);
 // the same pass with the sums in tensor memory: a whole row per block (nx ∈ {512, 1024, 2048})
 bool rows_tmem_supported(int nx, int n_corr);
+// rows y0 .. y0 + rows − 1 of the map (rows < 0: to the last), so a caller can copy the map out
+// in row chunks while the later rows run
 cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const float2* tw_nx,
                                     const CombineParams& cp, const double* n00, float* map, unsigned long long* best,
-                                    float* zero, cudaStream_t st);
+                                    float* zero, cudaStream_t st, int y0 = 0, int rows = -1);
 // the split S of the row pass for nx (smallest divisor keeping its shared memory in budget); 0
 // when none fits
 int row_split(int nx, int n_corr);

@@ -69,7 +69,7 @@ template <int N, int NF, bool EXACT, bool CALIB>
 __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__ Q, size_t pstride, int WP, int n_corr,
                                                       const float2* __restrict__ tw, CombineParams cp,
                                                       const double* __restrict__ n00p, float* __restrict__ map,
-                                                      unsigned long long* best, float* zero_out) {
+                                                      unsigned long long* best, float* zero_out, int y0) {
     constexpr int TL = rows_tl<N>();           // threads per line
     constexpr int LINES = 512 / TL;            // lines per round
     constexpr int J = N / 128;                 // cells per TMEM lane
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
     const uint32_t tq = tb + ((uint32_t)(32 * (w & 3)) << 16);  // this warp's lane quadrant
     const int grp = w >> 2;                                      // 0..3: which j's this warp takes
 
-    const int y = blockIdx.x;
+    const int y = y0 + blockIdx.x;  // rows y0 .. y0 + gridDim.x − 1
     const int line = threadIdx.x / TL, t = threadIdx.x - line * TL;
     float2* buf = lines + line * PL;
     const int npairs = (n_corr + 1) / 2;
@@ -235,27 +235,29 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
 
 template <int N, int NF, bool EXACT, bool CALIB>
 cudaError_t launch_tmem(const float2* Q, const MapGeom& g, int n_corr, const float2* tw, const CombineParams& cp,
-                        const double* n00, float* map, unsigned long long* best, float* zero, cudaStream_t st) {
+                        const double* n00, float* map, unsigned long long* best, float* zero, cudaStream_t st, int y0,
+                        int rows) {
     constexpr int TL = rows_tl<N>(), LINES = 512 / TL;
     const int extra = n_corr > kTmemSlots ? n_corr - kTmemSlots : 0;
     const size_t sm = (size_t)LINES * padded_len(N) * sizeof(float2) + (size_t)extra * N * sizeof(float);
     auto k = k_rows_tmem<N, NF, EXACT, CALIB>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k<<<g.ny, 512, sm, st>>>(Q, (size_t)g.ny * g.WP, g.WP, n_corr, tw, cp, n00, map, best, zero);
+    k<<<rows, 512, sm, st>>>(Q, (size_t)g.ny * g.WP, g.WP, n_corr, tw, cp, n00, map, best, zero, y0);
     return cudaGetLastError();
 }
 
 template <int N>
 cudaError_t dispatch_tmem(const float2* Q, const MapGeom& g, int n_corr, const float2* tw, const CombineParams& cp,
-                          const double* n00, float* map, unsigned long long* best, float* zero, cudaStream_t st) {
+                          const double* n00, float* map, unsigned long long* best, float* zero, cudaStream_t st, int y0,
+                          int rows) {
     if (cp.nf == 4) {
-        if (!cp.exact) return launch_tmem<N, 4, false, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
-        if (cp.calib) return launch_tmem<N, 4, true, true>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
-        return launch_tmem<N, 4, true, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
+        if (!cp.exact) return launch_tmem<N, 4, false, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
+        if (cp.calib) return launch_tmem<N, 4, true, true>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
+        return launch_tmem<N, 4, true, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
     }
-    if (!cp.exact) return launch_tmem<N, 3, false, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
-    if (cp.calib) return launch_tmem<N, 3, true, true>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
-    return launch_tmem<N, 3, true, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st);
+    if (!cp.exact) return launch_tmem<N, 3, false, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
+    if (cp.calib) return launch_tmem<N, 3, true, true>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
+    return launch_tmem<N, 3, true, false>(Q, g, n_corr, tw, cp, n00, map, best, zero, st, y0, rows);
 }
 
 }  // namespace
@@ -264,11 +266,13 @@ bool rows_tmem_supported(int nx, int n_corr) { return (nx == 512 || nx == 1024 |
 
 cudaError_t inverse_rows_score_tmem(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const float2* tw_nx,
                                     const CombineParams& cp, const double* n00, float* map, unsigned long long* best,
-                                    float* zero, cudaStream_t st) {
+                                    float* zero, cudaStream_t st, int y0, int rows) {
+    if (rows < 0) rows = g.ny - y0;
+    if (y0 < 0 || rows <= 0 || y0 + rows > g.ny) return cudaErrorInvalidValue;
     switch (g.nx) {
-        case 512: return dispatch_tmem<512>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st);
-        case 1024: return dispatch_tmem<1024>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st);
-        case 2048: return dispatch_tmem<2048>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st);
+        case 512: return dispatch_tmem<512>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st, y0, rows);
+        case 1024: return dispatch_tmem<1024>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st, y0, rows);
+        case 2048: return dispatch_tmem<2048>(Q, g, plan.n_corr, tw_nx, cp, n00, map, best, zero, st, y0, rows);
         default: return cudaErrorNotSupported;
     }
 }
