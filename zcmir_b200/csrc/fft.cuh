@@ -289,6 +289,36 @@ __device__ __forceinline__ void mix_mid(float2* __restrict__ buf, const float2* 
     }
 }
 
+// the last stage of a compile-time line, its outputs to out(y, v)
+template <int N, int TL, bool INV, class Out>
+__device__ __forceinline__ void mix_last(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
+                                         Out&& out) {
+    using MX = Mix<N>;
+    constexpr int RL = MX::radix(MX::kStages - 1), NSL = N / RL, ML = N / RL, BML = (ML + TL - 1) / TL;
+    if (act) {
+#pragma unroll
+        for (int b = 0; b < BML; ++b) {
+            const int j = t + b * TL;
+            if (ML % TL == 0 || j < ML) {
+                float2 v[RL];
+#pragma unroll
+                for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
+                // k = j mod NSL = j
+                constexpr int OFFL = stage_tw_off(N, MX::kStages - 1);
+#pragma unroll
+                for (int r = 1; r < RL; ++r) {
+                    float2 w = __ldg(&tw[N + OFFL + (r - 1) * NSL + j]);
+                    if (INV) w.y = -w.y;
+                    v[r] = cmul(v[r], w);
+                }
+                dft<RL, INV>(v);
+#pragma unroll
+                for (int r = 0; r < RL; ++r) out(j + r * NSL, v[r]);
+            }
+        }
+    }
+}
+
 // The whole line with its ends in registers: the first stage's butterflies take their inputs
 // straight from in(y) (point y of the line, typically a global load) and the last stage hands
 // its outputs to out(y, v), so the line is staged into and out of shared memory by neither the
@@ -317,30 +347,29 @@ __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float
     }
     __syncthreads();
     mix_mid<N, TL, INV, 1, R0>(buf, tw, t, act);
-    constexpr int RL = MX::radix(MX::kStages - 1), NSL = N / RL, ML = N / RL, BML = (ML + TL - 1) / TL;
-    if (act) {
-#pragma unroll
-        for (int b = 0; b < BML; ++b) {
-            const int j = t + b * TL;
-            if (ML % TL == 0 || j < ML) {
-                float2 v[RL];
-#pragma unroll
-                for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
-                // k = j mod NSL = j
-                constexpr int OFFL = stage_tw_off(N, MX::kStages - 1);
-#pragma unroll
-                for (int r = 1; r < RL; ++r) {
-                    float2 w = __ldg(&tw[N + OFFL + (r - 1) * NSL + j]);
-                    if (INV) w.y = -w.y;
-                    v[r] = cmul(v[r], w);
-                }
-                dft<RL, INV>(v);
-#pragma unroll
-                for (int r = 0; r < RL; ++r) out(j + r * NSL, v[r]);
-            }
-        }
-    }
+    mix_last<N, TL, INV>(buf, tw, t, act, out);
 }
+
+// The whole line with its first stage's inputs already in registers: v = this thread's one
+// butterfly (j = t, so the first stage's butterflies must number exactly TL), then as mix_fft_io,
+// with between() called after the middle stages. Lets a caller load the next line's inputs while
+// this one transforms.
+template <int N, int TL, bool INV, class Out, class Between>
+__device__ __forceinline__ void mix_fft_regs(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
+                                             float2 (&v)[Mix<N>::radix(0)], Out&& out, Between&& between) {
+    constexpr int R0 = Mix<N>::radix(0);
+    static_assert(N / R0 == TL, "one first-stage butterfly per thread");
+    if (act) {
+        dft<R0, INV>(v);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) buf[pad_idx(t * R0 + r)] = v[r];
+    }
+    __syncthreads();
+    mix_mid<N, TL, INV, 1, R0>(buf, tw, t, act);
+    between();  // before the last stage: a caller may use registers the middle stages freed
+    mix_last<N, TL, INV>(buf, tw, t, act, out);
+}
+
 
 // The whole line with its first stage fed from in(y) (as mix_fft_io) and the result left in buf
 // in natural order, the block synchronised, as run() leaves it.

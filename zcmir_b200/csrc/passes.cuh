@@ -186,6 +186,65 @@ __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ 
         });
 }
 
+// The inverse columns as a persistent pipeline (lines of N points whose first stage has one
+// butterfly per line thread: N = 1024, 2048): 1 block per SM walks the items (column tile,
+// correlation slot), correlation fastest so the blocks running together share tiles in L2. Each
+// thread holds its next item's 2 × R0 products' operands in registers: they load while the
+// current item transforms, so the loads' latency hides behind the butterflies instead of
+// stalling a whole block (the one-item-per-block kernel above waits on them).
+template <int N>
+__global__ void __launch_bounds__(512, 1) k_inv_cols_pipe(const float2* __restrict__ ha, const float2* __restrict__ hb,
+                                                          size_t pstride, int WP, int ncols, CorrPlanDev plan,
+                                                          const float2* __restrict__ tw, int tx, float2* __restrict__ Q,
+                                                          int nitems) {
+    constexpr int TL = N / 16, R0 = Mix<N>::radix(0), M0 = N / R0;
+    static_assert(M0 == TL, "one first-stage butterfly per line thread");
+    extern __shared__ float2 smem[];
+    const int c = threadIdx.x % tx, t = threadIdx.x / tx;
+    float2* buf = smem + c * line_pitch(N);
+    const int nk = plan.n_corr;
+    float2 pa[R0], pb[R0];
+    auto load = [&](int item) {
+        const int k = item % nk, col = (item / nk) * tx + c;
+        const bool okc = col < ncols;
+        const float2* A = ha + (size_t)plan.ca[k] * pstride + (okc ? col : 0);
+        const float2* B = hb + (size_t)plan.cb[k] * pstride + (okc ? col : 0);
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const size_t o = (size_t)(t + r * M0) * WP;
+            pa[r] = okc ? __ldg(&A[o]) : make_float2(0.f, 0.f);
+            pb[r] = okc ? __ldg(&B[o]) : make_float2(0.f, 0.f);
+        }
+    };
+    int item = blockIdx.x;
+    if (item < nitems) load(item);
+    for (; item < nitems; item += gridDim.x) {
+        float2 v[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = cmulc(pa[r], pb[r]);
+        const int k = item % nk, col = (item / nk) * tx + c;
+        const bool okc = col < ncols;
+        float2* O = Q + (size_t)k * pstride + (okc ? col : 0);
+        if (item + (int)gridDim.x < nitems) load(item + gridDim.x);
+        mix_fft_regs<N, TL, true>(
+            buf, tw, t, true, v,
+            [&](int y, float2 val) {
+                if (okc) O[(size_t)y * WP] = val;
+            },
+            [] {});
+        __syncthreads();  // the line buffers are refilled by the next item
+    }
+}
+
+template <class F>
+struct FixedN {
+    static constexpr int value = 0;
+};
+template <int N, int TPL>
+struct FixedN<FixedLine<N, TPL>> {
+    static constexpr int value = N;
+};
+
 // ── inverse rows + per-shift score ──────────────────────────────────────────────────────────
 
 // block (row y, split s, item): every correlation pair's row (Hermitian full row from the half
@@ -448,6 +507,21 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
         return cudaGetLastError();
     } else if constexpr (P == Pass::InvCols) {
         const int ncols = g.nx / 2 + 1;
+        constexpr int NF = FixedN<F>::value;
+        if constexpr (NF == 1024 || NF == 2048) {
+            if (a.batch == 1 && tl == NF / 16) {
+                const int tx = 512 / tl;
+                const size_t sm = (size_t)tx * line_pitch(NF) * sizeof(float2);
+                const int nitems = plan.n_corr * ((ncols + tx - 1) / tx);
+                int dev = 0, sms = 148;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                cudaFuncSetAttribute(k_inv_cols_pipe<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                k_inv_cols_pipe<NF><<<std::min(nitems, sms), 512, sm, st>>>(a.half, a.half_b, pstride, g.WP, ncols, plan,
+                                                                            f.tw, tx, a.Q, nitems);
+                return cudaGetLastError();
+            }
+        }
         const int tx = col_tile(g.ny, tl, ncols);
         const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
         cudaFuncSetAttribute(k_inv_cols<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
