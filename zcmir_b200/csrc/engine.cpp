@@ -85,14 +85,19 @@ Engine::~Engine() {
         s.feat.release();
         s.mag.release();
         s.stack.release();
+        s.acf_dev.release();
+        if (s.built_ev) cudaEventDestroy(s.built_ev);
     }
+    if (up_ev_) cudaEventDestroy(up_ev_);
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
                       &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &sw_il_[0], &sw_il_[1], &sw_poses_,
                       &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
-    for (auto& s : stack_)
-        for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack}) b->release();
+    for (auto& s : stack_) {
+        for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack, &s.acf_dev}) b->release();
+        if (s.built_ev) cudaEventDestroy(s.built_ev);
+    }
     stack_res_.release();
     for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_, &ffd_dev_, &ffd_out_,
                       &ffd_pk_, &ffd_cells_, &ffd_coef_})
@@ -122,7 +127,15 @@ bool Engine::set_image(int s, const float* data, int w, int h, bool preprocess) 
     Side& sd = side[s];
     const size_t n = (size_t)w * h;
     if (!cuda_ok(sd.raw.ensure(n * 4), "set_image_gray")) return false;
-    if (!cuda_ok(cudaMemcpyAsync(sd.raw.p, data, n * 4, cudaMemcpyHostToDevice, st), "set_image_gray")) return false;
+    // the upload on the copy stream, so it runs beside the other side's feature build; it waits
+    // for this side's previous build (the only reader of `raw`), the build waits for it
+    if (!copy_st_ && !cuda_ok(cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking), "set_image_gray")) return false;
+    if (!up_ev_ && !cuda_ok(cudaEventCreateWithFlags(&up_ev_, cudaEventDisableTiming), "set_image_gray")) return false;
+    if ((sd.built_ev && !cuda_ok(cudaStreamWaitEvent(copy_st_, sd.built_ev, 0), "set_image_gray")) ||
+        !cuda_ok(cudaMemcpyAsync(sd.raw.p, data, n * 4, cudaMemcpyHostToDevice, copy_st_), "set_image_gray") ||
+        !cuda_ok(cudaEventRecord(up_ev_, copy_st_), "set_image_gray") ||
+        !cuda_ok(cudaStreamWaitEvent(st, up_ev_, 0), "set_image_gray"))
+        return false;
     sd.has = true;
     sd.w = w;
     sd.h = h;
@@ -219,27 +232,25 @@ bool Engine::build_side(int s) {
               cuda_ok(rank_tmp_.ensure(n * 4), "features") && cuda_ok(fs_stats_.ensure(22 * 8), "features") &&
               cuda_ok(fs_hist_.ensure(256 * 4), "features") && cuda_ok(fs_wt_.ensure(20 * 4), "features") &&
               cuda_ok(fs_acfpart_.ensure((size_t)ntiles * 1156 * 4), "features") &&
-              cuda_ok(fs_acf_.ensure(1156 * 8), "features");
+              cuda_ok(sd.acf_dev.ensure(1156 * 8), "features");
     if (!ok) return false;
     fs_.stats = fs_stats_.as<double>();
     fs_.hist = fs_hist_.as<unsigned>();
     fs_.wt = fs_wt_.as<float>();
     fs_.acf_part = fs_acfpart_.as<float>();
     fs_.acf_part_cap = fs_acfpart_.cap / 4;
-    fs_.acf = fs_acf_.as<double>();
+    fs_.acf = sd.acf_dev.as<double>();
     if (!bake(s)) return false;
     if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rank_tmp_.as<float>(), sd.feat.as<float>(),
                                 sd.mag.as<float>(), sd.stack.as<float>(), fs_, st),
                  "features"))
         return false;
     counts[0] += 13;
-    double acf[1156];
-    if (!cuda_ok(cudaMemcpyAsync(acf, fs_.acf, sizeof acf, cudaMemcpyDeviceToHost, st), "features")) return false;
-    if (!cuda_ok(cudaStreamSynchronize(st), "features")) return false;
-    counts[2] += 1;
-    counts[3] += 1;
-    // normalise by the zero lag (smi.wgsl:1572-1578)
-    for (int k = 0; k < 1156; ++k) sd.acf[k] = acf[k] / std::max(acf[144 * 4 + (k & 3)], 1e-12);
+    if (!sd.built_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.built_ev, cudaEventDisableTiming), "features")) return false;
+    if (!cuda_ok(cudaEventRecord(sd.built_ev, st), "features")) return false;
+    // the autocorrelation is read back when next needed (finish_acf), so the host does not wait
+    // for the build here
+    sd.acf_pending = true;
     sd.built = true;
     sd.mode = mode;
     sd.half = half;
@@ -255,6 +266,28 @@ bool Engine::need_images() {
         if (!sd.built || sd.mode != mode || sd.half != set.b("half") || (sd.preprocess && sd.bake != bake_key()))
             if (!build_side(s)) return false;
     }
+    return finish_acf();
+}
+
+bool Engine::finish_acf() {
+    double raw[2][1156];
+    bool any = false;
+    for (int s = 0; s < 2; ++s)
+        if (side[s].acf_pending) {
+            if (!cuda_ok(cudaMemcpyAsync(raw[s], side[s].acf_dev.p, sizeof raw[s], cudaMemcpyDeviceToHost, st), "features"))
+                return false;
+            any = true;
+        }
+    if (!any) return true;
+    if (!cuda_ok(cudaStreamSynchronize(st), "features")) return false;
+    counts[2] += 1;
+    counts[3] += 1;
+    for (int s = 0; s < 2; ++s)
+        if (side[s].acf_pending) {
+            // normalise by the zero lag (smi.wgsl:1572-1578)
+            for (int k = 0; k < 1156; ++k) side[s].acf[k] = raw[s][k] / std::max(raw[s][144 * 4 + (k & 3)], 1e-12);
+            side[s].acf_pending = false;
+        }
     return true;
 }
 

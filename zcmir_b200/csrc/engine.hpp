@@ -41,6 +41,9 @@ struct Side {
     DevBuf mag;    // Sobel magnitude of the rank
     DevBuf stack;  // [1, f0..f3]
     std::array<double, 1156> acf{};  // normalised autocorrelation, 289 lags × 4 planes
+    DevBuf acf_dev;                  // its raw sums on the device, read back when next needed
+    bool acf_pending = false;        // acf_dev holds sums that acf does not yet
+    cudaEvent_t built_ev = nullptr;  // recorded after the last build, which read `raw`
     bool built = false;
     int mode = -1;
     bool half = false;
@@ -136,7 +139,8 @@ class Engine {
     int device = 0;
     cudaDeviceProp prop{};
     cudaStream_t st = nullptr;
-    cudaStream_t copy_st_ = nullptr;  // device → host copies that overlap the row pass
+    cudaStream_t copy_st_ = nullptr;  // copies that overlap kernels: image uploads, map row chunks
+    cudaEvent_t up_ev_ = nullptr;     // an image upload done
     static constexpr int kChunkEvents = 16;
     cudaEvent_t chunk_ev_[kChunkEvents] = {};
 
@@ -156,6 +160,8 @@ class Engine {
     // RGBA8 → gray (0.299 R + 0.587 G + 0.114 B), always preprocessed (src/engine.zig:422-426)
     bool set_image_rgba(int s, const unsigned char* rgba, int w, int h);
     bool need_images();
+    // the sides' autocorrelations read back from the device (one wait for both), normalised
+    bool finish_acf();
     bool features(int s, float* out, size_t len);
     bool work_image(int s, float* out, size_t len);
     double pair_area() const;
