@@ -89,6 +89,11 @@ Engine::~Engine() {
         if (s.built_ev) cudaEventDestroy(s.built_ev);
     }
     if (up_ev_) cudaEventDestroy(up_ev_);
+    for (DevBuf* b : {&fs2_stats_, &fs2_hist_, &fs2_wt_, &fs2_acfpart_, &rank_tmp2_}) b->release();
+    if (st2_) {
+        cudaStreamSynchronize(st2_);
+        cudaStreamDestroy(st2_);
+    }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
                       &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &sw_il_[0], &sw_il_[1], &sw_poses_,
@@ -133,9 +138,12 @@ bool Engine::set_image(int s, const float* data, int w, int h, bool preprocess) 
     if (!up_ev_ && !cuda_ok(cudaEventCreateWithFlags(&up_ev_, cudaEventDisableTiming), "set_image_gray")) return false;
     if ((sd.built_ev && !cuda_ok(cudaStreamWaitEvent(copy_st_, sd.built_ev, 0), "set_image_gray")) ||
         !cuda_ok(cudaMemcpyAsync(sd.raw.p, data, n * 4, cudaMemcpyHostToDevice, copy_st_), "set_image_gray") ||
-        !cuda_ok(cudaEventRecord(up_ev_, copy_st_), "set_image_gray") ||
-        !cuda_ok(cudaStreamWaitEvent(st, up_ev_, 0), "set_image_gray"))
+        !cuda_ok(cudaEventRecord(up_ev_, copy_st_), "set_image_gray"))
         return false;
+    sd.has = true;
+    sd.preprocess = preprocess;
+    cudaStream_t bs = st;
+    if (!build_stream(s, bs) || !cuda_ok(cudaStreamWaitEvent(bs, up_ev_, 0), "set_image_gray")) return false;
     sd.has = true;
     sd.w = w;
     sd.h = h;
@@ -168,13 +176,13 @@ std::string Engine::bake_key() const {
     return b;
 }
 
-bool Engine::bake(int s) {
+bool Engine::bake(int s, cudaStream_t bs) {
     Side& sd = side[s];
     const int n = sd.w * sd.h;
     const bool half = set.b("half");
     float* work = sd.work.as<float>();
     sd.bake = sd.preprocess ? bake_key() : std::string();
-    if (!sd.preprocess) return cuda_ok(cudaMemcpyAsync(work, sd.raw.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st), "features");
+    if (!sd.preprocess) return cuda_ok(cudaMemcpyAsync(work, sd.raw.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, bs), "features");
     // CLAHE (clip limit 40, the settings' grid and bins) from the f32 image, else its texels
     if (set.b("clahe")) {
         if (!cuda_ok(pp_clahe_.ensure(clahe_scratch_bytes((int)set.u("clahe_grid"), (int)set.u("clahe_bins"))), "clahe") ||
@@ -220,34 +228,55 @@ bool Engine::bake(int s) {
     return true;
 }
 
+// The stream a side's features build on: side 1 without preprocessing on a stream of its own
+// with its own scratch, so its build runs beside side 0's (the preprocessing scratch is shared,
+// so preprocessed sides build in order on the engine stream). Safe because every call that reads
+// a side's buffers waits for its work before returning: when a build starts, the only pending
+// work is other builds.
+bool Engine::build_stream(int s, cudaStream_t& bs) {
+    bs = st;
+    if (s != 1 || side[s].preprocess) return true;
+    if (!st2_ && !cuda_ok(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking), "features")) return false;
+    bs = st2_;
+    return true;
+}
+
 bool Engine::build_side(int s) {
     Side& sd = side[s];
     const size_t n = (size_t)sd.w * sd.h;
+    cudaStream_t bs = st;
+    if (!build_stream(s, bs)) return false;
+    const bool own = bs != st;
+    DevBuf &stats = own ? fs2_stats_ : fs_stats_, &hist = own ? fs2_hist_ : fs_hist_, &wt = own ? fs2_wt_ : fs_wt_;
+    DevBuf &part = own ? fs2_acfpart_ : fs_acfpart_, &rtmp = own ? rank_tmp2_ : rank_tmp_;
+    FeatScratch& fsc = own ? fs2_ : fs_;
     const std::string& fm = set.e("smi_features");
     const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
     const bool half = set.b("half");
     const int ntiles = ((sd.w + 31) / 32) * ((sd.h + 31) / 32);
     bool ok = cuda_ok(sd.work.ensure(n * 4), "features") && cuda_ok(sd.feat.ensure(n * 16), "features") &&
               cuda_ok(sd.mag.ensure(n * 4), "features") && cuda_ok(sd.stack.ensure(n * 20), "features") &&
-              cuda_ok(rank_tmp_.ensure(n * 4), "features") && cuda_ok(fs_stats_.ensure(22 * 8), "features") &&
-              cuda_ok(fs_hist_.ensure(256 * 4), "features") && cuda_ok(fs_wt_.ensure(20 * 4), "features") &&
-              cuda_ok(fs_acfpart_.ensure((size_t)ntiles * 1156 * 4), "features") &&
+              cuda_ok(rtmp.ensure(n * 4), "features") && cuda_ok(stats.ensure(22 * 8), "features") &&
+              cuda_ok(hist.ensure(256 * 4), "features") && cuda_ok(wt.ensure(20 * 4), "features") &&
+              cuda_ok(part.ensure((size_t)ntiles * 1156 * 4), "features") &&
               cuda_ok(sd.acf_dev.ensure(1156 * 8), "features");
     if (!ok) return false;
-    fs_.stats = fs_stats_.as<double>();
-    fs_.hist = fs_hist_.as<unsigned>();
-    fs_.wt = fs_wt_.as<float>();
-    fs_.acf_part = fs_acfpart_.as<float>();
-    fs_.acf_part_cap = fs_acfpart_.cap / 4;
-    fs_.acf = sd.acf_dev.as<double>();
-    if (!bake(s)) return false;
-    if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rank_tmp_.as<float>(), sd.feat.as<float>(),
-                                sd.mag.as<float>(), sd.stack.as<float>(), fs_, st),
+    fsc.stats = stats.as<double>();
+    fsc.hist = hist.as<unsigned>();
+    fsc.wt = wt.as<float>();
+    fsc.acf_part = part.as<float>();
+    fsc.acf_part_cap = part.cap / 4;
+    fsc.acf = sd.acf_dev.as<double>();
+    if (!bake(s, bs)) return false;
+    if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rtmp.as<float>(), sd.feat.as<float>(),
+                                sd.mag.as<float>(), sd.stack.as<float>(), fsc, bs),
                  "features"))
         return false;
     counts[0] += 13;
     if (!sd.built_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.built_ev, cudaEventDisableTiming), "features")) return false;
-    if (!cuda_ok(cudaEventRecord(sd.built_ev, st), "features")) return false;
+    if (!cuda_ok(cudaEventRecord(sd.built_ev, bs), "features")) return false;
+    // the engine stream's later work (maps, scores) waits for a build on the side stream
+    if (own && !cuda_ok(cudaStreamWaitEvent(st, sd.built_ev, 0), "features")) return false;
     // the autocorrelation is read back when next needed (finish_acf), so the host does not wait
     // for the build here
     sd.acf_pending = true;

@@ -266,13 +266,17 @@ class Engine {
     bool build_side(int s);
     // the work image of side s from its raw image: CLAHE, band pass, invert as set (preprocessed
     // sides), else the raw image as is
-    bool bake(int s);
+    bool bake(int s, cudaStream_t bs);
+    bool build_stream(int s, cudaStream_t& bs);
     std::string bake_key() const;
     bool line_plan(int n, LinePlan& p);
     const float2* twiddles(int n);
 
     FeatScratch fs_;
     DevBuf fs_stats_, fs_hist_, fs_wt_, fs_acfpart_, fs_acf_, rank_tmp_;
+    FeatScratch fs2_;  // side 1's own scratch when it builds on st2_
+    DevBuf fs2_stats_, fs2_hist_, fs2_wt_, fs2_acfpart_, rank_tmp2_;
+    cudaStream_t st2_ = nullptr;
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
     DevBuf rs_fwd_, rs_inv_, rs_map_;
