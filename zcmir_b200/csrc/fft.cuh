@@ -296,7 +296,7 @@ __device__ __forceinline__ void mix_last(float2* __restrict__ buf, const float2*
     using MX = Mix<N>;
     constexpr int RL = MX::radix(MX::kStages - 1), NSL = N / RL, ML = N / RL, BML = (ML + TL - 1) / TL;
     if (act) {
-#pragma unroll
+#pragma unroll 1
         for (int b = 0; b < BML; ++b) {
             const int j = t + b * TL;
             if (ML % TL == 0 || j < ML) {
@@ -352,8 +352,8 @@ __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float
 
 // The whole line with its first stage's inputs already in registers: v = this thread's one
 // butterfly (j = t, so the first stage's butterflies must number exactly TL), then as mix_fft_io,
-// with between() called after the middle stages. Lets a caller load the next line's inputs while
-// this one transforms.
+// with between() called once the first stage has consumed v. Lets a caller start loading the next
+// line's inputs while this one transforms.
 template <int N, int TL, bool INV, class Out, class Between>
 __device__ __forceinline__ void mix_fft_regs(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
                                              float2 (&v)[Mix<N>::radix(0)], Out&& out, Between&& between) {
@@ -365,8 +365,8 @@ __device__ __forceinline__ void mix_fft_regs(float2* __restrict__ buf, const flo
         for (int r = 0; r < R0; ++r) buf[pad_idx(t * R0 + r)] = v[r];
     }
     __syncthreads();
+    between();  // after the first stage: v is consumed, so the caller may refill its source
     mix_mid<N, TL, INV, 1, R0>(buf, tw, t, act);
-    between();  // before the last stage: a caller may use registers the middle stages freed
     mix_last<N, TL, INV>(buf, tw, t, act, out);
 }
 
