@@ -36,6 +36,23 @@ __host__ __device__ __forceinline__ int line_pitch(int n) {
     return p + ((4 - (p & 15)) & 15);
 }
 
+// Padded slots of the points i0 + r·D (r = 0, 1, ...) from p0 = pad_idx(i0), for a compile-time
+// step D, folded to constant offsets: when D is a multiple of 16 every step adds D + D/16; when
+// all the points lie in one aligned group of 16 (the caller guarantees it) every step adds D.
+template <int D, bool ONE_GROUP = false>
+__device__ __forceinline__ int pad_at(int p0, int r) {
+    static_assert(D % 16 == 0 || ONE_GROUP, "steps that cross 16-point groups need pad_idx");
+    return p0 + r * (D % 16 == 0 ? D + D / 16 : D);
+}
+
+// The padded slot of output r of first-stage butterfly j (point j·R0 + r): one aligned group of
+// 16 holds the butterfly when R0 divides 16.
+template <int R0>
+__device__ __forceinline__ int first_slot(int j, int r) {
+    if constexpr (16 % R0 == 0) return pad_at<1, true>(pad_idx(j * R0), r);
+    else return pad_idx(j * R0 + r);
+}
+
 // ── small DFTs, natural order in and out; INV flips the sign of the exponent ──
 
 template <bool INV>
@@ -240,8 +257,14 @@ __device__ __forceinline__ void mix_stage(float2* __restrict__ buf, const float2
         for (int b = 0; b < BM; ++b) {
             const int j = t + b * TL;
             if (M % TL == 0 || j < M) {
+                if constexpr (M % 16 == 0) {
+                    const int p = pad_idx(j);
 #pragma unroll
-                for (int r = 0; r < R; ++r) v[b][r] = buf[pad_idx(j + r * M)];
+                    for (int r = 0; r < R; ++r) v[b][r] = buf[pad_at<M>(p, r)];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[b][r] = buf[pad_idx(j + r * M)];
+                }
             }
         }
     }
@@ -262,8 +285,16 @@ __device__ __forceinline__ void mix_stage(float2* __restrict__ buf, const float2
                 }
                 dft<R, INV>(v[b]);
                 const int base = (j - k) * R + k;
+                // a butterfly's outputs are R points NS apart from base; when R·NS divides 16
+                // they lie in one aligned group of 16 (base mod R·NS = k < NS)
+                if constexpr (NS % 16 == 0 || 16 % (R * NS) == 0) {
+                    const int p = pad_idx(base);
 #pragma unroll
-                for (int r = 0; r < R; ++r) buf[pad_idx(base + r * NS)] = v[b][r];
+                    for (int r = 0; r < R; ++r) buf[pad_at<NS, (NS % 16 != 0)>(p, r)] = v[b][r];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) buf[pad_idx(base + r * NS)] = v[b][r];
+                }
             }
         }
     }
@@ -301,8 +332,14 @@ __device__ __forceinline__ void mix_last(float2* __restrict__ buf, const float2*
             const int j = t + b * TL;
             if (ML % TL == 0 || j < ML) {
                 float2 v[RL];
+                if constexpr (ML % 16 == 0) {
+                    const int p = pad_idx(j);
 #pragma unroll
-                for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
+                    for (int r = 0; r < RL; ++r) v[r] = buf[pad_at<ML>(p, r)];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) v[r] = buf[pad_idx(j + r * ML)];
+                }
                 // k = j mod NSL = j
                 constexpr int OFFL = stage_tw_off(N, MX::kStages - 1);
 #pragma unroll
@@ -341,7 +378,7 @@ __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float
                 for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
                 dft<R0, INV>(v);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) buf[pad_idx(j * R0 + r)] = v[r];
+                for (int r = 0; r < R0; ++r) buf[first_slot<R0>(j, r)] = v[r];
             }
         }
     }
@@ -362,7 +399,7 @@ __device__ __forceinline__ void mix_fft_regs(float2* __restrict__ buf, const flo
     if (act) {
         dft<R0, INV>(v);
 #pragma unroll
-        for (int r = 0; r < R0; ++r) buf[pad_idx(t * R0 + r)] = v[r];
+        for (int r = 0; r < R0; ++r) buf[first_slot<R0>(t, r)] = v[r];
     }
     __syncthreads();
     between();  // after the first stage: v is consumed, so the caller may refill its source
@@ -387,7 +424,7 @@ __device__ __forceinline__ void mix_fft_in(float2* __restrict__ buf, const float
                 for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
                 dft<R0, INV>(v);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) buf[pad_idx(j * R0 + r)] = v[r];
+                for (int r = 0; r < R0; ++r) buf[first_slot<R0>(j, r)] = v[r];
             }
         }
     }
