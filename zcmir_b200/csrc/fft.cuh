@@ -89,15 +89,10 @@ __device__ __forceinline__ void dft4(float2* v) {
     v[3] = csub(a1, a3);
 }
 
+// dft8 after its first butterfly layer: a_r = v_r + v_{r+4}, b_r = v_r − v_{r+4}
 template <bool INV>
-__device__ __forceinline__ void dft8(float2* v) {
+__device__ __forceinline__ void dft8_ab(float2 (&a)[4], float2 (&b)[4], float2* v) {
     const float h = 0.70710678118654752440f;
-    float2 a[4], b[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        a[r] = cadd(v[r], v[r + 4]);
-        b[r] = csub(v[r], v[r + 4]);
-    }
     // b_r ·= w8^r
     b[1] = INV ? make_float2(h * (b[1].x - b[1].y), h * (b[1].x + b[1].y))
                : make_float2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
@@ -114,19 +109,29 @@ __device__ __forceinline__ void dft8(float2* v) {
 }
 
 template <bool INV>
-__device__ __forceinline__ void dft16(float2* v) {
+__device__ __forceinline__ void dft8(float2* v) {
+    float2 a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        a[r] = cadd(v[r], v[r + 4]);
+        b[r] = csub(v[r], v[r + 4]);
+    }
+    dft8_ab<INV>(a, b, v);
+}
+
+// dft16 after its first butterfly layer: a_r = v_r + v_{r+8}, d_r = v_r − v_{r+8}
+template <bool INV>
+__device__ __forceinline__ void dft16_ad(float2 (&a)[8], float2 (&d)[8], float2* v) {
     // w16^r = (cos 2πr/16, ∓sin 2πr/16), r = 0..7
     const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
     const float h = 0.70710678118654752440f;
     const float cs[8] = {1.f, c1, h, s1, 0.f, -s1, -h, -c1};
     const float sn[8] = {0.f, s1, h, c1, 1.f, c1, h, s1};
-    float2 a[8], b[8];
+    float2 b[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-        a[r] = cadd(v[r], v[r + 8]);
-        const float2 d = csub(v[r], v[r + 8]);
         const float si = INV ? sn[r] : -sn[r];
-        b[r] = make_float2(d.x * cs[r] - d.y * si, d.x * si + d.y * cs[r]);
+        b[r] = make_float2(d[r].x * cs[r] - d[r].y * si, d[r].x * si + d[r].y * cs[r]);
     }
     dft8<INV>(a);
     dft8<INV>(b);
@@ -137,6 +142,17 @@ __device__ __forceinline__ void dft16(float2* v) {
     }
 }
 
+template <bool INV>
+__device__ __forceinline__ void dft16(float2* v) {
+    float2 a[8], d[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        a[r] = cadd(v[r], v[r + 8]);
+        d[r] = csub(v[r], v[r + 8]);
+    }
+    dft16_ad<INV>(a, d, v);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2* v) {
     if constexpr (R == 2) dft2<INV>(v);
@@ -144,6 +160,32 @@ __device__ __forceinline__ void dft(float2* v) {
     else if constexpr (R == 4) dft4<INV>(v);
     else if constexpr (R == 8) dft8<INV>(v);
     else dft16<INV>(v);
+}
+
+// The small DFT of R points whose upper half (v_r, r ≥ R/2) is zero and is not read: the first
+// butterfly layer reduces to copies (zero-padded lines: their first stage reads half the points).
+template <int R, bool INV>
+__device__ __forceinline__ void dft_lo(float2* v) {
+    static_assert(R % 2 == 0, "an odd radix has no zero half");
+    if constexpr (R == 16) {
+        float2 a[8], d[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) a[r] = d[r] = v[r];
+        dft16_ad<INV>(a, d, v);
+    } else if constexpr (R == 8) {
+        float2 a[4], b[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) a[r] = b[r] = v[r];
+        dft8_ab<INV>(a, b, v);
+    } else if constexpr (R == 4) {
+        const float2 a = v[0], b = v[1], mb = mul_mi<INV>(v[1]);
+        v[0] = cadd(a, b);
+        v[1] = cadd(a, mb);
+        v[2] = csub(a, b);
+        v[3] = csub(a, mb);
+    } else {
+        v[1] = v[0];
+    }
 }
 
 // One Stockham stage of radix R over a line in shared memory. Thread `t` of the line's `tlc`
@@ -356,13 +398,28 @@ __device__ __forceinline__ void mix_last(float2* __restrict__ buf, const float2*
     }
 }
 
+// The first stage's butterfly j from in(y), y = j + r·M0: all R0 points, or with LO (the line's
+// points y ≥ N/2 are zero, R0 even) only the lower R0/2, and the transformed points left in v.
+template <int R0, int M0, bool INV, bool LO, class In>
+__device__ __forceinline__ void first_in(float2 (&v)[R0], int j, In& in) {
+    if constexpr (LO && R0 % 2 == 0) {
+#pragma unroll
+        for (int r = 0; r < R0 / 2; ++r) v[r] = in(j + r * M0);
+        dft_lo<R0, INV>(v);
+    } else {
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
+        dft<R0, INV>(v);
+    }
+}
+
 // The whole line with its ends in registers: the first stage's butterflies take their inputs
 // straight from in(y) (point y of the line, typically a global load) and the last stage hands
 // its outputs to out(y, v), so the line is staged into and out of shared memory by neither the
 // caller nor this function (two shared-memory passes fewer than run()). Every thread of the
 // block calls it; buf is this thread's line buffer (padded_len(N) points). On return the
 // buffer may still be read by other threads of the line: synchronise before reusing it.
-template <int N, int TL, bool INV, class In, class Out>
+template <int N, int TL, bool INV, bool LO = false, class In, class Out>
 __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
                                            In&& in, Out&& out) {
     using MX = Mix<N>;
@@ -374,9 +431,7 @@ __device__ __forceinline__ void mix_fft_io(float2* __restrict__ buf, const float
             const int j = t + b * TL;
             if (M0 % TL == 0 || j < M0) {
                 float2 v[R0];
-#pragma unroll
-                for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
-                dft<R0, INV>(v);
+                first_in<R0, M0, INV, LO>(v, j, in);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) buf[first_slot<R0>(j, r)] = v[r];
             }
@@ -410,7 +465,7 @@ __device__ __forceinline__ void mix_fft_regs(float2* __restrict__ buf, const flo
 
 // The whole line with its first stage fed from in(y) (as mix_fft_io) and the result left in buf
 // in natural order, the block synchronised, as run() leaves it.
-template <int N, int TL, bool INV, class In>
+template <int N, int TL, bool INV, bool LO = false, class In>
 __device__ __forceinline__ void mix_fft_in(float2* __restrict__ buf, const float2* __restrict__ tw, int t, bool act,
                                            In&& in) {
     constexpr int R0 = Mix<N>::radix(0), M0 = N / R0, BM0 = (M0 + TL - 1) / TL;
@@ -420,9 +475,7 @@ __device__ __forceinline__ void mix_fft_in(float2* __restrict__ buf, const float
             const int j = t + b * TL;
             if (M0 % TL == 0 || j < M0) {
                 float2 v[R0];
-#pragma unroll
-                for (int r = 0; r < R0; ++r) v[r] = in(j + r * M0);
-                dft<R0, INV>(v);
+                first_in<R0, M0, INV, LO>(v, j, in);
 #pragma unroll
                 for (int r = 0; r < R0; ++r) buf[first_slot<R0>(j, r)] = v[r];
             }
@@ -433,7 +486,8 @@ __device__ __forceinline__ void mix_fft_in(float2* __restrict__ buf, const float
 }
 
 // Line-FFT policies the map kernels are written against: n(), threads per line, run<INV>(),
-// run_io<INV>(buf, t, act, in, out) (mix_fft_io's contract) and run_in<INV>(buf, t, act, in).
+// run_io<INV, LO>(buf, t, act, in, out) (mix_fft_io's contract) and run_in<INV, LO>(buf, t, act,
+// in); LO: the caller guarantees in(y) = 0 for y ≥ n/2, so a compile-time line reads only y < n/2.
 struct GenericLine {
     LinePlan p;
     __host__ __device__ __forceinline__ int n() const { return p.n; }
@@ -442,8 +496,8 @@ struct GenericLine {
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
         line_fft<INV>(buf, p, act ? t : (1 << 30));
     }
-    // runtime lines stage through shared memory around the transform
-    template <bool INV, class In, class Out>
+    // runtime lines stage through shared memory around the transform (LO: no shortcut)
+    template <bool INV, bool LO = false, class In, class Out>
     __device__ __forceinline__ void run_io(float2* buf, int t, bool act, In&& in, Out&& out) const {
         const bool a = act && t < p.tl;
         if (a)
@@ -453,7 +507,7 @@ struct GenericLine {
         if (a)
             for (int y = t; y < p.n; y += p.tl) out(y, buf[pad_idx(y)]);
     }
-    template <bool INV, class In>
+    template <bool INV, bool LO = false, class In>
     __device__ __forceinline__ void run_in(float2* buf, int t, bool act, In&& in) const {
         const bool a = act && t < p.tl;
         if (a)
@@ -475,13 +529,13 @@ struct FixedLine {
     __device__ __forceinline__ void run(float2* buf, int t, bool act) const {
         mix_fft<N, TPL, INV>(buf, tw, t, act && t < TPL);
     }
-    template <bool INV, class In, class Out>
+    template <bool INV, bool LO = false, class In, class Out>
     __device__ __forceinline__ void run_io(float2* buf, int t, bool act, In&& in, Out&& out) const {
-        mix_fft_io<N, TPL, INV>(buf, tw, t, act && t < TPL, in, out);
+        mix_fft_io<N, TPL, INV, LO>(buf, tw, t, act && t < TPL, in, out);
     }
-    template <bool INV, class In>
+    template <bool INV, bool LO = false, class In>
     __device__ __forceinline__ void run_in(float2* buf, int t, bool act, In&& in) const {
-        mix_fft_in<N, TPL, INV>(buf, tw, t, act && t < TPL, in);
+        mix_fft_in<N, TPL, INV, LO>(buf, tw, t, act && t < TPL, in);
     }
 };
 

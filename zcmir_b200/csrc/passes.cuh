@@ -84,7 +84,8 @@ __device__ __forceinline__ float real_plane_row(int r, const float* row, int cw,
 // One block per grid row y < ch; lines = packed plane pairs (2z, 2z+1), lpb of them at a time.
 // The row's 5 stack values per cell are staged in shared memory once (after the line buffers).
 // Batched over blockIdx.y: item b reads grid + b·gbs and writes half + b·hbs.
-template <class F>
+// LO: cw ≤ nx/2, so the first butterflies read only the row's lower half.
+template <class F, bool LO>
 __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ grid, int cw, int ch, int WP,
                                                      CorrPlanDev plan, F f, int lpb, float2* __restrict__ half,
                                                      size_t pstride, size_t gbs, size_t hbs) {
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
         const int ra = act ? planes[2 * z] : 0;
         const int rb = act ? planes[2 * z + 1] : -1;
         // the first butterflies read the staged row directly (real planes ra + i·rb, zero past cw)
-        f.template run_in<false>(buf, t, act, [&](int x) {
+        f.template run_in<false, LO>(buf, t, act, [&](int x) {
             float2 v = make_float2(0.f, 0.f);
             if (x < cw) {
                 v.x = real_plane_row(ra, row, cw, x);
@@ -140,7 +141,8 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
 // ≥ rows_in read as zero. Thread (column c, line thread t), c fastest, so each load or store of
 // a warp covers 8 rows × 4 adjacent columns (whole 32-byte sectors); the first butterflies read
 // global memory and the last write it (run_io), with only the middle stages in shared memory.
-template <class F, bool INV>
+// LO: rows_in ≤ n/2, so the first butterflies read only rows y < n/2 (the rest are zero).
+template <class F, bool INV, bool LO>
 __global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size_t pstride, int WP, int ncols,
                                                  int rows_in, F f, int tx) {
     extern __shared__ float2 smem[];
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size
     const int c = threadIdx.x % tx, t = threadIdx.x / tx, col = x0 + c;
     const bool okc = col < ncols;
     float2* p = base + col;
-    f.template run_io<INV>(
+    f.template run_io<INV, LO>(
         smem + c * pl, t, true,
         [&](int y) { return (okc && y < rows_in) ? p[(size_t)y * WP] : make_float2(0.f, 0.f); },
         [&](int y, float2 v) {
@@ -493,16 +495,18 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
         // up to 256 threads of lines (one line of more for the longest rows: 8192 points, 512 threads)
         const int lines = std::min(lines_per_block(tl, 256), n_cplx);
         const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)5 * g.cw * sizeof(float);
-        cudaFuncSetAttribute(k_fwd_rows<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_fwd_rows<F><<<dim3(g.ch, a.batch), lines * tl, sm, st>>>(a.grid, g.cw, g.ch, g.WP, plan, f, lines, a.half,
+        auto k = 2 * g.cw <= g.nx ? k_fwd_rows<F, true> : k_fwd_rows<F, false>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<dim3(g.ch, a.batch), lines * tl, sm, st>>>(a.grid, g.cw, g.ch, g.WP, plan, f, lines, a.half,
                                                                    pstride, a.grid_stride, a.half_stride);
         return cudaGetLastError();
     } else if constexpr (P == Pass::FwdCols) {
         const int ncols = g.nx / 2 + 1;
         const int tx = col_tile(g.ny, tl, ncols);
         const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
-        cudaFuncSetAttribute(k_cols<F, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_cols<F, false><<<dim3((ncols + tx - 1) / tx, plan.n_real * a.batch), tx * tl, sm, st>>>(
+        auto k = 2 * g.ch <= g.ny ? k_cols<F, false, true> : k_cols<F, false, false>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<dim3((ncols + tx - 1) / tx, plan.n_real * a.batch), tx * tl, sm, st>>>(
             a.half, pstride, g.WP, ncols, g.ch, f, tx);
         return cudaGetLastError();
     } else if constexpr (P == Pass::InvCols) {
