@@ -87,6 +87,8 @@ Engine::~Engine() {
         s.stack.release();
         s.acf_dev.release();
         if (s.built_ev) cudaEventDestroy(s.built_ev);
+        if (s.acf_ev) cudaEventDestroy(s.acf_ev);
+        if (s.acf_host) cudaFreeHost(s.acf_host);
     }
     if (up_ev_) cudaEventDestroy(up_ev_);
     for (DevBuf* b : {&fs2_stats_, &fs2_hist_, &fs2_wt_, &fs2_acfpart_, &rank_tmp2_}) b->release();
@@ -102,6 +104,8 @@ Engine::~Engine() {
     for (auto& s : stack_) {
         for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack, &s.acf_dev}) b->release();
         if (s.built_ev) cudaEventDestroy(s.built_ev);
+        if (s.acf_ev) cudaEventDestroy(s.acf_ev);
+        if (s.acf_host) cudaFreeHost(s.acf_host);
     }
     stack_res_.release();
     for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_, &ffd_dev_, &ffd_out_,
@@ -273,12 +277,20 @@ bool Engine::build_side(int s) {
                  "features"))
         return false;
     counts[0] += 13;
+    // the autocorrelation sums go back to the host on the build's stream; finish_acf waits for
+    // that copy alone when they are next needed, so neither this call nor a map waits for a build
+    if (!sd.acf_host && !cuda_ok(cudaMallocHost(&sd.acf_host, 1156 * sizeof(double)), "features")) return false;
+    if (!sd.acf_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.acf_ev, cudaEventDisableTiming), "features")) return false;
+    if (!cuda_ok(cudaMemcpyAsync(sd.acf_host, sd.acf_dev.p, 1156 * sizeof(double), cudaMemcpyDeviceToHost, bs),
+                 "features") ||
+        !cuda_ok(cudaEventRecord(sd.acf_ev, bs), "features"))
+        return false;
+    counts[2]++;
     if (!sd.built_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.built_ev, cudaEventDisableTiming), "features")) return false;
     if (!cuda_ok(cudaEventRecord(sd.built_ev, bs), "features")) return false;
-    // the engine stream's later work (maps, scores) waits for a build on the side stream
-    if (own && !cuda_ok(cudaStreamWaitEvent(st, sd.built_ev, 0), "features")) return false;
-    // the autocorrelation is read back when next needed (finish_acf), so the host does not wait
-    // for the build here
+    // the engine stream's later work (maps, scores) waits for a build on the side stream when it
+    // first needs the side (join_side), so a map's passes over side 0 may start before it
+    sd.join_pending = own;
     sd.acf_pending = true;
     sd.built = true;
     sd.mode = mode;
@@ -286,7 +298,7 @@ bool Engine::build_side(int s) {
     return true;
 }
 
-bool Engine::need_images() {
+bool Engine::need_built(bool join) {
     if (!side[0].has || !side[1].has) return fail("NoImages");
     const std::string& fm = set.e("smi_features");
     const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
@@ -295,28 +307,30 @@ bool Engine::need_images() {
         if (!sd.built || sd.mode != mode || sd.half != set.b("half") || (sd.preprocess && sd.bake != bake_key()))
             if (!build_side(s)) return false;
     }
-    return finish_acf();
+    return !join || (join_side(0) && join_side(1));
 }
 
+bool Engine::join_side(int s) {
+    Side& sd = side[s];
+    if (!sd.join_pending) return true;
+    if (!cuda_ok(cudaStreamWaitEvent(st, sd.built_ev, 0), "features")) return false;
+    sd.join_pending = false;
+    return true;
+}
+
+bool Engine::need_images() { return need_built() && finish_acf(); }
+
 bool Engine::finish_acf() {
-    double raw[2][1156];
-    bool any = false;
-    for (int s = 0; s < 2; ++s)
-        if (side[s].acf_pending) {
-            if (!cuda_ok(cudaMemcpyAsync(raw[s], side[s].acf_dev.p, sizeof raw[s], cudaMemcpyDeviceToHost, st), "features"))
-                return false;
-            any = true;
-        }
-    if (!any) return true;
-    if (!cuda_ok(cudaStreamSynchronize(st), "features")) return false;
-    counts[2] += 1;
-    counts[3] += 1;
-    for (int s = 0; s < 2; ++s)
-        if (side[s].acf_pending) {
-            // normalise by the zero lag (smi.wgsl:1572-1578)
-            for (int k = 0; k < 1156; ++k) side[s].acf[k] = raw[s][k] / std::max(raw[s][144 * 4 + (k & 3)], 1e-12);
-            side[s].acf_pending = false;
-        }
+    for (int s = 0; s < 2; ++s) {
+        Side& sd = side[s];
+        if (!sd.acf_pending) continue;
+        if (!cuda_ok(cudaEventSynchronize(sd.acf_ev), "features")) return false;
+        counts[3]++;
+        // normalise by the zero lag (smi.wgsl:1572-1578)
+        const double* raw = sd.acf_host;
+        for (int k = 0; k < 1156; ++k) sd.acf[k] = raw[k] / std::max(raw[144 * 4 + (k & 3)], 1e-12);
+        sd.acf_pending = false;
+    }
     return true;
 }
 
@@ -348,7 +362,7 @@ bool Engine::features(int s, float* out, size_t len) {
 bool Engine::work_image(int s, float* out, size_t len) {
     if (s < 0 || s > 1 || !side[s].has) return fail("work_image: NoImage");
     Side& sd = side[s];
-    if (!sd.built && !build_side(s)) return false;
+    if ((!sd.built && !build_side(s)) || !join_side(s)) return false;
     const size_t n = (size_t)sd.w * sd.h;
     if (len < n) return fail("work_image: BufferTooSmall");
     if (!cuda_ok(cudaMemcpyAsync(out, sd.work.p, n * 4, cudaMemcpyDeviceToHost, st), "work_image")) return false;
@@ -420,7 +434,10 @@ bool Engine::line_plan(int n, LinePlan& p) {
 // ── shift map ─────────────────────────────────────────────────────────────────────────────────
 
 bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap, double min_overlap, MapJob& job) {
-    if (!need_images()) return false;
+    // the features only enqueued, side 1's build not yet joined: run_map queues side 0's passes
+    // first and joins side 1 before its own; the correlation area the calibrated score needs is
+    // read when the row pass is launched, so the host does not wait for the builds here
+    if (!need_built(false)) return false;
     if (!metric_ok("shift_map")) return false;
     const bool ladder = set.e("fft_sizes") == "ladder";
     if (!ladder) return fail("shift_map: fft_sizes=\"compact\" is not supported by this build (use \"ladder\")");
@@ -461,7 +478,8 @@ bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap,
     cp.calib = job.calibrated ? 1 : 0;
     cp.nf = three ? 3 : 4;
     cp.min_n = (float)std::max(12u, floor_n);
-    cp.area = std::max(1.0, pair_area() * (1.0 / (gcell * gcell)));
+    cp.area = 0.0;  // set by run_map
+    job.gcell = gcell;
     cp.ridge = 1e-4;
     cp.inv_nn = 1.0 / ((double)g.nx * (double)g.ny);
     return true;
@@ -491,36 +509,58 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
     unsigned long long* best = reinterpret_cast<unsigned long long*>(res);
     float* zero = reinterpret_cast<float*>(res + 8);
     double* n00 = reinterpret_cast<double*>(res + 16);
-    rec(0);
-    if (!cuda_ok(warp_stack(A.stack.as<float>(), A.w, A.h, hif, okdet, g.W, g.Hh, canvas_a_.as<float>(), st), "canvas") ||
-        !cuda_ok(paste_stack(B.stack.as<float>(), B.w, B.h, g.ox, g.oy, g.W, g.Hh, canvas_b_.as<float>(), st), "canvas"))
-        return false;
-    const float* ga = canvas_a_.as<float>();
-    const float* gb = canvas_b_.as<float>();
-    if (!job.identity_grid) {
-        if (!cuda_ok(resample_grid(ga, g.W, g.Hh, g.cw, g.ch, grid_a_.as<float>(), st), "resample") ||
-            !cuda_ok(resample_grid(gb, g.W, g.Hh, g.cw, g.ch, grid_b_.as<float>(), st), "resample"))
+    // a side's canvas (moving warped, fixed pasted) and, when cells exceed a pixel, its grid
+    auto canvas_side = [&](int s, const float*& grid) {
+        float* canvas = (s == 0 ? canvas_a_ : canvas_b_).as<float>();
+        const cudaError_t e = s == 0 ? warp_stack(A.stack.as<float>(), A.w, A.h, hif, okdet, g.W, g.Hh, canvas, st)
+                                     : paste_stack(B.stack.as<float>(), B.w, B.h, g.ox, g.oy, g.W, g.Hh, canvas, st);
+        if (!cuda_ok(e, "canvas")) return false;
+        grid = canvas;
+        if (!job.identity_grid) {
+            float* gd = (s == 0 ? grid_a_ : grid_b_).as<float>();
+            if (!cuda_ok(resample_grid(canvas, g.W, g.Hh, g.cw, g.ch, gd, st), "resample")) return false;
+            grid = gd;
+        }
+        return true;
+    };
+    auto lag0 = [&](const float* ga, const float* gb) {
+        return cuda_ok(lag0_count(ga, gb, g.cw, g.ch, n00, st), "lag0") &&
+               cuda_ok(cudaMemsetAsync(best, 0, 8, st), "shift_map");
+    };
+    auto rows_of = [&](int s, const float* grid) {
+        return cuda_ok(forward_rows(grid, g, job.plan, job.row, (s == 0 ? half_a_ : half_b_).as<float2>(), st),
+                       "forward rows");
+    };
+    auto cols_of = [&](int s) {
+        return cuda_ok(forward_cols((s == 0 ? half_a_ : half_b_).as<float2>(), g, job.plan, job.col, st),
+                       "forward columns");
+    };
+    const float *ga = nullptr, *gb = nullptr;
+    if (!join_side(0)) return false;
+    if (ev) {
+        // in stage order, so each stage's events bracket its own passes
+        if (!join_side(1)) return false;
+        rec(0);
+        if (!canvas_side(0, ga) || !canvas_side(1, gb) || !lag0(ga, gb)) return false;
+        rec(1);
+        if (!rows_of(0, ga) || !rows_of(1, gb)) return false;
+        rec(2);
+        if (!cols_of(0) || !cols_of(1)) return false;
+        rec(3);
+    } else {
+        // side 0's passes first: they need only its own build, so they run while side 1's build
+        // (on a stream of its own) may still be going; then the wait for it and side 1's passes
+        if (!canvas_side(0, ga) || !rows_of(0, ga) || !cols_of(0) || !join_side(1) || !canvas_side(1, gb) ||
+            !lag0(ga, gb) || !rows_of(1, gb) || !cols_of(1))
             return false;
-        ga = grid_a_.as<float>();
-        gb = grid_b_.as<float>();
     }
-    if (!cuda_ok(lag0_count(ga, gb, g.cw, g.ch, n00, st), "lag0") ||
-        !cuda_ok(cudaMemsetAsync(best, 0, 8, st), "shift_map"))
-        return false;
-    rec(1);
-    // the two sides' forward transforms: rows of both, then columns of both
-    if (!cuda_ok(forward_rows(ga, g, job.plan, job.row, half_a_.as<float2>(), st), "forward rows") ||
-        !cuda_ok(forward_rows(gb, g, job.plan, job.row, half_b_.as<float2>(), st), "forward rows"))
-        return false;
-    rec(2);
-    if (!cuda_ok(forward_cols(half_a_.as<float2>(), g, job.plan, job.col, st), "forward columns") ||
-        !cuda_ok(forward_cols(half_b_.as<float2>(), g, job.plan, job.col, st), "forward columns"))
-        return false;
-    rec(3);
     if (!cuda_ok(inverse_columns(half_a_.as<float2>(), half_b_.as<float2>(), g, job.plan, job.col, q_.as<float2>(), st),
                  "inverse columns"))
         return false;
     rec(4);
+    // the correlation area (from both sides' autocorrelations) enters the row pass's score
+    if (!finish_acf()) return false;
+    job.cp.area = std::max(1.0, pair_area() * (1.0 / (job.gcell * job.gcell)));
     const bool tmem = row_pass != "split" && rows_tmem_supported(g.nx, job.plan.n_corr);
     if (tmem && host_map) {
         // the map's rows in chunks of whole waves (one block per SM per row), each chunk copied to

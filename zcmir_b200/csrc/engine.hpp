@@ -41,9 +41,12 @@ struct Side {
     DevBuf mag;    // Sobel magnitude of the rank
     DevBuf stack;  // [1, f0..f3]
     std::array<double, 1156> acf{};  // normalised autocorrelation, 289 lags × 4 planes
-    DevBuf acf_dev;                  // its raw sums on the device, read back when next needed
-    bool acf_pending = false;        // acf_dev holds sums that acf does not yet
+    DevBuf acf_dev;                  // its raw sums on the device
+    double* acf_host = nullptr;      // pinned copy of those sums, made on the build's stream
+    cudaEvent_t acf_ev = nullptr;    // recorded after that copy
+    bool acf_pending = false;        // acf_host holds (or will hold) sums that acf does not yet
     cudaEvent_t built_ev = nullptr;  // recorded after the last build, which read `raw`
+    bool join_pending = false;       // built on a stream of its own; the engine stream has not yet waited
     bool built = false;
     int mode = -1;
     bool half = false;
@@ -67,7 +70,8 @@ struct MapJob {
     CorrPlanDev plan;
     LinePlan row, col, line;
     int S;
-    CombineParams cp;
+    CombineParams cp;  // cp.area set when the row pass is launched
+    double gcell = 1.0;  // canvas pixels per grid cell
     bool identity_grid;
     bool exact, calibrated;
 };
@@ -160,7 +164,13 @@ class Engine {
     // RGBA8 → gray (0.299 R + 0.587 G + 0.114 B), always preprocessed (src/engine.zig:422-426)
     bool set_image_rgba(int s, const unsigned char* rgba, int w, int h);
     bool need_images();
-    // the sides' autocorrelations read back from the device (one wait for both), normalised
+    // both sides present and their features built (enqueued) for the current settings; with
+    // join, the engine stream also waits for the builds made on a stream of their own
+    bool need_built(bool join = true);
+    // the engine stream waits for side s's build, if it ran on a stream of its own
+    bool join_side(int s);
+    // the sides' autocorrelations as their builds copied them back (a wait on each pending
+    // side's copy only), normalised
     bool finish_acf();
     bool features(int s, float* out, size_t len);
     bool work_image(int s, float* out, size_t len);
