@@ -83,6 +83,7 @@ Engine::~Engine() {
         s.raw.release();
         s.work.release();
         s.feat.release();
+        s.feat4.release();
         s.mag.release();
         s.stack.release();
         s.acf_dev.release();
@@ -102,7 +103,7 @@ Engine::~Engine() {
                       &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
     for (auto& s : stack_) {
-        for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.mag, &s.stack, &s.acf_dev}) b->release();
+        for (DevBuf* b : {&s.raw, &s.work, &s.feat, &s.feat4, &s.mag, &s.stack, &s.acf_dev}) b->release();
         if (s.built_ev) cudaEventDestroy(s.built_ev);
         if (s.acf_ev) cudaEventDestroy(s.acf_ev);
         if (s.acf_host) cudaFreeHost(s.acf_host);
@@ -259,6 +260,7 @@ bool Engine::build_side(int s) {
     const bool half = set.b("half");
     const int ntiles = ((sd.w + 31) / 32) * ((sd.h + 31) / 32);
     bool ok = cuda_ok(sd.work.ensure(n * 4), "features") && cuda_ok(sd.feat.ensure(n * 16), "features") &&
+              cuda_ok(sd.feat4.ensure(n * 16), "features") &&
               cuda_ok(sd.mag.ensure(n * 4), "features") && cuda_ok(sd.stack.ensure(n * 20), "features") &&
               cuda_ok(rtmp.ensure(n * 4), "features") && cuda_ok(stats.ensure(22 * 8), "features") &&
               cuda_ok(hist.ensure(256 * 4), "features") && cuda_ok(wt.ensure(20 * 4), "features") &&
@@ -274,9 +276,10 @@ bool Engine::build_side(int s) {
     if (!bake(s, bs)) return false;
     if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rtmp.as<float>(), sd.feat.as<float>(),
                                 sd.mag.as<float>(), sd.stack.as<float>(), fsc, bs),
-                 "features"))
+                 "features") ||
+        !cuda_ok(interleave_features(sd.feat.as<float>(), (int)n, sd.feat4.as<float4>(), bs), "features"))
         return false;
-    counts[0] += 13;
+    counts[0] += 14;
     // the autocorrelation sums go back to the host on the build's stream; finish_acf waits for
     // that copy alone when they are next needed, so neither this call nor a map waits for a build
     if (!sd.acf_host && !cuda_ok(cudaMallocHost(&sd.acf_host, 1156 * sizeof(double)), "features")) return false;

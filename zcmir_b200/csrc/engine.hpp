@@ -38,6 +38,7 @@ struct Side {
     DevBuf raw;    // the image as uploaded (f32 gray)
     DevBuf work;   // the work image the features are built from (f16-quantised when half)
     DevBuf feat;   // 4 whitened planes, plane-major
+    DevBuf feat4;  // the same, interleaved: one float4 per pixel (the pose kernels' bilinear taps)
     DevBuf mag;    // Sobel magnitude of the rank
     DevBuf stack;  // [1, f0..f3]
     std::array<double, 1156> acf{};  // normalised autocorrelation, 289 lags × 4 planes

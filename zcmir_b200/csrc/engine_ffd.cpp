@@ -99,7 +99,8 @@ bool Engine::ffd_gradient(const Mat3& H, double* score, double* grad, size_t len
     float hinv[18];
     for (int k = 0; k < 9; ++k) hinv[k] = (float)Hi[k], hinv[9 + k] = (float)Hii[k];
     const Side &A = side[0], &B = side[1];
-    const PoseSide pa{A.feat.as<float>(), A.w, A.h}, pb{B.feat.as<float>(), B.w, B.h};
+    const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
+        pb{B.feat.as<float>(), B.feat4.as<float4>(), B.w, B.h};
     const bool src = set.b("ffd_source");
     const PoseFfd ff{ffd_dev_.as<float>(), (int)g, src ? 1 : 0};
     const PoseFfd fi{ffd_dev_.as<float>() + 2 * kFfdMax * kFfdMax, (int)g, src ? 0 : 1};
@@ -347,7 +348,8 @@ bool Engine::spline_stage(const Mat3& H, double& lam, bool& moved, double& score
     PoseFfd ff, fi;
     if (!ffd_pose_dirs(cur_cps.data(), 1, ff, fi)) return false;
     const Side &A = side[0], &B = side[1];
-    const PoseSide pa{A.feat.as<float>(), A.w, A.h}, pb{B.feat.as<float>(), B.w, B.h};
+    const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
+        pb{B.feat.as<float>(), B.feat4.as<float4>(), B.w, B.h};
     const Mat3 Hi = inv3(H), Hii = inv3(Hi);
     float mats[36];  // per direction: hinv, pose
     for (int k = 0; k < 9; ++k) {

@@ -84,7 +84,8 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
     if (!cuda_ok(cudaMemcpyAsync(dh, pose_host_.data(), m * 9 * 4, cudaMemcpyHostToDevice, st), "score") ||
         !cuda_ok(cudaMemcpyAsync(dg, gens, 2 * 72 * 4, cudaMemcpyHostToDevice, st), "score"))
         return false;
-    const PoseSide pa{A.feat.as<float>(), A.w, A.h}, pb{B.feat.as<float>(), B.w, B.h};
+    const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
+        pb{B.feat.as<float>(), B.feat4.as<float4>(), B.w, B.h};
     double* sums = pose_sums_.as<double>();
     double* tsum = pose_tsum_.as<double>();
     float* coef = pose_coef_.as<float>();

@@ -151,9 +151,12 @@ cudaError_t ncc_grid(const float* ca, const float* cb, int W, int Hh, int cw, in
 
 // ── pose scores and gradients (pose.cu) ──
 struct PoseSide {
-    const float* feat;  // 4 whitened planes, plane-major
+    const float* feat;    // 4 whitened planes, plane-major
+    const float4* feat4;  // the same planes interleaved, one float4 per pixel
     int w, h;
 };
+// the 4 plane-major feature planes of n pixels interleaved into one float4 per pixel
+cudaError_t interleave_features(const float* feat, int n, float4* out, cudaStream_t st);
 // A cubic B-spline on top of the pose: g × g control points (x, y per point, in half-image units
 // of the lattice's image), on b (the destination: it moves b's pixel before H⁻¹) or, source, on a
 // (it moves the sample after H⁻¹). cps null: no spline.

@@ -53,6 +53,15 @@ __device__ __forceinline__ float4 cubic_w(float t) {
 }
 __device__ __forceinline__ float comp4(const float4& v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
 
+// The 2×2 taps at i00, i00 + 1, i00 + aw, i00 + aw + 1 of an image whose four feature planes are
+// interleaved (one float4 per pixel): one 16-byte load per tap instead of one per plane and tap.
+struct Taps4 {
+    float4 v00, v10, v01, v11;
+};
+__device__ __forceinline__ Taps4 taps4(const float4* __restrict__ a, size_t i00, int aw) {
+    return {__ldg(&a[i00]), __ldg(&a[i00 + 1]), __ldg(&a[i00 + aw]), __ldg(&a[i00 + aw + 1])};
+}
+
 // A block's view of a spline: its control points staged in shared memory (c null: none).
 struct FfdView {
     const float* c;
@@ -94,6 +103,40 @@ __device__ __forceinline__ float2 ffd_disp(const FfdView& f, float xf, float yf,
     return make_float2(dx, dy);
 }
 
+// A grid-stride walk over a w × h image in tiles of 8 × 4 pixels, one tile per warp and step
+// (lane → (lane mod 8, lane / 8)): a warp's 32 pixels are a compact patch, so the bilinear taps
+// they gather on the other image under any rotation fall on few rows (few sectors per load).
+// Tile coordinates are stepped along, not divided out per tile.
+struct TileWalk {
+    int T, nt, step, tx, ty, sx, sy, ntx, lx, ly, w, h;
+    __device__ __forceinline__ TileWalk(int w_, int h_) : w(w_), h(h_) {
+        ntx = (w + 7) >> 3;
+        nt = ntx * ((h + 3) >> 2);
+        const int lane = threadIdx.x & 31;
+        lx = lane & 7;
+        ly = lane >> 3;
+        T = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+        step = (int)((gridDim.x * blockDim.x) >> 5);
+        ty = T / ntx;
+        tx = T - ty * ntx;
+        sy = step / ntx;
+        sx = step - sy * ntx;
+    }
+    __device__ __forceinline__ bool ok() const { return T < nt; }
+    __device__ __forceinline__ void next() {
+        T += step;
+        tx += sx;
+        ty += sy;
+        if (tx >= ntx) {
+            tx -= ntx;
+            ++ty;
+        }
+    }
+    __device__ __forceinline__ int x() const { return (tx << 3) + lx; }
+    __device__ __forceinline__ int y() const { return (ty << 2) + ly; }
+    __device__ __forceinline__ bool in() const { return x() < w && y() < h; }
+};
+
 // pose sample position of b pixel (x, y) (smi.wgsl overlap_moments 1003-1016): with a spline on
 // b the pixel moves first, X = (x + 1 + dx, y + 1 + dy); on a the sample H⁻¹X − 1 moves after.
 // ph = H⁻¹X, (Xx, Xy) = X. False when outside a's valid interior.
@@ -111,8 +154,13 @@ __device__ __forceinline__ bool sample_pos(const float* Hi, const FfdView& f, in
     ph.y = Hi[3] * Xx + Hi[4] * Xy + Hi[5];
     ph.z = Hi[6] * Xx + Hi[7] * Xy + Hi[8];
     if (fabsf(ph.z) < 1e-8f) return false;
-    fx = ph.x / ph.z - 1.f;
-    fy = ph.y / ph.z - 1.f;
+    if (ph.z == 1.f) {  // affine poses: the division is exact, skip it
+        fx = ph.x - 1.f;
+        fy = ph.y - 1.f;
+    } else {
+        fx = ph.x / ph.z - 1.f;
+        fy = ph.y / ph.z - 1.f;
+    }
     if (FFD && f.source) {
         const float2 d = ffd_disp(f, fx, fy, (float)aw, (float)ah);
         fx = fx + d.x;
@@ -124,8 +172,8 @@ __device__ __forceinline__ bool sample_pos(const float* Hi, const FfdView& f, in
 // The 45 sums: 0 Σw, 1–4 Σw a, 5–8 Σw b, 9–24 Σw a_i b_j, 25–34 / 35–44 upper triangles of
 // Σw a aᵀ and Σw b bᵀ.
 template <bool FFD>
-__global__ void __launch_bounds__(256) k_pose_moments(const float* __restrict__ fa, int aw, int ah,
-                                                      const float* __restrict__ fb, int bw, int bh,
+__global__ void __launch_bounds__(256) k_pose_moments(const float4* __restrict__ fa, int aw, int ah,
+                                                      const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, double* __restrict__ sums,
                                                       PoseFfd ffd) {
     __shared__ float Hs[9];
@@ -141,9 +189,10 @@ __global__ void __launch_bounds__(256) k_pose_moments(const float* __restrict__ 
     float acc[kMom];
 #pragma unroll
     for (int k = 0; k < kMom; ++k) acc[k] = 0.f;
-    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
-        const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
+    for (TileWalk pw(bw, bh); pw.ok(); pw.next()) {
+        if (!pw.in()) continue;
+        const int y = pw.y(), x = pw.x();
+        const size_t t = (size_t)y * bw + x;
         float fx, fy, Xx, Xy;
         float3 ph;
         if (!sample_pos<FFD>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, Xx, Xy)) continue;
@@ -154,13 +203,14 @@ __global__ void __launch_bounds__(256) k_pose_moments(const float* __restrict__ 
         const float ax = fx - flx, ay = fy - fly;
         const size_t i00 = (size_t)fly * aw + (size_t)flx;
         float va[4], vb[4];
+        const Taps4 tp = taps4(fa, i00, aw);
+        const float4 b4 = __ldg(&fb[t]);
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            const float* P = fa + p * na;
-            const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
-            const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+            const float v00 = comp4(tp.v00, p), v10 = comp4(tp.v10, p);
+            const float v01 = comp4(tp.v01, p), v11 = comp4(tp.v11, p);
             va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
-            vb[p] = __ldg(&fb[p * nb + t]);
+            vb[p] = comp4(b4, p);
         }
         acc[0] += wt;
 #pragma unroll
@@ -341,8 +391,8 @@ __global__ void k_pose_coefs(const double* __restrict__ sums, int n, int exact, 
 // needs the two scalars cx, cy = (∂S/∂v_a)·∇v_a plus the taper's boundary term, times each
 // tangent's flow ∂(sample)/∂ξ_k = ((M_k X)·ph.z − ph·(M_k X).z)/ph.z², M_k = −H⁻¹ G_k.
 template <bool FFD>
-__global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ fa, int aw, int ah,
-                                                      const float* __restrict__ fb, int bw, int bh,
+__global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__ fa, int aw, int ah,
+                                                      const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, const float* __restrict__ coef,
                                                       const float* __restrict__ gens, int hess, double* __restrict__ out,
                                                       PoseFfd ffd) {
@@ -367,9 +417,10 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
     float h36[36];
 #pragma unroll
     for (int k = 0; k < 36; ++k) h36[k] = 0.f;
-    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
-        const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
+    for (TileWalk pw(bw, bh); pw.ok(); pw.next()) {
+        if (!pw.in()) continue;
+        const int y = pw.y(), x = pw.x();
+        const size_t t = (size_t)y * bw + x;
         float fx, fy, X, Y;
         float3 ph;
         if (!sample_pos<FFD>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, X, Y)) continue;
@@ -379,15 +430,16 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
         const float ax = fx - flx, ay = fy - fly;
         const size_t i00 = (size_t)fly * aw + (size_t)flx;
         float va[4], gx[4], gy[4], vb[4];
+        const Taps4 tp = taps4(fa, i00, aw);
+        const float4 b4 = __ldg(&fb[t]);
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            const float* P = fa + p * na;
-            const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
-            const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+            const float v00 = comp4(tp.v00, p), v10 = comp4(tp.v10, p);
+            const float v01 = comp4(tp.v01, p), v11 = comp4(tp.v11, p);
             va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
             gx[p] = (v10 - v00) * (1.f - ay) + (v11 - v01) * ay;
             gy[p] = (v01 - v00) * (1.f - ax) + (v11 - v10) * ax;
-            vb[p] = __ldg(&fb[p * nb + t]);
+            vb[p] = comp4(b4, p);
         }
         // ∂S/∂v_a = 2 (W (v_b − μ_B) − M̂ (v_a − μ_A))
         float ra[4];
@@ -487,8 +539,8 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float* __restrict__ 
 // motion under a unit x or y displacement of one control point (through H⁻¹ on a b lattice,
 // directly on an a lattice), per unit basis weight — then each control point of the chunk takes
 // its basis weight B_i(u) B_j(v) (clamped lattice indices summed) times them.
-__global__ void __launch_bounds__(256) k_pose_ffd_grad(const float* __restrict__ fa, int aw, int ah,
-                                                       const float* __restrict__ fb, int bw, int bh,
+__global__ void __launch_bounds__(256) k_pose_ffd_grad(const float4* __restrict__ fa, int aw, int ah,
+                                                       const float4* __restrict__ fb, int bw, int bh,
                                                        const float* __restrict__ hinv, const float* __restrict__ coef,
                                                        PoseFfd ffd, int cp0, double* __restrict__ out) {
     __shared__ float Hs[9], cf[kCoef];
@@ -509,9 +561,10 @@ __global__ void __launch_bounds__(256) k_pose_ffd_grad(const float* __restrict__
     float acc[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) acc[k] = 0.f;
-    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += (size_t)gridDim.x * blockDim.x) {
-        const int y = (int)(t / bw), x = (int)(t - (size_t)y * bw);
+    for (TileWalk pw(bw, bh); pw.ok(); pw.next()) {
+        if (!pw.in()) continue;
+        const int y = pw.y(), x = pw.x();
+        const size_t t = (size_t)y * bw + x;
         float fx, fy, X, Y;
         float3 ph;
         if (!sample_pos<true>(Hi, fv, x, y, aw, ah, bw, bh, fx, fy, ph, X, Y)) continue;
@@ -521,15 +574,16 @@ __global__ void __launch_bounds__(256) k_pose_ffd_grad(const float* __restrict__
         const float ax = fx - flx, ay = fy - fly;
         const size_t i00 = (size_t)fly * aw + (size_t)flx;
         float va[4], gx[4], gy[4], vb[4];
+        const Taps4 tp = taps4(fa, i00, aw);
+        const float4 b4 = __ldg(&fb[t]);
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
-            const float* P = fa + p * na;
-            const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
-            const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+            const float v00 = comp4(tp.v00, p), v10 = comp4(tp.v10, p);
+            const float v01 = comp4(tp.v01, p), v11 = comp4(tp.v11, p);
             va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
             gx[p] = (v10 - v00) * (1.f - ay) + (v11 - v01) * ay;
             gy[p] = (v01 - v00) * (1.f - ax) + (v11 - v10) * ax;
-            vb[p] = __ldg(&fb[p * nb + t]);
+            vb[p] = comp4(b4, p);
         }
         float dga = 0.f, dgb = 0.f;
 #pragma unroll
@@ -618,8 +672,8 @@ constexpr int kFcTasks = 116;
 __device__ __forceinline__ int tri_i(int k) { return k < 4 ? 0 : k < 7 ? 1 : k < 9 ? 2 : 3; }
 __device__ __forceinline__ int tri_j(int k) { return k < 4 ? k : k < 7 ? k - 3 : k < 9 ? k - 5 : 3; }
 
-__global__ void __launch_bounds__(256) k_pose_ffd_cells(const float* __restrict__ fa, int aw, int ah,
-                                                        const float* __restrict__ fb, int bw, int bh,
+__global__ void __launch_bounds__(256) k_pose_ffd_cells(const float4* __restrict__ fa, int aw, int ah,
+                                                        const float4* __restrict__ fb, int bw, int bh,
                                                         const float* __restrict__ hinv, const float* __restrict__ hpose,
                                                         const float* __restrict__ coef, PoseFfd ffd, int nch,
                                                         float* __restrict__ out) {
@@ -679,7 +733,6 @@ __global__ void __launch_bounds__(256) k_pose_ffd_cells(const float* __restrict_
         bi = (task - 100) % 4, bj = (task - 100) / 4;
     }
     float3 acc = make_float3(0.f, 0.f, 0.f);
-    const size_t na = (size_t)aw * ah, nb = (size_t)bw * bh;
     const int ntile = (total + 255) / 256;
     for (int tile = chunk * ntile / nch; tile < (chunk + 1) * ntile / nch; ++tile) {
         const int base = tile * 256, pidx = base + threadIdx.x;
@@ -714,15 +767,16 @@ __global__ void __launch_bounds__(256) k_pose_ffd_cells(const float* __restrict_
                 const float ax = fx - flx, ay = fy - fly;
                 const size_t i00 = (size_t)fly * aw + (size_t)flx;
                 float va[4], gx[4], gy[4], vb[4];
+                const Taps4 tp = taps4(fa, i00, aw);
+                const float4 b4 = __ldg(&fb[t]);
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
-                    const float* P = fa + p * na;
-                    const float v00 = __ldg(&P[i00]), v10 = __ldg(&P[i00 + 1]);
-                    const float v01 = __ldg(&P[i00 + aw]), v11 = __ldg(&P[i00 + aw + 1]);
+                    const float v00 = comp4(tp.v00, p), v10 = comp4(tp.v10, p);
+                    const float v01 = comp4(tp.v01, p), v11 = comp4(tp.v11, p);
                     va[p] = (v00 * (1.f - ax) + v10 * ax) * (1.f - ay) + (v01 * (1.f - ax) + v11 * ax) * ay;
                     gx[p] = (v10 - v00) * (1.f - ay) + (v11 - v01) * ay;
                     gy[p] = (v01 - v00) * (1.f - ax) + (v11 - v10) * ax;
-                    vb[p] = __ldg(&fb[p * nb + t]);
+                    vb[p] = comp4(b4, p);
                 }
                 float rx = 0.f, ry = 0.f;
 #pragma unroll
@@ -835,22 +889,35 @@ int pose_blocks(size_t pixels, int n) {
 
 }  // namespace
 
+namespace {
+__global__ void k_feat_interleave(const float* __restrict__ feat, int n, float4* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = make_float4(feat[i], feat[(size_t)n + i], feat[2 * (size_t)n + i], feat[3 * (size_t)n + i]);
+}
+}  // namespace
+
+cudaError_t interleave_features(const float* feat, int n, float4* out, cudaStream_t st) {
+    const int blocks = std::min((n + 255) / 256, 148 * 8);
+    k_feat_interleave<<<std::max(blocks, 1), 256, 0, st>>>(feat, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
                          const PoseFfd& ffd) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(sums, 0, (size_t)n * kMom * sizeof(double), st);
     dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
     if (ffd.cps)
-        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, sums, ffd);
+        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd);
     else
-        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, sums, ffd);
+        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd);
     return cudaGetLastError();
 }
 
 cudaError_t pose_ffd_cells(const PoseSide& a, const PoseSide& b, const float* hinv, const float* hpose,
                            const float* coef, const PoseFfd& ffd, int nch, float* out, cudaStream_t st) {
     if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax || nch < 1) return cudaErrorInvalidValue;
-    k_pose_ffd_cells<<<ffd.g * ffd.g * nch, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, hpose, coef, ffd,
+    k_pose_ffd_cells<<<ffd.g * ffd.g * nch, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, hpose, coef, ffd,
                                                           nch, out);
     return cudaGetLastError();
 }
@@ -859,7 +926,7 @@ cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hin
                           const PoseFfd& ffd, int cp0, double* out, cudaStream_t st) {
     if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, 32 * sizeof(double), st);
-    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, 1), 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef,
+    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, 1), 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef,
                                                                        ffd, cp0, out);
     return cudaGetLastError();
 }
@@ -875,9 +942,9 @@ cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv
     cudaMemsetAsync(out, 0, (size_t)n * kGrad * sizeof(double), st);
     dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
     if (ffd.cps)
-        k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
+        k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
     else
-        k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat, a.w, a.h, b.feat, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
+        k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
     return cudaGetLastError();
 }
 

@@ -119,7 +119,8 @@ bool Engine::score_static(const double* Hs, int n, double* out3) {
     }
     if (!cuda_ok(cudaMemcpyAsync(hinv, hh, (size_t)m * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "score_static"))
         return false;
-    const PoseSide pa{side[0].feat.as<float>(), side[0].w, side[0].h}, pb{side[1].feat.as<float>(), side[1].w, side[1].h};
+    const PoseSide pa{side[0].feat.as<float>(), side[0].feat4.as<float4>(), side[0].w, side[0].h},
+        pb{side[1].feat.as<float>(), side[1].feat4.as<float4>(), side[1].w, side[1].h};
     // The moment sums accumulate with atomics and are the only part of the array that must
     // start at zero: pose_moments clears its n × 45 sums on the stream before accumulating. The
     // inverse poses, coefficients and scores are written in full before they are read.
