@@ -880,11 +880,26 @@ __global__ void __launch_bounds__(256) k_pose_ffd_cells(const float4* __restrict
     }
 }
 
-int pose_blocks(size_t pixels, int n) {
-    const size_t by_work = (pixels + 256 * 16 - 1) / (256 * 16);  // ≥ 16 pixels per thread
-    const size_t by_fill = (1184 + (size_t)n - 1) / (size_t)n;
-    size_t b = std::min(by_work, std::max<size_t>(by_fill, 1));
+// Blocks per pose over `pixels` fixed pixels, with `slots` blocks resident on the GPU at once:
+// about 16 pixels per thread, rounded so that whole poses fill whole waves (slots / b poses per
+// wave, or b a whole number of waves) — a wave and a few blocks would take two waves' time. The
+// count depends on the image alone, never on how many poses share the launch, so a pose's sums
+// (and score) are the same whatever batch it is scored in.
+int pose_blocks(size_t pixels, int slots) {
+    const size_t by_work = std::max<size_t>(1, (pixels + 256 * 16 - 1) / (256 * 16));
+    const size_t sl = (size_t)std::max(slots, 1);
+    const size_t b = by_work >= sl ? sl * (by_work / sl) : sl / ((sl + by_work - 1) / by_work);
     return (int)std::max<size_t>(1, std::min<size_t>(b, 4096));
+}
+
+// resident blocks of 256 threads of kernel k across the GPU
+template <class K>
+int pose_slots(K k) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, 0) != cudaSuccess || per < 1) per = 1;
+    return per * sms;
 }
 
 }  // namespace
@@ -906,7 +921,8 @@ cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv
                          const PoseFfd& ffd) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(sums, 0, (size_t)n * kMom * sizeof(double), st);
-    dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
+    static const int sl_s = pose_slots(k_pose_moments<true>), sl_p = pose_slots(k_pose_moments<false>);
+    dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
         k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd);
     else
@@ -926,7 +942,8 @@ cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hin
                           const PoseFfd& ffd, int cp0, double* out, cudaStream_t st) {
     if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, 32 * sizeof(double), st);
-    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, 1), 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef,
+    static const int sl = pose_slots(k_pose_ffd_grad);
+    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, sl), 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef,
                                                                        ffd, cp0, out);
     return cudaGetLastError();
 }
@@ -940,7 +957,8 @@ cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv
                          int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, (size_t)n * kGrad * sizeof(double), st);
-    dim3 g(pose_blocks((size_t)b.w * b.h, n), n);
+    static const int sl_s = pose_slots(k_pose_tangent<true>), sl_p = pose_slots(k_pose_tangent<false>);
+    dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
         k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
     else
