@@ -172,7 +172,7 @@ __device__ __forceinline__ bool sample_pos(const float* Hi, const FfdView& f, in
 // The 45 sums: 0 Σw, 1–4 Σw a, 5–8 Σw b, 9–24 Σw a_i b_j, 25–34 / 35–44 upper triangles of
 // Σw a aᵀ and Σw b bᵀ.
 template <bool FFD>
-__global__ void __launch_bounds__(256) k_pose_moments(const float4* __restrict__ fa, int aw, int ah,
+__global__ void __launch_bounds__(256, FFD ? 2 : 3) k_pose_moments(const float4* __restrict__ fa, int aw, int ah,
                                                       const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, double* __restrict__ sums,
                                                       PoseFfd ffd) {
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256) k_pose_moments(const float4* __restrict__
         if (wt <= 0.f) continue;
         const float flx = floorf(fx), fly = floorf(fy);
         const float ax = fx - flx, ay = fy - fly;
-        const size_t i00 = (size_t)fly * aw + (size_t)flx;
+        const size_t i00 = (size_t)(int)fly * aw + (int)flx;  // fx, fy ≥ 2 here
         float va[4], vb[4];
         const Taps4 tp = taps4(fa, i00, aw);
         const float4 b4 = __ldg(&fb[t]);
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__
         taper(fx, fy, (float)aw, (float)ah, wt, tpx, tpy);
         const float flx = floorf(fx), fly = floorf(fy);
         const float ax = fx - flx, ay = fy - fly;
-        const size_t i00 = (size_t)fly * aw + (size_t)flx;
+        const size_t i00 = (size_t)(int)fly * aw + (int)flx;  // fx, fy ≥ 2 here
         float va[4], gx[4], gy[4], vb[4];
         const Taps4 tp = taps4(fa, i00, aw);
         const float4 b4 = __ldg(&fb[t]);
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(256) k_pose_ffd_grad(const float4* __restrict_
         taper(fx, fy, (float)aw, (float)ah, wt, tpx, tpy);
         const float flx = floorf(fx), fly = floorf(fy);
         const float ax = fx - flx, ay = fy - fly;
-        const size_t i00 = (size_t)fly * aw + (size_t)flx;
+        const size_t i00 = (size_t)(int)fly * aw + (int)flx;  // fx, fy ≥ 2 here
         float va[4], gx[4], gy[4], vb[4];
         const Taps4 tp = taps4(fa, i00, aw);
         const float4 b4 = __ldg(&fb[t]);
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(256) k_pose_ffd_cells(const float4* __restrict
                 taper(fx, fy, sw, shh, wt, tpx, tpy);
                 const float flx = floorf(fx), fly = floorf(fy);
                 const float ax = fx - flx, ay = fy - fly;
-                const size_t i00 = (size_t)fly * aw + (size_t)flx;
+                const size_t i00 = (size_t)(int)fly * aw + (int)flx;  // fx, fy ≥ 2 here
                 float va[4], gx[4], gy[4], vb[4];
                 const Taps4 tp = taps4(fa, i00, aw);
                 const float4 b4 = __ldg(&fb[t]);

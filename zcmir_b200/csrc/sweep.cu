@@ -18,45 +18,55 @@ __global__ void k_interleave(const float* __restrict__ stack, int n, float4* __r
     }
 }
 
-// One thread per cell (x, y) of item z's window; the item's pose is poses[(slot0 + z)·12 ..]: the
-// dest → source map (row-major 3×3, 1-based pixels), taps per side, the window's first canvas
-// cell. The cell's value is the mean of k×k bilinear taps of the source stack at the cell's
-// sub-points (sweep.wgsl tap, pack_sweep); a tap whose 2×2 footprint leaves the image adds
-// nothing. Cells past the G×G canvas are zero. Output plane-major [5][win_y][win_x] per item.
-// With fixed weights fw ([Fy][Fx], the fixed window at canvas cell (fx0, fy0)) the item's zero-lag
-// overlap Σ w_moving · w_fixed over the cells both windows cover accumulates into n0[z] (sweep.wgsl
-// zero_lag reads the same value off the correlation of the weight planes).
+// Warp w of a block takes the 32 cells x0 .. x0 + 31 of row y of item z's window; the item's
+// pose is poses[(slot0 + z)·12 ..]: the dest → source map (row-major 3×3, 1-based pixels), taps
+// per side, the window's first canvas cell. The cell's value is the mean of k×k bilinear taps of
+// the source stack at the cell's sub-points (sweep.wgsl tap, pack_sweep); a tap whose 2×2
+// footprint leaves the image adds nothing. Cells past the G×G canvas are zero. Output plane-major
+// [5][win_y][win_x] per item. The taps run across the lanes: in each pass, groups of k lanes take
+// ⌊32/k⌋ cells, lane (g, tx) summing tap column tx of its cell over the k tap rows, so adjacent
+// lanes read adjacent pixels (one cache line serves several lanes) instead of pixels a cell apart;
+// each group's k column sums are then added across its lanes and handed to the lane that owns
+// the cell. With fixed weights fw ([Fy][Fx], the fixed window at canvas cell (fx0, fy0)) the
+// item's zero-lag overlap Σ w_moving · w_fixed over the cells both windows cover accumulates into
+// n0[z] (sweep.wgsl zero_lag reads the same value off the correlation of the weight planes).
 __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ il, int sw, int sh,
                                                     const float* __restrict__ poses, int slot0, int win_x, int win_y,
                                                     SweepCanvas cv, const float* __restrict__ fw, int fx0, int fy0,
                                                     int Fx, int Fy, float* __restrict__ grid, double* __restrict__ n0) {
-    // 256 threads as a 32 × 8 tile of cells
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5), z = blockIdx.z;
+    const int lane = threadIdx.x & 31;
+    const int x0 = blockIdx.x * 32, y = blockIdx.y * 8 + (threadIdx.x >> 5), z = blockIdx.z;
     const float* P = poses + (size_t)(slot0 + z) * 12;
-    const int cx = (int)P[10] + x, cy = (int)P[11] + y;
+    const int cy = (int)P[11] + y;
+    const int x = x0 + lane;
     const bool in_win = x < win_x && y < win_y;
+    const int k = min(max((int)P[9], 1), 32), cpw = 32 / k;
+    const float h0 = P[0], h1 = P[1], h2 = P[2], h3 = P[3], h4 = P[4], h5 = P[5], h6 = P[6], h7 = P[7], h8 = P[8];
+    const float inv = 1.f / (float)(k * k);
+    const int grp = lane / k, tx = lane - grp * k;
     float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    if (in_win && cx < cv.G && cy < cv.G) {
-        const int k = max((int)P[9], 1);
-        const float h0 = P[0], h1 = P[1], h2 = P[2], h3 = P[3], h4 = P[4], h5 = P[5], h6 = P[6], h7 = P[7], h8 = P[8];
+    for (int c0 = 0; c0 < 32; c0 += cpw) {
+        const int xw = x0 + c0 + grp, cx = (int)P[10] + xw;
+        const bool act = grp < cpw && c0 + grp < 32 && xw < win_x && y < win_y && cx < cv.G && cy < cv.G;
         float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
         float a4 = 0.f;
-        for (int ty = 0; ty < k; ++ty) {
-            const float py = cv.oy + ((float)cy + ((float)ty + 0.5f) / (float)k) * cv.cell;
-            for (int tx = 0; tx < k; ++tx) {
-                const float px = cv.ox + ((float)cx + ((float)tx + 0.5f) / (float)k) * cv.cell;
+        if (act) {
+            const float px = cv.ox + ((float)cx + ((float)tx + 0.5f) / (float)k) * cv.cell;
+            for (int ty = 0; ty < k; ++ty) {
+                const float py = cv.oy + ((float)cy + ((float)ty + 0.5f) / (float)k) * cv.cell;
                 const float qx = h0 * px + h1 * py + h2;
                 const float qy = h3 * px + h4 * py + h5;
                 const float qz = h6 * px + h7 * py + h8;
                 if (fabsf(qz) < 1e-8f) continue;
-                const float fx = qx / qz - 1.0f, fy = qy / qz - 1.0f;
+                // affine poses (qz = 1): the division is exact, skip it
+                const float fx = (qz == 1.f ? qx : qx / qz) - 1.0f, fy = (qz == 1.f ? qy : qy / qz) - 1.0f;
                 const float flx = floorf(fx), fly = floorf(fy);
                 // x0 ≥ 0 and x0 + 1 < w (NaN fails both), before any float → int conversion
                 if (!(flx >= 0.f && fly >= 0.f && flx < (float)(sw - 1) && fly < (float)(sh - 1))) continue;
-                const int x0 = (int)flx, y0 = (int)fly;
+                const int ix = (int)flx, iy = (int)fly;
                 const float ax = fx - flx, ay = fy - fly;
                 const float w00 = (1.f - ax) * (1.f - ay), w10 = ax * (1.f - ay), w01 = (1.f - ax) * ay, w11 = ax * ay;
-                const size_t i00 = (size_t)y0 * sw + x0, i01 = i00 + sw;
+                const size_t i00 = (size_t)iy * sw + ix, i01 = i00 + sw;
                 const float4 p00 = __ldg(&il[2 * i00]), p10 = __ldg(&il[2 * i00 + 2]);
                 const float4 p01 = __ldg(&il[2 * i01]), p11 = __ldg(&il[2 * i01 + 2]);
                 a.x += w00 * p00.x + w10 * p10.x + w01 * p01.x + w11 * p11.x;
@@ -67,12 +77,25 @@ __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ i
                       w01 * __ldg(&il[2 * i01 + 1]).x + w11 * __ldg(&il[2 * i01 + 3]).x;
             }
         }
-        const float inv = 1.f / (float)(k * k);
-        s[0] = a.x * inv;
-        s[1] = a.y * inv;
-        s[2] = a.z * inv;
-        s[3] = a.w * inv;
-        s[4] = a4 * inv;
+        // the group's k column sums, added in every lane of the group (k is the same for the warp)
+        float t[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int j = 0; j < k; ++j) {
+            const int src = min(grp * k + j, 31);
+            t[0] += __shfl_sync(0xffffffffu, a.x, src);
+            t[1] += __shfl_sync(0xffffffffu, a.y, src);
+            t[2] += __shfl_sync(0xffffffffu, a.z, src);
+            t[3] += __shfl_sync(0xffffffffu, a.w, src);
+            t[4] += __shfl_sync(0xffffffffu, a4, src);
+        }
+        // lane L owns strip cell L: this pass holds it when c0 ≤ L < c0 + cpw, in group L − c0
+        const int mine = lane - c0;
+        const bool here = mine >= 0 && mine < cpw;
+        const int src = here ? mine * k : 0;
+#pragma unroll
+        for (int p = 0; p < 5; ++p) {
+            const float v = __shfl_sync(0xffffffffu, t[p], src);
+            if (here) s[p] = v * inv;
+        }
     }
     if (in_win) {
         const size_t wn = (size_t)win_x * win_y;
@@ -83,7 +106,7 @@ __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ i
     if (!n0) return;
     double v = 0.0;
     if (in_win) {
-        const int fx = cx - fx0, fy = cy - fy0;
+        const int fx = (int)P[10] + x - fx0, fy = cy - fy0;
         if (fx >= 0 && fy >= 0 && fx < Fx && fy < Fy) v = (double)s[0] * (double)__ldg(&fw[(size_t)fy * Fx + fx]);
     }
     __shared__ double red[32];
