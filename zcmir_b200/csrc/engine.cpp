@@ -112,6 +112,8 @@ Engine::~Engine() {
     for (DevBuf* b : {&rs_fwd_, &rs_inv_, &rs_map_, &pp_rgba_, &pp_clahe_, &pp_tmp_, &pp_mm_, &ffd_dev_, &ffd_out_,
                       &ffd_pk_, &ffd_cells_, &ffd_coef_})
         b->release();
+    pose_in_pin_.release();
+    pose_out_pin_.release();
     for (auto& kv : tw_) cudaFree(kv.second);
     for (cudaEvent_t e : chunk_ev_)
         if (e) cudaEventDestroy(e);

@@ -31,6 +31,30 @@ struct DevBuf {
     }
 };
 
+// Page-locked host memory that grows on demand, for copies the copy engines run straight from
+// or into host memory (no staging pass). Regrown only while no copy into it is pending.
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        release();
+        const cudaError_t e = cudaMallocHost(&p, bytes);
+        if (e == cudaSuccess) cap = bytes;
+        else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
 struct Side {
     bool has = false;
     int w = 0, h = 0;
@@ -295,7 +319,7 @@ class Engine {
     std::vector<Side> stack_;
     DevBuf stack_res_;
     DevBuf sw_il_[2], sw_poses_, sw_fgrid_, sw_fhalf_, sw_grid_, sw_half_, sw_q_, sw_map_, sw_n0_, sw_ps_, sw_pi_;
-    std::vector<float> pose_host_;
+    PinnedBuf pose_in_pin_, pose_out_pin_;  // eval_poses: inverse poses + generators up, sums back
     std::vector<float> ffd_cps_ = std::vector<float>(2 * 16 * 16, 0.f);
     unsigned ffd_g_ = 4;
     bool ffd_suspended_ = false;  // the search's climbs run without the spline

@@ -60,20 +60,26 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
               cuda_ok(pose_coef_.ensure(m * kCoef * 4), "score") && cuda_ok(pose_score_.ensure(m * 8), "score") &&
               cuda_ok(pose_tsum_.ensure(m * kGrad * 8), "score") && cuda_ok(pose_gens_.ensure(2 * 72 * 4), "score");
     if (!ok) return false;
-    // inverse poses: forward direction H⁻¹; inverse direction (pose H⁻¹) its inverse
-    pose_host_.assign(m * 9 + 2 * 72, 0.f);
+    // inverse poses: forward direction H⁻¹; inverse direction (pose H⁻¹) its inverse; written to
+    // page-locked memory, as the sums come back into it, so neither copy is staged
+    const size_t n_in = m * 9 + 2 * 72, n_out = m * kMom + m + (grad ? m * kGrad : 0);
+    if (!cuda_ok(pose_in_pin_.ensure(n_in * sizeof(float)), "score") ||
+        !cuda_ok(pose_out_pin_.ensure(n_out * sizeof(double)), "score"))
+        return false;
+    float* pose_host = pose_in_pin_.as<float>();
+    std::fill(pose_host, pose_host + n_in, 0.f);
     for (int i = 0; i < n; ++i) {
         const Mat3 Hi = inv3(Hs[i]);
-        for (int k = 0; k < 9; ++k) pose_host_[(size_t)i * 9 + k] = (float)Hi[k];
+        for (int k = 0; k < 9; ++k) pose_host[(size_t)i * 9 + k] = (float)Hi[k];
         if (sym) {
             const Mat3 Hii = inv3(Hi);
-            for (int k = 0; k < 9; ++k) pose_host_[((size_t)n + i) * 9 + k] = (float)Hii[k];
+            for (int k = 0; k < 9; ++k) pose_host[((size_t)n + i) * 9 + k] = (float)Hii[k];
         }
     }
     const Side &A = side[0], &B = side[1];
     // generators in the destination's pixels: the fixed image forward, the moving one inverse
     const auto gf = generators(homog, B.w, B.h), gi = generators(homog, A.w, A.h);
-    float* gens = pose_host_.data() + m * 9;
+    float* gens = pose_host + m * 9;
     for (int k = 0; k < 8; ++k)
         for (int e = 0; e < 9; ++e) {
             gens[k * 9 + e] = (float)gf[k][e];
@@ -81,7 +87,7 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
         }
     float* dh = pose_hinv_.as<float>();
     float* dg = pose_gens_.as<float>();
-    if (!cuda_ok(cudaMemcpyAsync(dh, pose_host_.data(), m * 9 * 4, cudaMemcpyHostToDevice, st), "score") ||
+    if (!cuda_ok(cudaMemcpyAsync(dh, pose_host, m * 9 * 4, cudaMemcpyHostToDevice, st), "score") ||
         !cuda_ok(cudaMemcpyAsync(dg, gens, 2 * 72 * 4, cudaMemcpyHostToDevice, st), "score"))
         return false;
     const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
@@ -105,11 +111,13 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
             return false;
         counts[0] += nd;
     }
-    std::vector<double> hs(m * kMom), hsc(m), ht(grad ? m * kGrad : 0);
-    if (!cuda_ok(cudaMemcpyAsync(hs.data(), sums, m * kMom * 8, cudaMemcpyDeviceToHost, st), "score") ||
-        !cuda_ok(cudaMemcpyAsync(hsc.data(), pose_score_.p, m * 8, cudaMemcpyDeviceToHost, st), "score"))
+    double* hs = pose_out_pin_.as<double>();
+    double* hsc = hs + m * kMom;
+    double* ht = hsc + m;
+    if (!cuda_ok(cudaMemcpyAsync(hs, sums, m * kMom * 8, cudaMemcpyDeviceToHost, st), "score") ||
+        !cuda_ok(cudaMemcpyAsync(hsc, pose_score_.p, m * 8, cudaMemcpyDeviceToHost, st), "score"))
         return false;
-    if (grad && !cuda_ok(cudaMemcpyAsync(ht.data(), tsum, m * kGrad * 8, cudaMemcpyDeviceToHost, st), "score")) return false;
+    if (grad && !cuda_ok(cudaMemcpyAsync(ht, tsum, m * kGrad * 8, cudaMemcpyDeviceToHost, st), "score")) return false;
     if (!cuda_ok(cudaStreamSynchronize(st), "score")) return false;
     counts[1]++;
     counts[2] += grad ? 3 : 2;
@@ -121,7 +129,7 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
         g = Coords{};
         A.fill(0.0);
         if (!(nsum >= 12.0)) return;
-        const double* t = ht.data() + row * kGrad;
+        const double* t = ht + row * kGrad;
         for (int q = 0; q < nk; ++q) g[q] = t[q];
         int h = 8;
         for (int q = 0; q < 8; ++q)
