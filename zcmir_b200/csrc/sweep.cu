@@ -114,18 +114,21 @@ __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ i
     if (threadIdx.x == 0 && v != 0.0) atomicAdd(&n0[z], v);
 }
 
-// One block of 256 threads per item (sweep.wgsl peaks_sweep): lane l keeps the best 3×3 local
-// maximum (periodic, > 0, the first of equal ones) among the shifts t ≡ l (mod 256); the n_peak
-// best lanes (equal scores: the lower lane first) are written to slot (slot0 + z) as (score,
-// index), and (0, 0xffffffff) where fewer lanes found one.
-__global__ void __launch_bounds__(256) k_sweep_peaks(const float* __restrict__ maps, int nx, int ny, size_t mstride,
-                                                     int n_peak, int slot0, float* __restrict__ ps,
-                                                     uint32_t* __restrict__ pi) {
+// One block per item (sweep.wgsl peaks_sweep): lane l < 256 keeps the best 3×3 local maximum
+// (periodic, > 0, the first of equal ones) among the shifts t ≡ l (mod 256); the n_peak best lanes
+// (equal scores: the lower lane first) are written to slot (slot0 + z) as (score, index), and
+// (0, 0xffffffff) where fewer lanes found one. The block's 1024 threads scan each lane's shifts
+// four ways (thread (l, q) the shifts l + 256·(q + 4j)) and merge the four bests per lane by the
+// same rule (higher score, then lower shift), which is the lane's own best.
+__global__ void __launch_bounds__(1024) k_sweep_peaks(const float* __restrict__ maps, int nx, int ny, size_t mstride,
+                                                      int n_peak, int slot0, float* __restrict__ ps,
+                                                      uint32_t* __restrict__ pi) {
     const float* m = maps + (size_t)blockIdx.x * mstride;
     const int nn = nx * ny;
+    const int l = threadIdx.x & 255, q = threadIdx.x >> 8;
     float bv = 0.f;
     uint32_t bi = 0xffffffffu;
-    for (int t = threadIdx.x; t < nn; t += 256) {
+    for (int t = l + 256 * q; t < nn; t += 1024) {
         const float v = __ldg(&m[t]);
         if (v <= bv) continue;
         const int y = t / nx, x = t - y * nx;
@@ -138,10 +141,27 @@ __global__ void __launch_bounds__(256) k_sweep_peaks(const float* __restrict__ m
             bi = (uint32_t)t;
         }
     }
+    __shared__ float sv[3][256];
+    __shared__ uint32_t si[3][256];
+    if (q > 0) {
+        sv[q - 1][l] = bv;
+        si[q - 1][l] = bi;
+    }
+    __syncthreads();
+    if (q == 0)
+        for (int r = 0; r < 3; ++r) {
+            const float v = sv[r][l];
+            const uint32_t i = si[r][l];
+            if (v > bv || (v == bv && i < bi)) {
+                bv = v;
+                bi = i;
+            }
+        }
     // a positive float's bits order like the float: (score, inverted lane) as one key
-    unsigned long long key = bi == 0xffffffffu ? 0ull
-                                               : ((unsigned long long)__float_as_uint(bv) << 32) | (0xffffffffu - threadIdx.x);
-    __shared__ unsigned long long wmax[8];
+    unsigned long long key = (q > 0 || bi == 0xffffffffu)
+                                 ? 0ull
+                                 : ((unsigned long long)__float_as_uint(bv) << 32) | (0xffffffffu - (uint32_t)l);
+    __shared__ unsigned long long wmax[32];
     __shared__ unsigned long long top;
     for (int k = 0; k < n_peak; ++k) {
         unsigned long long w = key;
@@ -154,7 +174,7 @@ __global__ void __launch_bounds__(256) k_sweep_peaks(const float* __restrict__ m
         __syncthreads();
         if (threadIdx.x == 0) {
             unsigned long long b = 0;
-            for (int i = 0; i < 8; ++i) b = wmax[i] > b ? wmax[i] : b;
+            for (int i = 0; i < 32; ++i) b = wmax[i] > b ? wmax[i] : b;
             top = b;
         }
         __syncthreads();
@@ -197,7 +217,7 @@ cudaError_t sweep_pack(const float4* il, int sw, int sh, const float* poses, int
 
 cudaError_t sweep_peaks(const float* maps, int nx, int ny, size_t map_stride, int batch, int n_peak, int slot0,
                         float* ps, uint32_t* pi, cudaStream_t st) {
-    k_sweep_peaks<<<batch, 256, 0, st>>>(maps, nx, ny, map_stride, n_peak, slot0, ps, pi);
+    k_sweep_peaks<<<batch, 1024, 0, st>>>(maps, nx, ny, map_stride, n_peak, slot0, ps, pi);
     return cudaGetLastError();
 }
 
