@@ -444,7 +444,9 @@ inline int lines_per_block(int tl, int want_threads) { return std::max(1, want_t
 inline int col_tile(int n, int tl, int ncols) {
     int tx = std::min(lines_per_block(tl, 512), ncols);
     while (tx > 1 && (size_t)tx * line_pitch(n) * sizeof(float2) > 110 * 1024) tx >>= 1;
-    return tx;
+    // the same number of tiles, balanced: no last tile of mostly idle columns
+    const int tiles = (ncols + tx - 1) / tx;
+    return (ncols + tiles - 1) / tiles;
 }
 // the split row pass: as many lines as fit 512 threads, at most 4 (the score phase uses all 512)
 inline int split_lines(int tl) { return std::min(lines_per_block(tl, 512), 4); }
