@@ -2,6 +2,7 @@
 
     python -m zcmir_b200.profile_map [--n 1024] [--cap 2048] [--maps 2] [--features laplacian]
     python -m zcmir_b200.profile_map --sweep [--n 512] [--maps 1] [--nth 360] [--ns 9] [--batch 0]
+    python -m zcmir_b200.profile_map --search [--n 512] [--maps 1]
 
 Maps: builds the seeded segmented pair (zcmir_b200.synth.pair_segmented) at n², uploads it, then
 runs `--maps` maps at the identity pose (exact, calibrated) through the C ABI, printing the plan
@@ -13,6 +14,12 @@ Sweeps (--sweep): the seeded similarity pair (zcmir_b200.synth.pair_similarity) 
 by default) through zcb_sweep. Each sweep launches interleave ×2 and the fixed window's pack, then
 per plane size the fixed window's fwd_rows and cols, then per batch pack, fwd_rows, cols,
 inv_cols, rows and peaks.
+
+Searches (--search): the same pair and sweep grid, then `--maps` whole searches from the
+identity pose (the sweep, its peaks' non-maximum suppression, the batched Gauss–Newton screen and
+the finalists' climbs): after the sweep's launches, each Gauss–Newton step evaluates its poses
+with pose_moments (forward and inverse direction), pose_coefs and, for the gradient,
+pose_tangent.
 """
 import argparse
 
@@ -29,10 +36,22 @@ def main():
     ap.add_argument("--maps", type=int, default=2)
     ap.add_argument("--features", default="laplacian")
     ap.add_argument("--sweep", action="store_true")
+    ap.add_argument("--search", action="store_true")
     ap.add_argument("--nth", type=int, default=360)
     ap.add_argument("--ns", type=int, default=9)
     ap.add_argument("--batch", type=int, default=0)
     a = ap.parse_args()
+    if a.search:
+        n = a.n or 512
+        m, f, H = synth.pair_similarity(n=n, seed=2)
+        with zc.Registrar(half=False, smi_features=a.features, sw_nth=a.nth, sw_ns=a.ns, sw_smin=0.8, sw_smax=1.25,
+                          sw_grid=128) as reg:
+            reg.set_images(m, f, preprocess=False)
+            for _ in range(a.maps):
+                reg.pose = np.eye(3)
+                r = reg.search()
+            print(f"search: score {r.score:.1f}")
+        return
     if a.sweep:
         n = a.n or 512
         m, f, H = synth.pair_similarity(n=n, seed=2)
