@@ -74,7 +74,11 @@ Engine::Engine(int dev) : device(dev) {
     if (const char* v = getenv("ZCMIR_B200_ROW_PASS")) row_pass = v;
     cudaSetDevice(dev);
     cudaGetDeviceProperties(&prop, dev);
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    // priorities: side 1's feature build (st2_) highest, so it is not starved by side 0's passes
+    // queued beside it; the engine stream next; the autocorrelation's stream lowest, its blocks
+    // fill what the others leave (a lower number is a higher priority)
+    cudaDeviceGetStreamPriorityRange(&prio_lo_, &prio_hi_);
+    cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, std::min(prio_hi_ + 1, prio_lo_));
 }
 
 Engine::~Engine() {
@@ -96,6 +100,10 @@ Engine::~Engine() {
     if (st2_) {
         cudaStreamSynchronize(st2_);
         cudaStreamDestroy(st2_);
+    }
+    if (acf_st_) {
+        cudaStreamSynchronize(acf_st_);
+        cudaStreamDestroy(acf_st_);
     }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
@@ -243,7 +251,7 @@ bool Engine::bake(int s, cudaStream_t bs) {
 bool Engine::build_stream(int s, cudaStream_t& bs) {
     bs = st;
     if (s != 1 || side[s].preprocess) return true;
-    if (!st2_ && !cuda_ok(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking), "features")) return false;
+    if (!st2_ && !cuda_ok(cudaStreamCreateWithPriority(&st2_, cudaStreamNonBlocking, prio_hi_), "features")) return false;
     bs = st2_;
     return true;
 }
@@ -275,24 +283,32 @@ bool Engine::build_side(int s) {
     fsc.acf_part = part.as<float>();
     fsc.acf_part_cap = part.cap / 4;
     fsc.acf = sd.acf_dev.as<double>();
+    // the side's previous autocorrelation (on acf_st_) reads the features this build rewrites
+    if (sd.acf_ev && !cuda_ok(cudaStreamWaitEvent(bs, sd.acf_ev, 0), "features")) return false;
     if (!bake(s, bs)) return false;
     if (!cuda_ok(build_features(sd.work.as<float>(), sd.w, sd.h, mode, half, rtmp.as<float>(), sd.feat.as<float>(),
                                 sd.mag.as<float>(), sd.stack.as<float>(), fsc, bs),
                  "features") ||
         !cuda_ok(interleave_features(sd.feat.as<float>(), (int)n, sd.feat4.as<float4>(), bs), "features"))
         return false;
-    counts[0] += 14;
-    // the autocorrelation sums go back to the host on the build's stream; finish_acf waits for
-    // that copy alone when they are next needed, so neither this call nor a map waits for a build
-    if (!sd.acf_host && !cuda_ok(cudaMallocHost(&sd.acf_host, 1156 * sizeof(double)), "features")) return false;
-    if (!sd.acf_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.acf_ev, cudaEventDisableTiming), "features")) return false;
-    if (!cuda_ok(cudaMemcpyAsync(sd.acf_host, sd.acf_dev.p, 1156 * sizeof(double), cudaMemcpyDeviceToHost, bs),
-                 "features") ||
-        !cuda_ok(cudaEventRecord(sd.acf_ev, bs), "features"))
-        return false;
-    counts[2]++;
+    counts[0] += 12;
     if (!sd.built_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.built_ev, cudaEventDisableTiming), "features")) return false;
     if (!cuda_ok(cudaEventRecord(sd.built_ev, bs), "features")) return false;
+    // the autocorrelation (only the calibrated score's correlation area needs it) runs on a
+    // stream of its own at low priority, beside the passes that use the features, and its sums
+    // go back to the host there; finish_acf waits for that copy alone when the area is needed
+    if (!acf_st_ && !cuda_ok(cudaStreamCreateWithPriority(&acf_st_, cudaStreamNonBlocking, prio_lo_), "features"))
+        return false;
+    if (!sd.acf_host && !cuda_ok(cudaMallocHost(&sd.acf_host, 1156 * sizeof(double)), "features")) return false;
+    if (!sd.acf_ev && !cuda_ok(cudaEventCreateWithFlags(&sd.acf_ev, cudaEventDisableTiming), "features")) return false;
+    if (!cuda_ok(cudaStreamWaitEvent(acf_st_, sd.built_ev, 0), "features") ||
+        !cuda_ok(autocorrelation(sd.feat.as<float>(), sd.w, sd.h, fsc, acf_st_), "features") ||
+        !cuda_ok(cudaMemcpyAsync(sd.acf_host, sd.acf_dev.p, 1156 * sizeof(double), cudaMemcpyDeviceToHost, acf_st_),
+                 "features") ||
+        !cuda_ok(cudaEventRecord(sd.acf_ev, acf_st_), "features"))
+        return false;
+    counts[0] += 2;
+    counts[2]++;
     // the engine stream's later work (maps, scores) waits for a build on the side stream when it
     // first needs the side (join_side), so a map's passes over side 0 may start before it
     sd.join_pending = own;

@@ -312,6 +312,8 @@ class Engine {
     FeatScratch fs2_;  // side 1's own scratch when it builds on st2_
     DevBuf fs2_stats_, fs2_hist_, fs2_wt_, fs2_acfpart_, rank_tmp2_;
     cudaStream_t st2_ = nullptr;
+    cudaStream_t acf_st_ = nullptr;     // the features' autocorrelations, lowest priority
+    int prio_lo_ = 0, prio_hi_ = 0;     // the device's stream priority range
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
     DevBuf rs_fwd_, rs_inv_, rs_map_;

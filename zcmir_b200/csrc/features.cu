@@ -314,12 +314,16 @@ cudaError_t build_features(float* gray, int w, int h, int mode, bool half, float
     k_featmom<<<grid_for(n) < 296 ? grid_for(n) : 296, kThreads, 0, st>>>(feat, n, s.stats + 2);
     k_chol<<<1, 32, 0, st>>>(s.stats + 2, n, 1e-4f, s.wt);
     k_whiten<<<gb, kThreads, 0, st>>>(feat, n, s.wt);
+    k_stack<<<gb, kThreads, 0, st>>>(feat, n, stack);
+    return cudaGetLastError();
+}
+
+cudaError_t autocorrelation(const float* feat, int w, int h, FeatScratch& s, cudaStream_t st) {
     dim3 ga((w + kAcfTile - 1) / kAcfTile, (h + kAcfTile - 1) / kAcfTile);
     const int ntiles = ga.x * ga.y;
     if ((size_t)ntiles * 1156 > s.acf_part_cap) return cudaErrorInvalidValue;
     k_acf<<<ga, kAcfThreads, 0, st>>>(feat, w, h, s.acf_part);
     k_acf_finish<<<1156, kThreads, 0, st>>>(s.acf_part, ntiles, w, h, s.acf);
-    k_stack<<<gb, kThreads, 0, st>>>(feat, n, stack);
     return cudaGetLastError();
 }
 

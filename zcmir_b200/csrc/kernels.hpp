@@ -19,11 +19,13 @@ struct FeatScratch {
     double* acf = nullptr;       // 289 × 4 normalised autocorrelation
 };
 
-// gray (w×h f32, device) → feat (4 planes), mag (1 plane), stack (5 planes), acf (289×4,
-// device doubles in scratch.acf). mode: 0 laplacian, 1 three, 2 cubic. `half`: quantise the
-// input to f16 first (in place on `gray`).
+// gray (w×h f32, device) → feat (4 planes), mag (1 plane), stack (5 planes). mode: 0 laplacian,
+// 1 three, 2 cubic. `half`: quantise the input to f16 first (in place on `gray`).
 cudaError_t build_features(float* gray, int w, int h, int mode, bool half, float* rank_tmp, float* feat,
                            float* mag, float* stack, FeatScratch& s, cudaStream_t st);
+// the features' autocorrelation sums at |τ| ≤ 8 (289 lags × 4 planes, device doubles in s.acf;
+// per-tile partials in s.acf_part)
+cudaError_t autocorrelation(const float* feat, int w, int h, FeatScratch& s, cudaStream_t st);
 
 // ── shift maps (shiftmap.cu) ──
 struct MapGeom {
