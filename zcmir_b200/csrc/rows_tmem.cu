@@ -36,6 +36,12 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tmem_st1(uint32_t taddr, float v) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(taddr), "r"(__float_as_uint(v)) : "memory");
 }
+// two consecutive columns (taddr, taddr + 1) of this thread's lane
+__device__ __forceinline__ void tmem_st2(uint32_t taddr, float a, float b) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(__float_as_uint(a)),
+                 "r"(__float_as_uint(b))
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -101,6 +107,7 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
 
     if constexpr (rows_io<N>()) {
         static_assert(N / Mix<N>::radix(Mix<N>::kStages - 1) % 128 == 0, "last-stage outputs must fall in lane t");
+        const int n_tm = n_corr < kTmemSlots ? n_corr : kTmemSlots;
         for (int p0 = 0; p0 < npairs; p0 += LINES) {
             const int pr = p0 + line;
             const bool act = pr < npairs;
@@ -108,18 +115,22 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
             const bool h2 = k2 < n_corr;
             const float2* q1 = Q + (size_t)(act ? k1 : 0) * pstride + (size_t)y * WP;
             const float2* q2 = Q + (size_t)(act && h2 ? k2 : 0) * pstride + (size_t)y * WP;
-            fft.template run_io<true>(
-                buf, t, act,
-                [&](int x) {
-                    // Z = Q1 + i·Q2 on the half row, conj(Q1) + i·conj(Q2) mirrored above it
-                    const int ix = x <= N / 2 ? x : N - x;
-                    const float2 a = __ldg(&q1[ix]);
-                    const float2 b = h2 ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
-                    return x <= N / 2 ? make_float2(a.x - b.y, a.y + b.x) : make_float2(a.x + b.y, b.x - a.y);
-                },
-                [&](int m, float2 z) {
-                    // cell m lies in TMEM lane m mod 128 = t, this warp's quadrant; the warp's
-                    // lines all run, so each store is executed by the whole warp
+            // Z = Q1 + i·Q2 on the half row, conj(Q1) + i·conj(Q2) mirrored above it
+            auto in = [&](int x) {
+                const int ix = x <= N / 2 ? x : N - x;
+                const float2 a = __ldg(&q1[ix]);
+                const float2 b = h2 ? __ldg(&q2[ix]) : make_float2(0.f, 0.f);
+                return x <= N / 2 ? make_float2(a.x - b.y, a.y + b.x) : make_float2(a.x + b.y, b.x - a.y);
+            };
+            if (2 * (p0 + LINES) <= n_tm) {
+                // every line of the round has both its slots in TMEM: one two-column store per
+                // output (cell m lies in TMEM lane m mod 128 = t, this warp's quadrant)
+                fft.template run_io<true>(buf, t, true, in, [&](int m, float2 z) {
+                    tmem_st2(tq + (uint32_t)(m >> 7) * kTmemSlots + (uint32_t)k1, z.x, z.y);
+                });
+            } else {
+                fft.template run_io<true>(buf, t, act, in, [&](int m, float2 z) {
+                    // the warp's lines all run, so each store is executed by the whole warp
                     const uint32_t col = (uint32_t)(m >> 7) * kTmemSlots;
                     if (k1 < kTmemSlots) tmem_st1(tq + col + (uint32_t)k1, z.x);
                     else cs[(size_t)(k1 - kTmemSlots) * N + m] = z.x;
@@ -128,6 +139,7 @@ __global__ void __launch_bounds__(512, 1) k_rows_tmem(const float2* __restrict__
                         else cs[(size_t)(k2 - kTmemSlots) * N + m] = z.y;
                     }
                 });
+            }
             __syncthreads();  // the line buffers are refilled next round
         }
     } else {
