@@ -70,15 +70,14 @@ namespace {
 // ── forward: real planes → row R2C → column FFT ─────────────────────────────────────────────
 
 // Real correlation plane r of a staged row [5][cw] of premultiplied samples s = [w, w f0..w f3]
-// (smi.wgsl:641-649): 0 → w, 1..4 → w f_i, 5..14 → s_i s_j / s_0 (0 where s_0 ≤ 1e-6).
-__device__ __forceinline__ float real_plane_row(int r, const float* row, int cw, int x) {
+// (smi.wgsl:641-649): 0 → w, 1..4 → w f_i, 5..14 → s_i s_j / s_0 (0 where s_0 ≤ 1e-6), the
+// division as a product with inv0[x] = 1 / s_0 (0 where s_0 ≤ 1e-6), staged with the row.
+__device__ __forceinline__ float real_plane_row(int r, const float* row, const float* inv0, int cw, int x) {
     if (r < 5) return row[r * cw + x];
-    const float s0 = row[x];
-    if (s0 <= 1e-6f) return 0.f;
     const int k = r - 5;
     const int ti = (k < 4) ? 0 : (k < 7) ? 1 : (k < 9) ? 2 : 3;
     const int tj = (k < 4) ? k : (k < 7) ? k - 3 : (k < 9) ? k - 5 : 3;
-    return row[(1 + ti) * cw + x] * row[(1 + tj) * cw + x] / s0;
+    return row[(1 + ti) * cw + x] * row[(1 + tj) * cw + x] * inv0[x];
 }
 
 // One block per grid row y < ch; lines = packed plane pairs (2z, 2z+1), lpb of them at a time.
@@ -99,12 +98,15 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
     const int pl = padded_len(nx);
     float2* buf = smem + (line < lpb ? line : 0) * pl;
     float* row = reinterpret_cast<float*>(smem + lpb * pl);  // [5][cw]
+    float* inv0 = row + 5 * cw;                               // [cw]
     __shared__ int planes[16];
     if (threadIdx.x < 16) planes[threadIdx.x] = threadIdx.x < plan.n_real ? plan.planes[threadIdx.x] : -1;
     const size_t gn = (size_t)cw * ch;
     for (int i = threadIdx.x; i < 5 * cw; i += blockDim.x) {
         const int p = i / cw, x = i - p * cw;
-        row[i] = __ldg(&grid[p * gn + (size_t)y * cw + x]);
+        const float v = __ldg(&grid[p * gn + (size_t)y * cw + x]);
+        row[i] = v;
+        if (p == 0) inv0[x] = v <= 1e-6f ? 0.f : 1.f / v;
     }
     __syncthreads();
     const int n_cplx = (plan.n_real + 1) / 2;
@@ -117,8 +119,8 @@ __global__ void __launch_bounds__(512, 1) k_fwd_rows(const float* __restrict__ g
         f.template run_in<false, LO>(buf, t, act, [&](int x) {
             float2 v = make_float2(0.f, 0.f);
             if (x < cw) {
-                v.x = real_plane_row(ra, row, cw, x);
-                if (rb >= 0) v.y = real_plane_row(rb, row, cw, x);
+                v.x = real_plane_row(ra, row, inv0, cw, x);
+                if (rb >= 0) v.y = real_plane_row(rb, row, inv0, cw, x);
             }
             return v;
         });
@@ -496,7 +498,7 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
         const int n_cplx = (plan.n_real + 1) / 2;
         // up to 256 threads of lines (one line of more for the longest rows: 8192 points, 512 threads)
         const int lines = std::min(lines_per_block(tl, 256), n_cplx);
-        const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)5 * g.cw * sizeof(float);
+        const size_t sm = (size_t)lines * padded_len(g.nx) * sizeof(float2) + (size_t)6 * g.cw * sizeof(float);
         auto k = 2 * g.cw <= g.nx ? k_fwd_rows<F, true> : k_fwd_rows<F, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k<<<dim3(g.ch, a.batch), lines * tl, sm, st>>>(a.grid, g.cw, g.ch, g.WP, plan, f, lines, a.half,
