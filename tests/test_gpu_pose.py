@@ -61,6 +61,27 @@ def test_moments_score_gradient_match_oracle(pair, group):
     assert np.abs(g.hess - ref["hess"]).max() <= 1e-3 * np.abs(ref["hess"]).max()
 
 
+def test_ragged_images_match_oracle(pair):
+    """Image sides that are not multiples of the pose kernels' 8 × 4 pixel tiles (the last tile of
+    each tile row and the last tile row reach past the image): sums, scores and gradient as the
+    oracle has them."""
+    m, f, H = pair
+    m2, f2 = np.ascontiguousarray(m[3:160, 5:208]), np.ascontiguousarray(f[:139, 2:183])
+    Hp = _near(H)
+    with zc.Registrar(half=False, group="affine") as reg:
+        reg.set_images(m2, f2, preprocess=False)
+        A, B = reg.features(0), reg.features(1)
+        mom = reg.moments(Hp)
+        sc = reg.score(Hp)
+        g = reg.gradient(Hp, hess=True)
+    ref = P.pair_eval(A, B, Hp, homog=False, grad=True, hess=True)
+    assert ref["sums"][0] > 1000
+    np.testing.assert_allclose(mom, ref["sums"], rtol=0, atol=1e-5 * np.abs(ref["sums"]).max())
+    assert abs(sc.mean - ref["mean"]) <= 1e-5 * abs(ref["mean"])
+    assert np.linalg.norm(g.grad - ref["grad"]) <= 1e-3 * np.linalg.norm(ref["grad"])
+    assert np.abs(g.hess - ref["hess"]).max() <= 1e-3 * np.abs(ref["hess"]).max()
+
+
 def test_forward_only_and_edge_cases(pair):
     m, f, H = pair
     with zc.Registrar(half=False, symmetric=False) as reg:
