@@ -146,7 +146,7 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
         fhalf_max = std::max(fhalf_max, (size_t)plan.n_real * pstride);
     }
     const size_t na = (size_t)A.w * A.h, nb = (size_t)B.w * B.h;
-    bool ok = cuda_ok(sw_il_[0].ensure(na * 32), "sweep") && cuda_ok(sw_il_[1].ensure(nb * 32), "sweep") &&
+    bool ok = cuda_ok(sw_il_[0].ensure(na * 20), "sweep") && cuda_ok(sw_il_[1].ensure(nb * 20), "sweep") &&
               cuda_ok(sw_poses_.ensure(poses.size() * 4), "sweep") && cuda_ok(sw_fgrid_.ensure(fgrid * 4), "sweep") &&
               cuda_ok(sw_fhalf_.ensure(fhalf_max * 8), "sweep") &&
               cuda_ok(sw_grid_.ensure(grid_max * 4 * bmax), "sweep") &&

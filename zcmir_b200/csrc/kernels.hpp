@@ -106,7 +106,8 @@ struct SweepCanvas {
     float ox, oy, cell;
     int G;
 };
-// plane-major 5-plane stack of n pixels → 8 floats per pixel (w, w f0..w f3, 0, 0, 0)
+// plane-major 5-plane stack of n pixels → n float4 (w, w f0, w f1, w f2) followed by the fifth
+// plane (w f3) as n floats: 20 bytes per pixel
 cudaError_t sweep_interleave(const float* stack, int n, float4* il, cudaStream_t st);
 // the windows [batch][5][win_y][win_x] of slots slot0.. (poses: 12 floats per slot: dest →
 // source map, taps, first window cell); with fw (the fixed window's weights, [Fy][Fx] at cell

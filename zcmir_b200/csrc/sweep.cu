@@ -9,12 +9,14 @@
 namespace zc {
 namespace {
 
-// plane-major [5][n] → two float4 per pixel, (w, w f0, w f1, w f2) and (w f3, 0, 0, 0): one
-// 32-byte sector per bilinear tap (sweep.wgsl interleave)
+// plane-major [5][n] → n float4 (w, w f0, w f1, w f2), then the fifth plane (w f3) as n floats:
+// a bilinear tap is one 16-byte load per corner plus a scalar from a plane eight pixels to a
+// sector (sweep.wgsl interleave)
 __global__ void k_interleave(const float* __restrict__ stack, int n, float4* __restrict__ il) {
+    float* p4 = reinterpret_cast<float*>(il + n);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        il[2 * (size_t)i] = make_float4(stack[i], stack[(size_t)n + i], stack[2 * (size_t)n + i], stack[3 * (size_t)n + i]);
-        il[2 * (size_t)i + 1] = make_float4(stack[4 * (size_t)n + i], 0.f, 0.f, 0.f);
+        il[i] = make_float4(stack[i], stack[(size_t)n + i], stack[2 * (size_t)n + i], stack[3 * (size_t)n + i]);
+        p4[i] = stack[4 * (size_t)n + i];
     }
 }
 
@@ -41,6 +43,7 @@ __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ i
     const int x = x0 + lane;
     const bool in_win = x < win_x && y < win_y;
     const int k = min(max((int)P[9], 1), 32), cpw = 32 / k;
+    const float* p4 = reinterpret_cast<const float*>(il + (size_t)sw * sh);  // the fifth plane
     const float h0 = P[0], h1 = P[1], h2 = P[2], h3 = P[3], h4 = P[4], h5 = P[5], h6 = P[6], h7 = P[7], h8 = P[8];
     const float inv = 1.f / (float)(k * k);
     const int grp = lane / k, tx = lane - grp * k;
@@ -67,14 +70,14 @@ __global__ void __launch_bounds__(256) k_sweep_pack(const float4* __restrict__ i
                 const float ax = fx - flx, ay = fy - fly;
                 const float w00 = (1.f - ax) * (1.f - ay), w10 = ax * (1.f - ay), w01 = (1.f - ax) * ay, w11 = ax * ay;
                 const size_t i00 = (size_t)iy * sw + ix, i01 = i00 + sw;
-                const float4 p00 = __ldg(&il[2 * i00]), p10 = __ldg(&il[2 * i00 + 2]);
-                const float4 p01 = __ldg(&il[2 * i01]), p11 = __ldg(&il[2 * i01 + 2]);
+                const float4 p00 = __ldg(&il[i00]), p10 = __ldg(&il[i00 + 1]);
+                const float4 p01 = __ldg(&il[i01]), p11 = __ldg(&il[i01 + 1]);
                 a.x += w00 * p00.x + w10 * p10.x + w01 * p01.x + w11 * p11.x;
                 a.y += w00 * p00.y + w10 * p10.y + w01 * p01.y + w11 * p11.y;
                 a.z += w00 * p00.z + w10 * p10.z + w01 * p01.z + w11 * p11.z;
                 a.w += w00 * p00.w + w10 * p10.w + w01 * p01.w + w11 * p11.w;
-                a4 += w00 * __ldg(&il[2 * i00 + 1]).x + w10 * __ldg(&il[2 * i00 + 3]).x +
-                      w01 * __ldg(&il[2 * i01 + 1]).x + w11 * __ldg(&il[2 * i01 + 3]).x;
+                a4 += w00 * __ldg(&p4[i00]) + w10 * __ldg(&p4[i00 + 1]) + w01 * __ldg(&p4[i01]) +
+                      w11 * __ldg(&p4[i01 + 1]);
             }
         }
         // the group's k column sums, added in every lane of the group (k is the same for the warp)
