@@ -459,7 +459,10 @@ def run_gpu(args, rank, ws, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config({"parallelism": f"replicas{ws}", "none_28_correlations_maps_s": ws * 1000.0 / r28["ms_per_map"],
                               "plan": {k: r[k] for k in ("nx", "ny", "cw", "ch", "n_real", "n_corr", "split")},
-                              "stages_ms": r["stages_ms"]}),
+                              "stages_ms": r["stages_ms"],
+                              "timing": "CUDA events around replays of one captured CUDA graph of the map's passes; "
+                                        "stages_ms from event-instrumented maps",
+                              "ms_per_map_instrumented": r.get("ms_per_map_instrumented")}),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": b_launch, "launch_ms": t_launch,

@@ -12,9 +12,11 @@ extern "C" {
 /* Time `steps` shift maps at pose H after `warmup` untimed ones, with the images' features
  * resident on the GPU and an L2 flush between timed maps (outside the timed spans). flags: 1
  * exact, 2 calibrated; cap as zc_shift_map (0: 1024). out[16] (out_len ≥ 16): [0] ms per map
- * (CUDA events), [1..5] per-stage ms (canvas, forward rows, forward columns, inverse columns,
- * inverse rows + score), [7] canvas height, [8..15] nx, ny, cw, ch, real planes, correlations,
- * row split, canvas width. 0 / -1 with zc_error. */
+ * (CUDA events around replays of one CUDA graph of the map's passes; the instrumented maps' time
+ * when the graph cannot be captured), [1..5] per-stage ms of event-instrumented maps (canvas,
+ * forward rows, forward columns, inverse columns, inverse rows + score), [6] ms per instrumented
+ * map, [7] canvas height, [8..15] nx, ny, cw, ch, real planes, correlations, row split, canvas
+ * width. 0 / -1 with zc_error. */
 int32_t zcb_bench_maps(zc_engine* e, const double H[9], uint32_t flags, uint32_t cap, uint32_t warmup, uint32_t steps,
                        double* out, size_t out_len);
 

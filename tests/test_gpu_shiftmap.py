@@ -232,3 +232,21 @@ def test_row_pass_tensor_memory_matches_split(monkeypatch, n, cap):
         floor = (A.map == 0) != (B.map == 0)
         assert floor.mean() < 1e-4
         assert np.max(np.abs(A.map - B.map)[~floor]) <= 1e-5 * max(abs(A.peak), 1.0)
+
+
+def test_bench_maps_graph_replay_leaves_the_map_unchanged(c1_pair):
+    """zcb_bench_maps times replays of one captured CUDA graph of the map's passes (and
+    event-instrumented maps for the stages): the timings are sane and a map computed after the
+    replays is the map computed before them, value for value."""
+    m, f, H = c1_pair
+    with zc.Registrar(half=False) as reg:
+        reg.set_images(m, f, preprocess=False)
+        before = reg.shift_map(H, exact=True, calibrated=True, resolution=512)
+        r = reg.bench_maps(H, flags=3, cap=512, warmup=2, steps=4)
+        after = reg.shift_map(H, exact=True, calibrated=True, resolution=512)
+        ev = [e["text"] for e in reg.events() if e.get("kind") == "log"]
+    assert 0 < r["ms_per_map"] <= 1.5 * r["ms_per_map_instrumented"], r
+    assert abs(sum(r["stages_ms"].values()) - r["ms_per_map_instrumented"]) <= 0.05 * r["ms_per_map_instrumented"]
+    assert not any("graph replay unavailable" in t for t in ev), ev
+    assert (after.dx, after.dy, after.peak_index) == (before.dx, before.dy, before.peak_index)
+    np.testing.assert_array_equal(after.map, before.map)

@@ -503,8 +503,9 @@ class Registrar:
         return dict(zip(("launches", "submits", "reads", "waits"), list(out)))
 
     def bench_maps(self, H=None, *, flags=3, cap=1024, warmup=3, steps=10):
-        """Device-timed maps (CUDA events, inputs resident, L2 flushed between timed maps):
-        ms per map, per-stage ms and the plan."""
+        """Device-timed maps (CUDA events, inputs resident, L2 flushed between timed maps): ms per
+        map of replays of one captured CUDA graph of the map's passes, per-stage ms (and the total)
+        of event-instrumented maps, and the plan."""
         a, p = self._Hp(H)
         out = np.zeros(16, np.float64)
         self._check(self._lib.zcb_bench_maps(self._e, p, flags, cap, warmup, steps, out.ctypes.data_as(_native.f64p), 16),
@@ -512,6 +513,7 @@ class Registrar:
         stages = ("canvas", "fwd_rows", "fwd_cols", "inv_cols", "inv_rows_score")
         return {
             "ms_per_map": float(out[0]), "stages_ms": dict(zip(stages, map(float, out[1:6]))),
+            "ms_per_map_instrumented": float(out[6]),
             "nx": int(out[8]), "ny": int(out[9]), "cw": int(out[10]), "ch": int(out[11]),
             "n_real": int(out[12]), "n_corr": int(out[13]), "split": int(out[14]), "canvas_w": int(out[15]),
             "canvas_h": int(out[7]),

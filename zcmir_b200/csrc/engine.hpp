@@ -238,6 +238,9 @@ class Engine {
     bool stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,
                     bool calibrated, unsigned cap, zc_shift_result* out, float* ms);
     // benchmark: warmup + steps maps at H (device-resident inputs), per-step CUDA-event times
+    // ms per map of `steps` replays of one captured CUDA graph of job's passes (an L2 flush
+    // before each); -1 when the capture or its replay is refused
+    double graph_maps(MapJob& job, unsigned warmup, unsigned steps, size_t flush_bytes);
     bool bench_maps(const Mat3& H, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
                     size_t out_len);
 
