@@ -66,9 +66,12 @@ int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, con
  * gave the GPU's free memory to its own pool can see that allocation fail. The scratch is one
  * file-scope device array of 103,936 bytes: n ≤ 64 (larger n is rejected with an error), and
  * calls that overlap in time (any engines on the same device) race on it; it keeps the last
- * call's contents. The first call on each device looks up the array's address (make it before
- * any stream capture begins). The feature planes must already be built for the current
- * settings (by zc_set_image_gray, zc_score or zc_features); otherwise -1 with zc_error. 0 / -1. */
+ * call's contents. zc_create looks up the array's address on its device, which (with lazy module
+ * loading) loads the module holding it and so reserves its bytes then, not in a call; only if that
+ * look-up failed does the first call on the device retry it (make that call before any stream
+ * capture begins). The feature planes must already be built for the current settings (by
+ * zc_set_image_gray, zc_score or zc_features), else -1 with zc_error; a side still building on a
+ * stream of its own is waited for on the engine's stream. 0 / -1. */
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out);
 
 /* Gauss–Newton from each of n poses (Hs, row-major 3×3 each) at once for `iters` steps of the

@@ -52,12 +52,12 @@ def _engine(lib, settings):
     return e
 
 
-def _set_images(lib, e):
+def _set_images(lib, e, preprocess=0):
     m, f, H = synth.pair_remap(n=256, shift=(17, -9), seed=0)
     for side, img in ((0, m), (1, f)):
         a = np.ascontiguousarray(img, dtype=np.float32)
         h, w = a.shape
-        rc = lib.zc_set_image_gray(e, side, a.ctypes.data_as(_native.f32p), w, h, 0)
+        rc = lib.zc_set_image_gray(e, side, a.ctypes.data_as(_native.f32p), w, h, preprocess)
         assert rc == 0, _err(lib, e)
     return H
 
@@ -113,6 +113,22 @@ def test_static_scores_match_zc_score_twice(lib, symmetric):
         lib.zc_destroy(e)
 
 
+def test_static_scores_right_after_the_images(lib):
+    """The first call after zc_set_image_gray, with no zc_score before it: side 1's planes build on
+    a stream of their own, and the call must wait for that build rather than read planes still
+    being written."""
+    for rep in range(2):
+        e = _engine(lib, {"half": False, "symmetric": True})
+        try:
+            H = _set_images(lib, e)
+            Hs = _poses(H, 16, seed=11 + rep)
+            first = _static_scores(lib, e, Hs)
+            ref = _reference_scores(lib, e, Hs)
+            _check(first, ref, True)
+        finally:
+            lib.zc_destroy(e)
+
+
 def test_static_scores_refusals(lib):
     e = _engine(lib, {"half": False})
     try:
@@ -124,11 +140,32 @@ def test_static_scores_refusals(lib):
         _set_images(lib, e)
         rc = lib.zcb_score_static(e, Hs.ctypes.data_as(_native.f64p), MAX_POSES + 1, out.ctypes.data_as(_native.f64p))
         assert rc == -1 and "maximum of 64" in _err(lib, e)
+        # a count past 2^31 is refused for its size too (it is checked before anything is read)
+        rc = lib.zcb_score_static(e, Hs.ctypes.data_as(_native.f64p), 2**31 + 5, out.ctypes.data_as(_native.f64p))
+        assert rc == -1 and "maximum of 64" in _err(lib, e)
         # an empty batch is a no-op
         assert lib.zcb_score_static(e, Hs.ctypes.data_as(_native.f64p), 0, out.ctypes.data_as(_native.f64p)) == 0
         # settings that change the feature planes leave them unbuilt: refused, not rebuilt
         js = json.dumps({"smi_features": "three"}).encode()
         assert lib.zc_configure(e, js, len(js)) == 0, _err(lib, e)
+        rc = lib.zcb_score_static(e, Hs.ctypes.data_as(_native.f64p), 1, out.ctypes.data_as(_native.f64p))
+        assert rc == -1 and "not built" in _err(lib, e)
+    finally:
+        lib.zc_destroy(e)
+
+
+def test_static_scores_refuse_stale_preprocessing(lib):
+    """Planes baked with one preprocessing (CLAHE) are stale once a preprocessing setting changes:
+    the call refuses instead of scoring them (zc_score would re-bake)."""
+    e = _engine(lib, {"half": False})
+    try:
+        H = _set_images(lib, e, preprocess=1)
+        Hs = np.ascontiguousarray(H.reshape(1, 9))
+        ref = _reference_scores(lib, e, Hs.reshape(1, 3, 3))
+        _check(_static_scores(lib, e, Hs), ref, True)
+        js = json.dumps({"clahe_grid": 8}).encode()
+        assert lib.zc_configure(e, js, len(js)) == 0, _err(lib, e)
+        out = np.zeros((1, 3))
         rc = lib.zcb_score_static(e, Hs.ctypes.data_as(_native.f64p), 1, out.ctypes.data_as(_native.f64p))
         assert rc == -1 and "not built" in _err(lib, e)
     finally:

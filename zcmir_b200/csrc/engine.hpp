@@ -153,6 +153,10 @@ struct SideSwap {
 enum Stage { kCanvas = 0, kFwdRows, kFwdCols, kInvCols, kInvRows, kNumStages };
 extern const char* const kStageNames[kNumStages];
 
+// Looks up zcb_score_static's file-scope device array on device dev (score_static.cu); zc_create
+// calls it once per engine, so the calls themselves reserve nothing.
+void static_scratch_setup(int dev);
+
 class Engine {
   public:
     explicit Engine(int device);
@@ -252,7 +256,7 @@ class Engine {
     bool moments(const Mat3& H, double* out45);
     bool score3(const Mat3& H, double* out3);
     // scores of n ≤ 64 poses with every device buffer in a file-scope array (score_static.cu)
-    bool score_static(const double* Hs, int n, double* out3);
+    bool score_static(const double* Hs, uint32_t n, double* out3);
     bool gradient(const Mat3& H, bool hess, zc_grad_result* out);
     bool climb(zc_climb_result* out);
 

@@ -79,7 +79,11 @@ zc_engine* zc_create(const char* /*wgpu_path: the reference's WebGPU library, un
     int dev = 0;
     cudaGetDevice(&dev);
     try {
-        return new zc_engine(dev);
+        zc_engine* eng = new zc_engine(dev);
+        // the no-allocation pose scores' device array: looked up (its module loaded) here, once
+        // per device, so that zcb_score_static itself reserves nothing
+        zc::static_scratch_setup(dev);
+        return eng;
     } catch (const std::exception& x) {
         const std::string m = std::string("engine init failed: ") + x.what();
         g_create_err_len = copy_out(m, g_create_err, sizeof g_create_err);
@@ -430,7 +434,7 @@ int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, con
 
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out) {
     // allocates no device memory: the scratch is a file-scope array (score_static.cu)
-    return guarded(e, "score_static", [&] { return e->score_static(Hs, (int)n, out); });
+    return guarded(e, "score_static", [&] { return e->score_static(Hs, n, out); });
 }
 
 }  // extern "C"

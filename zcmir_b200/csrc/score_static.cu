@@ -17,9 +17,13 @@
 // zc_features and zc_set_image_gray build them); building them allocates, so this call refuses
 // rather than build.
 //
-// Set-up: the first call on each device looks up the array's device address with
-// cudaGetSymbolAddress, with that device current. Make that first call before any stream
-// capture begins.
+// Set-up: the array's device address is looked up with cudaGetSymbolAddress, with the device
+// current, once per device. zc_create does this for its device, so the first call of an engine
+// made there needs no set-up; only an engine whose device was never set up (its look-up at
+// creation failed) does it on its first call, which should then come before any stream capture
+// begins. With lazy module loading (the CUDA 12 default) the look-up is what loads the module that
+// holds the array, and so what reserves its 103,936 bytes on the device: at creation, not in a
+// call.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -77,12 +81,20 @@ cudaError_t scratch_on(int dev, unsigned char** out) {
 
 namespace zc {
 
-bool Engine::score_static(const double* Hs, int n, double* out3) {
-    if (n < 0 || (n > 0 && (!Hs || !out3))) return fail("score_static: null poses or output");
-    if (n > kMaxPoses)
-        return fail("score_static: " + std::to_string(n) + " poses exceed the static scratch's maximum of " +
+// Called by zc_create for the engine's device: looks the array up (and so loads its module)
+// before any call needs it. A failure here is not fatal; the first call retries and reports it.
+void static_scratch_setup(int dev) {
+    unsigned char* p = nullptr;
+    (void)scratch_on(dev, &p);
+}
+
+bool Engine::score_static(const double* Hs, uint32_t n_poses, double* out3) {
+    if (n_poses > (uint32_t)kMaxPoses)
+        return fail("score_static: " + std::to_string(n_poses) + " poses exceed the static scratch's maximum of " +
                     std::to_string(kMaxPoses) + " per call; score them in chunks of at most " +
                     std::to_string(kMaxPoses));
+    const int n = (int)n_poses;
+    if (n > 0 && (!Hs || !out3)) return fail("score_static: null poses or output");
     if (!side[0].has || !side[1].has) return fail("NoImages");
     if (set.e("metric") != "smi")
         return fail("score_static: metric \"" + set.e("metric") + "\" is not part of this build's SMI path");
@@ -90,10 +102,14 @@ bool Engine::score_static(const double* Hs, int n, double* out3) {
     const std::string& fm = set.e("smi_features");
     const int mode = fm == "laplacian" ? 0 : (fm == "three" ? 1 : 2);
     for (const Side& sd : side)
-        if (!sd.built || sd.mode != mode || sd.half != set.b("half"))
+        if (!sd.built || sd.mode != mode || sd.half != set.b("half") || (sd.preprocess && sd.bake != bake_key()))
             return fail(
                 "score_static: the feature planes are not built for the current settings; building them "
                 "allocates device memory, so call zc_score or zc_features once first");
+    // A side whose build ran on a stream of its own (side 1 after zc_set_image_gray) may still be
+    // writing its planes: the engine stream waits for that build's event. Only stream waits are
+    // issued here, nothing is allocated.
+    if (!join_side(0) || !join_side(1)) return false;
     if (n == 0) return true;
     unsigned char* base = nullptr;
     if (!cuda_ok(scratch_on(device, &base), "score_static: scratch set-up")) return false;
