@@ -6,8 +6,8 @@ One step = one full shift map of the pair at the identity pose (canvas → both 
 → forward FFTs → 45 correlation products → inverse FFTs → per-shift exact, calibrated score →
 argmax), the images' features resident in HBM. Device time per step is taken with CUDA events
 on the engine's stream, W untimed steps first, an L2 flush (a 256 MB write) between timed steps
-outside the timed spans. `e2e` is the same metric through the public API (Registrar.set_images
-from pinned host buffers + Registrar.shift_map copying the map back to pinned host memory).
+outside the timed spans. `e2e` is the same metric through the public API (Engine.set_images
+from pinned host buffers + Engine.shift_map copying the map back to pinned host memory).
 
 The path does not shard (one map needs all 45 correlations of every shift): N GPUs run N
 independent replicas, one process each (torchrun), and `value` is the maps/s of all ranks, timed
@@ -309,13 +309,13 @@ def run_stack(reg_cls, args, barrier, dist, torch, ws):
     imgs = [(s / 65535.0).astype(np.float32) for s in slices]
     reg = reg_cls(half=False)
     for _ in range(args.warmup):
-        reg.stack_maps(imgs, exact=True, calibrated=False, resolution=1024)
+        reg.stack_maps(imgs, exact=True, calibrated=False, cap=1024)
     barrier()
     t0 = time.perf_counter()
     n_steps = max(3, args.steps // 5)
     ms = []
     for _ in range(n_steps):
-        maps, m = reg.stack_maps(imgs, exact=True, calibrated=False, resolution=1024)
+        maps, m = reg.stack_maps(imgs, exact=True, calibrated=False, cap=1024)
         ms.append(m)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / n_steps
@@ -337,7 +337,7 @@ def run_stack(reg_cls, args, barrier, dist, torch, ws):
            "centre_error_px": {"median": float(np.median(errs)), "max": float(np.max(errs))},
            "e2e": {"value": ws * 31 / e2e_s, "unit": "maps/s", "seconds_per_stack": e2e_s,
                    "h2d_bytes_per_step": int(sum(a.nbytes for a in imgs)), "d2h_bytes_per_step": 31 * 88,
-                   "what": "Registrar.stack_maps from host slices: 32 uploads, 32 feature builds, 31 maps"}}
+                   "what": "Engine.stack_maps from host slices: 32 uploads, 32 feature builds, 31 maps"}}
     reg.close()
     return out, imgs
 
@@ -389,9 +389,9 @@ def run_gpu(args, rank, ws, local):
     import zcmir_b200 as zc
 
     m, f, H = make_pair()
-    reg = zc.Registrar(half=False)
+    reg = zc.Engine(half=False)
     reg.set_images(m, f, preprocess=False)
-    sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048)
+    sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=2048)
     assert (sm.dx, sm.dy) == (-H[0, 2], -H[1, 2]), (sm.dx, sm.dy, H)
 
     # device-timed maps: the 45-correlation workload, and the 28-correlation ("none") one
@@ -423,12 +423,12 @@ def run_gpu(args, rank, ws, local):
     out = torch.empty(2048 * 2048, dtype=torch.float32, pin_memory=True).numpy()
     for _ in range(args.warmup):
         reg.set_images(pm, pf, preprocess=False)
-        reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048, out=out)
+        reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=2048, out=out)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         reg.set_images(pm, pf, preprocess=False)
-        e = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048, out=out)
+        e = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=2048, out=out)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / args.steps
     if dist:
@@ -478,11 +478,11 @@ def run_gpu(args, rank, ws, local):
             line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "maps/s", "cores": os.cpu_count(), "kind": "port",
                                     "sample": "one full 1024² map of the same pair (float64 oracle, scipy FFTs)"}
     reg.close()
-    sweep, sm_, sf_ = run_sweep(zc.Registrar, args, barrier, dist, torch, ws)
-    stack, st_imgs = run_stack(zc.Registrar, args, barrier, dist, torch, ws)
+    sweep, sm_, sf_ = run_sweep(zc.Engine, args, barrier, dist, torch, ws)
+    stack, st_imgs = run_stack(zc.Engine, args, barrier, dist, torch, ws)
     from zcmir_b200 import synth
 
-    proposal = run_proposal(zc.Registrar, sm_, sf_, synth.pair_similarity(n=512, seed=2)[2])
+    proposal = run_proposal(zc.Engine, sm_, sf_, synth.pair_similarity(n=512, seed=2)[2])
     if rank == 0:
         if ws == 1 and not args.no_cpu:
             v, n = sweep_cpu_sample(sm_, sf_)

@@ -144,11 +144,16 @@ def sweep_setup(mw, mh, fw, fh, H0, gv, G=128, sizes="ladder"):
             "fixed_taps": float(min(6, max(1, math.ceil(cell - 1e-3)))), "cands": cands, "perm": perm}
 
 
-def pack_window(stack, Hinv, taps, gx0, gy0, win_x, win_y, nx, ny, ox, oy, cell, G):
+def pack_window(stack, Hinv, taps, gx0, gy0, win_x, win_y, nx, ny, ox, oy, cell, G, f32_positions=False):
     """(5, ny, nx) premultiplied samples of a window of canvas cells at the plane origin
     (``shaders/sweep.wgsl:62-152``): each cell the mean of k×k bilinear taps of the source stack
     mapped through Hinv (dest → source, 1-based); a tap whose 2×2 footprint leaves the image adds
-    nothing. Zero outside the window and the G×G canvas."""
+    nothing. Zero outside the window and the G×G canvas.
+
+    f32_positions: the tap positions (px, py, the mapped qx, qy, qz and x = qx/qz − 1) in float32,
+    one rounding per operation, as the reference's shader computes them
+    (``shaders/sweep.wgsl:132-138``); the interpolation stays float64. A tap within ~1e-4 px of
+    the image's edge enters or leaves with that rounding, and its whole sample with it."""
     src = np.asarray(stack, np.float64)
     h, w = src.shape[1:]
     k = max(int(taps), 1)
@@ -158,16 +163,27 @@ def pack_window(stack, Hinv, taps, gx0, gy0, win_x, win_y, nx, ny, ox, oy, cell,
     inside = (cx < G) & (cy < G)
     acc = np.zeros((5,) + xx.shape)
     Hi = np.asarray(Hinv, np.float64).reshape(3, 3)
+    if f32_positions:
+        F = np.float32
+        Hi = Hi.astype(F)
+        cxf, cyf, kf, oxf, oyf, cellf = cx.astype(F), cy.astype(F), F(k), F(ox), F(oy), F(cell)
     for ty in range(k):
-        py = oy + (cy + (ty + 0.5) / k) * cell
+        if f32_positions:
+            py = oyf + (cyf + (F(ty) + F(0.5)) / kf) * cellf
+        else:
+            py = oy + (cy + (ty + 0.5) / k) * cell
         for tx in range(k):
-            px = ox + (cx + (tx + 0.5) / k) * cell
+            if f32_positions:
+                px = oxf + (cxf + (F(tx) + F(0.5)) / kf) * cellf
+            else:
+                px = ox + (cx + (tx + 0.5) / k) * cell
             qx = Hi[0, 0] * px + Hi[0, 1] * py + Hi[0, 2]
             qy = Hi[1, 0] * px + Hi[1, 1] * py + Hi[1, 2]
             qz = Hi[2, 0] * px + Hi[2, 1] * py + Hi[2, 2]
             okz = np.abs(qz) >= 1e-8
-            qzs = np.where(okz, qz, 1.0)
-            x, y = qx / qzs - 1.0, qy / qzs - 1.0
+            qzs = np.where(okz, qz, qz.dtype.type(1))
+            x, y = qx / qzs - qz.dtype.type(1), qy / qzs - qz.dtype.type(1)
+            x, y = x.astype(np.float64), y.astype(np.float64)
             x0, y0 = np.floor(x), np.floor(y)
             ok = okz & (x0 >= 0) & (y0 >= 0) & (x0 + 1 < w) & (y0 + 1 < h) & inside
             fx, fy = x - x0, y - y0
@@ -188,13 +204,13 @@ def zero_lag(c, setup):
     return ly * c["nx"] + lx
 
 
-def candidate_map(prep_a, prep_b, setup, c, exact=True, three=False, min_n=12):
+def candidate_map(prep_a, prep_b, setup, c, exact=True, three=False, min_n=12, f32_positions=False):
     """One candidate's shift map (ny × nx, cell units, float64) and its zero-lag overlap."""
     nx, ny, Fx, Fy = c["nx"], c["ny"], setup["Fx"], setup["Fy"]
     sa = pack_window(prep_a["stack"], np.linalg.inv(c["H"]), c["taps"], c["gx0"], c["gy0"], nx - Fx + 1, ny - Fy + 1,
-                     nx, ny, setup["ox"], setup["oy"], setup["cell"], setup["G"])
+                     nx, ny, setup["ox"], setup["oy"], setup["cell"], setup["G"], f32_positions)
     sb = pack_window(prep_b["stack"], np.eye(3), setup["fixed_taps"], setup["fcx"][0], setup["fcy"][0], Fx, Fy, nx, ny,
-                     setup["ox"], setup["oy"], setup["cell"], setup["G"])
+                     setup["ox"], setup["oy"], setup["cell"], setup["G"], f32_positions)
     ids, corrs = O.corr_plan(exact, three)
     corr = O.correlations(O.real_planes(sa, ids), O.real_planes(sb, ids), ids, corrs, nx, ny)
     n0 = corr[0].ravel()[zero_lag(c, setup)]
@@ -244,9 +260,10 @@ def min_count(min_overlap, fw, fh, cell):
 
 
 def sweep(prep_a, prep_b, H0, gv, G=128, exact=True, three=False, min_overlap=0.05, n_peak=4, sizes="ladder",
-          only=None):
+          only=None, f32_positions=False):
     """Every candidate's peaks (slot order, as the reference appends them) and each candidate's
-    best score; ``only``: restrict to these candidate indices (for small checks)."""
+    best score; ``only``: restrict to these candidate indices (for small checks);
+    ``f32_positions``: the taps placed in float32 as the reference places them (pack_window)."""
     mh, mw = prep_a["stack"].shape[1:]
     fh, fw = prep_b["stack"].shape[1:]
     st = sweep_setup(mw, mh, fw, fh, H0, gv, G, sizes)
@@ -258,7 +275,7 @@ def sweep(prep_a, prep_b, H0, gv, G=128, exact=True, three=False, min_overlap=0.
         if only is not None and ci not in only:
             continue
         c = st["cands"][ci]
-        m, _ = candidate_map(prep_a, prep_b, st, c, exact, three, min_n)
+        m, _ = candidate_map(prep_a, prep_b, st, c, exact, three, min_n, f32_positions)
         top = lane_peaks(m, n_peak)
         raw[ci] = top
         for k, (v0, t) in enumerate(top):

@@ -30,7 +30,7 @@ def test_ncc_score_and_map_match_oracle(half, crop):
         m = m[: crop[0], : crop[1]]
         f = f[:190, :170]
     H = _turn(H, 3.0, 1.02, (100.5, 80.5))
-    with zc.Registrar(half=half, metric="ncc") as reg:
+    with zc.Engine(half=half, metric="ncc") as reg:
         reg.set_images(np.clip(m, 0, 1), np.clip(f, 0, 1), preprocess=False)
         wa, wb = reg.work_image(0), reg.work_image(1)
         sc = reg.score(H)
@@ -57,7 +57,7 @@ def test_ncc_map_finds_a_planted_shift():
     fixed = big[40:340, 40:340]
     tx, ty = -19, 12
     moving = big[40 - ty:340 - ty, 40 - tx:340 - tx]
-    with zc.Registrar(half=False, metric="ncc") as reg:
+    with zc.Engine(half=False, metric="ncc") as reg:
         reg.set_images(moving.astype(np.float32), fixed.astype(np.float32), preprocess=False)
         sm = reg.shift_map(np.eye(3))
         s0 = reg.score(np.eye(3)).mean
@@ -73,7 +73,7 @@ def test_ncc_metric_leaves_the_smi_paths(golden):
     (tests/test_api.py:144): |score| ≤ 1 at the landsat-b truth."""
     d = np.load(golden / "landsat_b.npz")
     mv, fx, truth = d["moving"], d["fixed"], d["truth"]
-    with zc.Registrar(metric="ncc") as reg:
+    with zc.Engine(metric="ncc") as reg:
         reg.set_images(mv, fx)
         s = reg.score(truth).mean
         g_ncc = reg.gradient(truth)

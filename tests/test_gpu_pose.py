@@ -43,7 +43,7 @@ def test_moments_score_gradient_match_oracle(pair, group):
     m, f, H = pair
     Hp = _near(H)
     homog = group == "homography"
-    with zc.Registrar(half=False, group=group) as reg:
+    with zc.Engine(half=False, group=group) as reg:
         reg.set_images(m, f, preprocess=False)
         A, B = reg.features(0), reg.features(1)
         mom = reg.moments(Hp)
@@ -68,7 +68,7 @@ def test_ragged_images_match_oracle(pair):
     m, f, H = pair
     m2, f2 = np.ascontiguousarray(m[3:160, 5:208]), np.ascontiguousarray(f[:139, 2:183])
     Hp = _near(H)
-    with zc.Registrar(half=False, group="affine") as reg:
+    with zc.Engine(half=False, group="affine") as reg:
         reg.set_images(m2, f2, preprocess=False)
         A, B = reg.features(0), reg.features(1)
         mom = reg.moments(Hp)
@@ -84,7 +84,7 @@ def test_ragged_images_match_oracle(pair):
 
 def test_forward_only_and_edge_cases(pair):
     m, f, H = pair
-    with zc.Registrar(half=False, symmetric=False) as reg:
+    with zc.Engine(half=False, symmetric=False) as reg:
         reg.set_images(m, f, preprocess=False)
         A, B = reg.features(0), reg.features(1)
         s = reg.score(H)
@@ -112,7 +112,7 @@ def test_climb_recovers_pose_and_gn_step_is_small(golden):
     mh, mw = m.shape
     assert corner_dist(start, H, mw, mh) > 5
     for group in ("homography", "affine"):
-        with zc.Registrar(half=False, group=group) as reg:
+        with zc.Engine(half=False, group=group) as reg:
             reg.set_images(m, f, preprocess=False)
             reg.pose = start
             c = reg.climb()
@@ -133,7 +133,7 @@ def test_climb_ascends_to_a_stationary_point(pair):
     shift: perspective terms trade overlap on this small pair)."""
     m, f, H = pair
     start = _near(H, th=2.0, s=1.015, t=(2.0, -1.5))
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         s0 = reg.score(start).mean
         reg.pose = start
@@ -159,7 +159,7 @@ def test_climb_roto_scale_hop(golden):
     T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
     start = T(*c) @ R @ T(*-c) @ H
     assert corner_dist(start, H, mw, mh) > 30
-    with zc.Registrar(half=False, group="affine", hop_fm=True) as reg:
+    with zc.Engine(half=False, group="affine", hop_fm=True) as reg:
         reg.set_images(m, f, preprocess=False)
         reg.pose = start
         r = reg.climb()

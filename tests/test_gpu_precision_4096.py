@@ -43,9 +43,9 @@ def lags(rng, planted):
 def test_precision_study_4096():
     m, f, H = synth.pair_segmented(n=N, seed=4, max_shift=800)
     planted = (int(-H[0, 2]), int(-H[1, 2]))
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
-        sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=8192)
+        sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=8192)
         fa, fb = reg.features(0), reg.features(1)
     assert (sm.n, sm.ny, sm.cw, sm.ch) == (8192, 8192, N, N)
     assert (sm.dx, sm.dy) == planted

@@ -30,7 +30,7 @@ def rgba_of(u8):
 def test_clahe_work_image_is_bit_exact(landsat, half):
     mv, fx, _ = landsat
     crop = mv[:333, :517]  # sizes that the 4×4 tiles do not divide: the reflected padding
-    with zc.Registrar(half=half) as reg:
+    with zc.Engine(half=half) as reg:
         reg.set_images(crop, fx)
         got = reg.work_image(0)
         s = reg.settings
@@ -44,7 +44,7 @@ def test_band_pass_and_invert(clahe, half):
     m = m[:, :131]
     settings = dict(clahe=clahe, band=True, bp_fine=1.5, bp_coarse=3.0, invert=True, half=half, clahe_grid=6,
                     clahe_bins=100)
-    with zc.Registrar(**settings) as reg:
+    with zc.Engine(**settings) as reg:
         reg.set_images(np.clip(m, 0, 1), np.clip(f, 0, 1), preprocess=True)
         got = reg.work_image(0)
         s = reg.settings
@@ -57,7 +57,7 @@ def test_band_pass_and_invert(clahe, half):
 def test_rgb_to_gray_and_rebake(landsat):
     mv, fx, _ = landsat
     rgb = np.stack([mv, np.roll(mv, 3, axis=1), 255 - mv], axis=2)
-    with zc.Registrar(half=False, clahe=False) as reg:
+    with zc.Engine(half=False, clahe=False) as reg:
         reg.set_images(rgb, fx)
         np.testing.assert_array_equal(reg.work_image(0), P.rgba_gray(rgb))
         # a preprocessing setting changes the work image the next time it is needed
@@ -75,11 +75,11 @@ def test_known_answers_in_the_reference_setup(landsat):
     of (14, −9), and the roto-scale map of the truth turned by 6° and scaled by 1.08 within 2°."""
     mv, fx, truth = landsat
     T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
-    with zc.Registrar(symmetric=False) as reg:
+    with zc.Engine(symmetric=False) as reg:
         reg.set_images(mv, fx)
         sm = reg.shift_map(T(14, -9) @ truth, exact=True, calibrated=False)
         assert np.hypot(sm.dx - 14, sm.dy + 9) < 2, (sm.dx, sm.dy)
-        c = reg.rs_map(truth, return_maps=False).center
+        c = reg.rs_map(truth, want_maps=False).center
         a = np.deg2rad(6)
         turn = np.array([[1.08 * np.cos(a), -1.08 * np.sin(a), 0], [1.08 * np.sin(a), 1.08 * np.cos(a), 0], [0, 0, 1]])
         r = reg.rs_map(T(*c) @ turn @ T(-c[0], -c[1]) @ truth)

@@ -72,7 +72,7 @@ def test_trained_network_gains_over_the_landscape_alone():
     maps)."""
     import zcmir_b200 as zc
     net = P.Network.load()
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         x, y = P.dataset(reg, range(200_000, 200_048))
         top = np.argsort(-net.logits(x), axis=1)
         base = []

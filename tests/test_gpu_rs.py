@@ -50,7 +50,7 @@ def check(g, o, n0, tight=1e-4, loose=1e-2):
 @pytest.mark.parametrize("calibrated", [False, True])
 def test_rs_map_matches_oracle(calibrated):
     m, f, H = synth.pair_remap(n=192, shift=(6, -4), seed=2)
-    with zc.Registrar(half=False, calibrated=calibrated) as reg:
+    with zc.Engine(half=False, calibrated=calibrated) as reg:
         reg.set_images(m, f, preprocess=False)
         Hp = turned((96.5, 96.5), 9.0, 1.05, H)
         r = reg.rs_map(Hp)
@@ -77,18 +77,18 @@ def test_rs_map_matches_oracle(calibrated):
 def test_rs_known_answers(golden):
     d = np.load(golden / "landsat_b.npz")
     truth = d["truth"]
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(d["moving"].astype(np.float32) / 255, d["fixed"].astype(np.float32) / 255, preprocess=False)
-        c = reg.rs_map(truth, return_maps=False).center
+        c = reg.rs_map(truth, want_maps=False).center
         r = reg.rs_map(turned(c, 6.0, 1.08, truth))
         assert abs(-np.rad2deg(r.dth) - 6) < 2 and abs(np.exp(-r.dsg) - 1.08) < 0.03
-        t = reg.rs_map(truth, return_maps=False)
+        t = reg.rs_map(truth, want_maps=False)
         assert abs(t.dth) < 0.02 and abs(t.dsg) < 0.02
 
 
 def test_rs_one_sided_and_scale_mask():
     m, f, H = synth.pair_remap(n=128, shift=(3, 2), seed=3)
-    with zc.Registrar(half=False, rs_smin=0.9, rs_smax=1.1) as reg:
+    with zc.Engine(half=False, rs_smin=0.9, rs_smax=1.1) as reg:
         reg.set_images(m, f, preprocess=False)
         one = reg.rs_map(H, symmetric=False)
         assert not one.symmetric and one.inv is None

@@ -46,7 +46,7 @@ def c1_pair():
 
 def test_features_match_oracle(c1_pair):
     m, f, _ = c1_pair
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         for side, img in ((0, m), (1, f)):
             gpu = reg.features(side)
@@ -59,7 +59,7 @@ def test_features_match_oracle(c1_pair):
 def test_features_half_and_modes(c1_pair):
     m, f, _ = c1_pair
     for mode in ("three", "cubic"):
-        with zc.Registrar(half=True, smi_features=mode) as reg:
+        with zc.Engine(half=True, smi_features=mode) as reg:
             reg.set_images(m, f, preprocess=False)
             gpu = reg.features(1)
             ora = O.prepare(f, mode, half=True)["feat"]
@@ -72,10 +72,10 @@ def test_features_half_and_modes(c1_pair):
 def test_c1_map_exact_uncalibrated(c1_pair):
     """The 256² map workload: 45 correlations zero-padded to 512², exact whitening, no calibration."""
     m, f, H = c1_pair
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
-        sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=1024)
+        sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=1024)
     ref = O.shift_map(pa, pb, np.eye(3), exact=True, calibrated=False, cap=1024, return_corr=True)
     assert (sm.n, sm.ny, sm.cw, sm.ch) == (512, 512, 256, 256)
     check_map(sm, ref, ref["corr"][0])
@@ -88,10 +88,10 @@ def test_c1_map_variants(c1_pair):
     m, f, _ = c1_pair
     for kw, mode in (({"exact": False, "calibrated": False}, "laplacian"), ({"exact": True, "calibrated": True}, "laplacian"),
                      ({"exact": True, "calibrated": False}, "three")):
-        with zc.Registrar(half=False, smi_features=mode) as reg:
+        with zc.Engine(half=False, smi_features=mode) as reg:
             reg.set_images(m, f, preprocess=False)
             pa, pb = prep_from(reg.features(0), mode), prep_from(reg.features(1), mode)
-            sm = reg.shift_map(np.eye(3), resolution=1024, **kw)
+            sm = reg.shift_map(np.eye(3), cap=1024, **kw)
         ref = O.shift_map(pa, pb, np.eye(3), cap=1024, return_corr=True, **kw)
         check_map(sm, ref, ref["corr"][0])
 
@@ -102,7 +102,7 @@ def test_settings_map_auto_resolution(golden):
     d = np.load(golden / "landsat_b.npz")
     m, f = d["moving"].astype(np.float32) / 255, d["fixed"].astype(np.float32) / 255
     H0 = np.array([[1, 0, 14], [0, 1, -9], [0, 0, 1.0]]) @ d["truth"]
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
         sm = reg.shift_map(H0)
@@ -121,10 +121,10 @@ def test_landsat_full_resolution_ladder_fft(golden):
     d = np.load(golden / "landsat_b.npz")
     m, f = d["moving"].astype(np.float32) / 255, d["fixed"].astype(np.float32) / 255
     H0 = np.array([[1, 0, 14], [0, 1, -9], [0, 0, 1.0]]) @ d["truth"]
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
-        sm = reg.shift_map(H0, exact=True, calibrated=False, resolution=2048)
+        sm = reg.shift_map(H0, exact=True, calibrated=False, cap=2048)
     assert (sm.n, sm.cw) == (1944, 917)
     assert (sm.dx, sm.dy) == (14.0, -9.0)
     ref = O.shift_map(pa, pb, H0, exact=True, calibrated=False, cap=2048, return_corr=True)
@@ -136,12 +136,12 @@ def test_segmented_1024_full_size_properties():
     map at a spread of lags equals the score of the FFT-free float64 direct sums of the same
     planes (the GPU's own features)."""
     m, f, H = synth.pair_segmented(n=1024, seed=1)
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
-        sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=2048)
+        sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=2048)
         area = sm.corr_area_px
-        sm3 = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=2048)
+        sm3 = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=2048)
     assert (sm.n, sm.ny, sm.cw) == (2048, 2048, 1024)
     assert (sm.dx, sm.dy) == (-H[0, 2], -H[1, 2])
     assert (sm3.dx, sm3.dy) == (-H[0, 2], -H[1, 2])
@@ -165,15 +165,15 @@ def test_segmented_1024_full_size_properties():
 
 
 def test_errors_and_boundaries():
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         with pytest.raises(RuntimeError, match="NoImages"):
             reg.shift_map(np.eye(3), exact=True)
         with pytest.raises(RuntimeError, match="BadImage"):
-            reg.set_moving(np.zeros((4, 64), np.float32), preprocess=False)
+            reg.set_image(0, np.zeros((4, 64), np.float32), preprocess=False)
         with pytest.raises(RuntimeError, match="UnknownSetting"):
             reg.configure(nope=1)
         with pytest.raises(ValueError, match="always preprocessed"):
-            reg.set_moving(np.zeros((64, 64), np.uint8), preprocess=False)
+            reg.set_image(0, np.zeros((64, 64), np.uint8), preprocess=False)
         m, f, _ = synth.pair_remap(n=64, seed=9)
         reg.set_images(m, f, preprocess=False)
         small = np.empty(16, np.float32)
@@ -185,7 +185,7 @@ def test_errors_and_boundaries():
             a, b = rng.random(shape).astype(np.float32), rng.random(shape).astype(np.float32)
             reg.set_images(a, b, preprocess=False)
             pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
-            sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=1024)
+            sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=1024)
             ref = O.shift_map(pa, pb, np.eye(3), exact=True, calibrated=False, cap=1024, return_corr=True)
             check_map(sm, ref, ref["corr"][0], tight=1e-3, loose=1e-2)
 
@@ -198,10 +198,10 @@ def test_rotated_pose_canvas(c1_pair):
     R = np.array([[s * np.cos(th), -s * np.sin(th), 0], [s * np.sin(th), s * np.cos(th), 0], [0, 0, 1]])
     T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
     H = T(c + 6, c - 4) @ R @ T(-c, -c)
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0)), prep_from(reg.features(1))
-        sm = reg.shift_map(H, exact=True, calibrated=False, resolution=1024)
+        sm = reg.shift_map(H, exact=True, calibrated=False, cap=1024)
         origin, size, Hc = reg.canvas(H)
     ref = O.shift_map(pa, pb, H, exact=True, calibrated=False, cap=1024, return_corr=True)
     assert origin == (ref["ox"], ref["oy"]) and size == (ref["canvas_w"], ref["canvas_h"])
@@ -218,10 +218,10 @@ def test_row_pass_tensor_memory_matches_split(monkeypatch, n, cap):
     maps = {}
     for mode in ("split", "tmem"):
         monkeypatch.setenv("ZCMIR_B200_ROW_PASS", mode)
-        with zc.Registrar(half=False) as reg:
+        with zc.Engine(half=False) as reg:
             reg.set_images(m, f, preprocess=False)
-            maps[mode] = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=cap)
-            g3 = reg.shift_map(np.eye(3), exact=True, calibrated=False, resolution=cap)
+            maps[mode] = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=cap)
+            g3 = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=cap)
             maps[mode + "3"] = g3
     for a, b in (("split", "tmem"), ("split3", "tmem3")):
         A, B = maps[a], maps[b]
@@ -239,11 +239,11 @@ def test_bench_maps_graph_replay_leaves_the_map_unchanged(c1_pair):
     event-instrumented maps for the stages): the timings are sane and a map computed after the
     replays is the map computed before them, value for value."""
     m, f, H = c1_pair
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
-        before = reg.shift_map(H, exact=True, calibrated=True, resolution=512)
+        before = reg.shift_map(H, exact=True, calibrated=True, cap=512)
         r = reg.bench_maps(H, flags=3, cap=512, warmup=2, steps=4)
-        after = reg.shift_map(H, exact=True, calibrated=True, resolution=512)
+        after = reg.shift_map(H, exact=True, calibrated=True, cap=512)
         ev = [e["text"] for e in reg.events() if e.get("kind") == "log"]
     assert 0 < r["ms_per_map"] <= 1.5 * r["ms_per_map_instrumented"], r
     assert abs(sum(r["stages_ms"].values()) - r["ms_per_map_instrumented"]) <= 0.05 * r["ms_per_map_instrumented"]

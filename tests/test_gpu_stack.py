@@ -1,17 +1,16 @@
 """GPU checks of the stack path: zcb_stack_maps (every slice's features once, one map per
-consecutive pair) against one zc_shift_map per pair and the oracle, and register_stack end to end
-on a drifting stack.
+consecutive pair) against one zc_shift_map per pair and the oracle. (register_stack end to end, the
+reference's own loop over this library, is in test_gpu_dropin.py.)
 
 Tolerances: stack maps equal the per-pair maps (the same kernels on the same features: peak index
 exact, peak score within 1e-6 relative); the first pair's map matches the float64 oracle as the
-map tests require (index exact, peak within 1e-4 relative); register_stack lands every pair within
-2 px of the planted similarity at every corner."""
+map tests require (index exact, peak within 1e-4 relative)."""
 import numpy as np
 import pytest
 
 import zcmir_b200 as zc
 from oracle import smi_oracle as O
-from zcmir_b200 import api, synth
+from zcmir_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
@@ -34,20 +33,20 @@ def test_stack_maps_equal_per_pair_maps(stack):
     n = len(slices)
     priors = [np.array([[1, 0, (s0.shape[1] - s1.shape[1]) / 2], [0, 1, (s0.shape[0] - s1.shape[0]) / 2], [0, 0, 1.0]])
               for s0, s1 in zip(slices[:-1], slices[1:])]
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         a, b, _ = synth.pair_remap(n=128, seed=1)
         reg.set_images(a, b, preprocess=False)
         reg.pose = np.diag([1.0, 1.0, 1.0])
         before = reg.score(np.eye(3)).mean
-        maps, ms = reg.stack_maps(slices, exact=True, calibrated=False, resolution=1024)
+        maps, ms = reg.stack_maps(slices, exact=True, calibrated=False, cap=1024)
         assert len(maps) == n - 1 and ms > 0
         # the engine's own pair is untouched
         assert reg.score(np.eye(3)).mean == pytest.approx(before, rel=1e-9) and tuple(reg.image_size(0)) == (128, 128)
         # explicit priors equal to the default (centres aligned) give the same maps
-        maps2, _ = reg.stack_maps(slices, priors, exact=True, calibrated=False, resolution=1024)
+        maps2, _ = reg.stack_maps(slices, priors, exact=True, calibrated=False, cap=1024)
         for k in range(1, n):
             reg.set_images(slices[k], slices[k - 1], preprocess=False)
-            one = reg.shift_map(priors[k - 1], exact=True, calibrated=False, resolution=1024, return_map=False)
+            one = reg.shift_map(priors[k - 1], exact=True, calibrated=False, cap=1024, want_map=False)
             for s in (maps[k - 1], maps2[k - 1]):
                 assert s.peak_index == one.peak_index and (s.dx, s.dy) == (one.dx, one.dy)
                 assert abs(s.peak - one.peak) <= 1e-6 * abs(one.peak)
@@ -62,24 +61,8 @@ def test_stack_maps_equal_per_pair_maps(stack):
 
 
 def test_stack_maps_errors():
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         with pytest.raises(ValueError, match="at least 2"):
             reg.stack_maps([np.zeros((64, 64), np.float32)])
         with pytest.raises(RuntimeError, match="BadImage"):
             reg.stack_maps([np.zeros((64, 64), np.float32), np.zeros((4, 64), np.float32)])
-
-
-def test_register_stack_follows_a_drifting_stack(stack):
-    slices, truths = stack
-    moving, fixed = slices[1:], slices[:-1]
-    seen = []
-    # the truth is a similarity: refine in the affine group (a homography's extra freedom lets a
-    # 300 px multimodal pair settle a few px off it)
-    r = api.register_stack(moving, fixed, model="affine", preprocess=False, half=False,
-                           progress=lambda i, n, x: seen.append(i))
-    assert seen == list(range(len(moving)))
-    assert r.slices[0].method == "search"
-    for k, (reg_k, H) in enumerate(zip(r.slices, truths)):
-        h, w = moving[k].shape
-        assert corner_dist(reg_k.H, H, w, h) < 2, (k, reg_k.method, corner_dist(reg_k.H, H, w, h))
-    assert not any(r.flagged)

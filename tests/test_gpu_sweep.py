@@ -13,7 +13,7 @@ import pytest
 import zcmir_b200 as zc
 from oracle import smi_oracle as O
 from oracle import sweep_oracle as S
-from zcmir_b200 import api, synth
+from zcmir_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
@@ -37,10 +37,10 @@ def small():
     return synth.pair_similarity(n=128, seed=5, deg=40.0, scale=1.1, shift=(6.0, -4.0))
 
 
-def check_lanes(gs, gi, ref, nc, n_peak, cell):
+def check_lanes(gs, gi, ref, nc, n_peak, cell, only=None):
     c2 = cell * cell
     clear_top = 0
-    for ci in range(nc):
+    for ci in (range(nc) if only is None else sorted(only)):
         top = ref["raw"][ci]
         o_s = np.array([v for v, _ in top]) * c2
         o_i = [t for _, t in top]
@@ -67,7 +67,7 @@ def test_sweep_lane_peaks_match_oracle(small, exact, features):
     m, f, H = small
     settings = dict(half=False, exact=exact, smi_features=features, sw_nth=12, sw_ns=3, sw_smin=0.8, sw_smax=1.25,
                     sw_grid=64)
-    with zc.Registrar(**settings) as reg:
+    with zc.Engine(**settings) as reg:
         reg.set_images(m, f, preprocess=False)
         pa, pb = prep_from(reg.features(0), features), prep_from(reg.features(1), features)
         sw = reg.sweep(n_peak=4)
@@ -86,6 +86,39 @@ def test_sweep_lane_peaks_match_oracle(small, exact, features):
     np.testing.assert_allclose(sw.scores, sw2.scores, rtol=1e-6, atol=0)
 
 
+@pytest.mark.slow
+def test_sweep_lane_peaks_full_size_sample():
+    """The 512² sweep workload: 360 rotations × 9 scales = 3240 candidate maps on the 128-cell
+    grid, in plane classes of 192², 256² and 144². Up to 32 candidates of each class, evenly
+    spread over the class, are mapped by the float64 oracle (tap positions in float32, as the
+    reference computes them); the GPU's full sweep must hold each one's lane maxima as the
+    small-grid test requires."""
+    m16, f16, _ = synth.pair_similarity(n=512, seed=2)
+    m, f = zc.gray32(m16), zc.gray32(f16)
+    settings = dict(half=False, sw_nth=360, sw_ns=9, sw_smin=0.8, sw_smax=1.25, sw_grid=128)
+    with zc.Engine(**settings) as eng:
+        eng.set_images(m, f, preprocess=False)
+        pa, pb = prep_from(eng.features(0)), prep_from(eng.features(1))
+        sw = eng.sweep(n_peak=4, batch=128)
+    gv = S.sweep_grid(n_theta=360, n_sigma=9, s_min=0.8, s_max=1.25)
+    st = S.sweep_setup(512, 512, 512, 512, np.eye(3), gv, 128)
+    classes = {}
+    for ci, c in enumerate(st["cands"]):
+        classes.setdefault((c["nx"], c["ny"]), []).append(ci)
+    assert sorted(classes) == [(144, 144), (192, 192), (256, 256)], sorted(classes)
+    only = set()
+    for members in classes.values():
+        only.update(members[int(i)] for i in np.linspace(0, len(members) - 1, min(32, len(members))))
+    # taps placed in float32 as the reference's shader places them: at this size a few taps sit
+    # within 1e-4 px of the image edge, where the rounding decides whether their whole sample
+    # counts (with float64 positions one candidate's top score moves by 3e-4)
+    ref = S.sweep(pa, pb, np.eye(3), gv, G=128, exact=True, only=only, f32_positions=True)
+    nc = len(st["cands"])
+    assert int(sw.info["candidates"]) == nc == 3240 and sw.info["min_n"] == ref["min_n"]
+    n_clear = check_lanes(sw.scores.astype(np.float64), sw.index, ref, nc, 4, st["cell"], only)
+    assert n_clear >= len(only) // 2, (n_clear, len(only))
+
+
 @pytest.mark.parametrize("seed,near_truth", [(7, True), (11, True), (3, False)])
 def test_search_recovers_a_similarity(seed, near_truth):
     """From the identity over the full circle and scales 0.5–2 (the default grid: 1800 maps).
@@ -93,12 +126,12 @@ def test_search_recovers_a_similarity(seed, near_truth):
     climb stays at the planted pose, the search lands within 5 px of it. (Seed 3 is a pair whose
     SMI optimum lies a few px off the planted pose: the climb from the truth leaves it.)"""
     m, f, H = synth.pair_similarity(n=256, seed=seed)
-    with zc.Registrar(half=False) as reg:
+    with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         s0 = reg.score(np.eye(3)).mean
         r = reg.search()
         assert r.improved and r.count_a > 0 and r.count_b > 0
-        assert r.previous == pytest.approx(s0)
+        assert r.prev == pytest.approx(s0)
         np.testing.assert_allclose(reg.pose, r.H)
         ev = reg.events()
         assert any("search done" in e.get("text", "") for e in ev)
@@ -111,21 +144,9 @@ def test_search_recovers_a_similarity(seed, near_truth):
             assert corner_dist(r.H, H, 256, 256) < 5, corner_dist(r.H, H, 256, 256)
 
 
-def test_search_ranges_shear_stretch_and_misses():
-    m, f, H = synth.pair_similarity(n=256, seed=7, deg=25.0, scale=0.9, shift=(10.0, -12.0))
-    J = H[:2, :2]
-    ang = np.degrees(np.arctan2(J[1, 0] - J[0, 1], J[0, 0] + J[1, 1]))
-    common = dict(preprocess=False, half=False)
-    r = api.search(m, f, rotation=(ang - 40, ang + 40), sw_nth=21, shear=0.05, stretch=(0.05, 3), **common)
-    assert isinstance(r, api.Registration) and r.method == "search (sweep)"
-    assert corner_dist(r.H, H, 256, 256) < 5, corner_dist(r.H, H, 256, 256)
-    miss = api.search(m, f, rotation=(ang + 90, ang + 150), sw_nth=11, **common)
-    assert corner_dist(miss.H, H, 256, 256) > 5
-
-
 def test_search_refusals():
     m, f, _ = synth.pair_similarity(n=128, seed=5, deg=10.0, scale=1.0, shift=(0.0, 0.0))
-    with zc.Registrar(half=False, search_mode="cloud") as reg:
+    with zc.Engine(half=False, search_mode="cloud") as reg:
         reg.set_images(m, f, preprocess=False)
         with pytest.raises(RuntimeError, match="cloud"):
             reg.search()
@@ -139,7 +160,7 @@ def test_sweep_shards_merge_to_the_whole_sweep(small):
     merge them (sum of scores, minimum of indices), give the whole sweep; the search finished
     from the merged lanes (zcb_search_lanes) reaches the same pose as search()."""
     m, f, H = small
-    with zc.Registrar(half=False, sw_nth=12, sw_ns=3, sw_smin=0.8, sw_smax=1.25, sw_grid=64) as reg:
+    with zc.Engine(half=False, sw_nth=12, sw_ns=3, sw_smin=0.8, sw_smax=1.25, sw_grid=64) as reg:
         reg.set_images(m, f, preprocess=False)
         whole = reg.sweep(n_peak=4)
         parts = [reg.sweep(n_peak=4, shard=r, nshard=3) for r in range(3)]

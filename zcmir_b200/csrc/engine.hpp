@@ -299,6 +299,9 @@ class Engine {
     // Gauss–Newton on many poses at once (src/search.zig gnBatch)
     bool gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
                   std::vector<ScoredPose>& out);
+    // zc_match without keypoints: the SMI sweep search from the images' centres aligned gives
+    // the fit, which becomes the pose (keypoint counts 0)
+    bool match_by_sweep(zc_match_result* out);
     // sweep → NMS → batched Gauss–Newton screen → finalists (src/search.zig runSweep)
     bool search(zc_search_result* out);
     // the sweep grid, canvas size and prior pose the settings ask for

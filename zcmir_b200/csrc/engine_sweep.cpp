@@ -411,6 +411,31 @@ bool Engine::search(zc_search_result* out) {
     return search_finish(res, gv, H0, out);
 }
 
+bool Engine::match_by_sweep(zc_match_result* out) {
+    if (!need_images()) return false;
+    // a keypoint fit has no prior: start from the images' centres aligned
+    const double lw = side[0].w, lh = side[0].h, rw = side[1].w, rh = side[1].h;
+    H = translate((rw - lw) / 2, (rh - lh) / 2);
+    const std::string mode = set.e("search_mode");
+    std::string err;
+    if (mode != "sweep") {
+        const char* js = "{\"search_mode\":\"sweep\"}";
+        set.apply(js, strlen(js), err);
+    }
+    log_event("match  no keypoint matcher in this build: the SMI sweep search fits the pose");
+    zc_search_result r{};
+    const bool ok = search(&r);
+    if (mode != "sweep") {
+        const std::string back = "{\"search_mode\":\"" + mode + "\"}";  // an enum tag: no escaping
+        set.apply(back.c_str(), back.size(), err);
+    }
+    if (!ok) return false;
+    zc_match_result m{};
+    std::memcpy(m.H, H.data(), sizeof m.H);
+    *out = m;
+    return true;
+}
+
 bool Engine::search_lanes(const float* scores, const uint32_t* idx, size_t n, zc_search_result* out) {
     if (!search_check()) return false;
     SweepGrid gv;

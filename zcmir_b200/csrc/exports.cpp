@@ -282,8 +282,27 @@ int32_t zc_pg_info(zc_engine* e, double*) { return unsupported(e, "pg_info"); }
 int32_t zc_pg_maps(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "pg_maps"); }
 int32_t zc_pg_descriptors(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "pg_descriptors"); }
 int32_t zc_match_scores(zc_engine* e, float*, size_t) { return unsupported(e, "match_scores"); }
-int32_t zc_detect(zc_engine* e, zc_detect_result*) { return unsupported(e, "detect"); }
-int32_t zc_match(zc_engine* e, zc_match_result*) { return unsupported(e, "match"); }
+// Keypoints are outside this build's SMI path. So that callers which start a registration from
+// keypoints (the reference's register() without a start pose, register_stack's first pair and its
+// re-detections) run unchanged, zc_detect finds no keypoints and succeeds, and zc_match takes its
+// fit from the SMI sweep search instead of a keypoint fit (Engine::match_by_sweep). The keypoint
+// and match listings below stay refused.
+int32_t zc_detect(zc_engine* e, zc_detect_result* out) {
+    return guarded(e, "detect", [&] {
+        if (!e->need_images()) return false;
+        if (out) *out = zc_detect_result{};
+        e->log_event("detect  no keypoint detector in this build: 0 keypoints (zc_match fits by the SMI sweep)");
+        return true;
+    });
+}
+int32_t zc_match(zc_engine* e, zc_match_result* out) {
+    return guarded(e, "match", [&] {
+        zc_match_result r{};
+        if (!e->match_by_sweep(&r)) return false;
+        if (out) *out = r;
+        return true;
+    });
+}
 int32_t zc_auto(zc_engine* e, zc_climb_result*) { return unsupported(e, "auto"); }
 int32_t zc_keypoints(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "keypoints"); }
 int32_t zc_keypoint_frames(zc_engine* e, uint32_t, float*, size_t) { return unsupported(e, "keypoint_frames"); }

@@ -44,7 +44,7 @@ def main():
     if a.search:
         n = a.n or 512
         m, f, H = synth.pair_similarity(n=n, seed=2)
-        with zc.Registrar(half=False, smi_features=a.features, sw_nth=a.nth, sw_ns=a.ns, sw_smin=0.8, sw_smax=1.25,
+        with zc.Engine(half=False, smi_features=a.features, sw_nth=a.nth, sw_ns=a.ns, sw_smin=0.8, sw_smax=1.25,
                           sw_grid=128) as reg:
             reg.set_images(m, f, preprocess=False)
             for _ in range(a.maps):
@@ -55,7 +55,7 @@ def main():
     if a.sweep:
         n = a.n or 512
         m, f, H = synth.pair_similarity(n=n, seed=2)
-        with zc.Registrar(half=False, smi_features=a.features, sw_nth=a.nth, sw_ns=a.ns, sw_smin=0.8, sw_smax=1.25,
+        with zc.Engine(half=False, smi_features=a.features, sw_nth=a.nth, sw_ns=a.ns, sw_smin=0.8, sw_smax=1.25,
                           sw_grid=128) as reg:
             reg.set_images(m, f, preprocess=False)
             for _ in range(a.maps):
@@ -66,10 +66,10 @@ def main():
         return
     n = a.n or 1024
     m, f, H = synth.pair_segmented(n=n, seed=1, max_shift=min(200, n // 5))
-    with zc.Registrar(half=False, smi_features=a.features) as reg:
+    with zc.Engine(half=False, smi_features=a.features) as reg:
         reg.set_images(m, f, preprocess=False)
         for _ in range(a.maps):
-            sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, resolution=a.cap, return_map=False)
+            sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=a.cap, want_map=False)
         print(f"n {sm.n}x{sm.ny} grid {sm.cw}x{sm.ch} peak {sm.peak:.3f} at ({sm.dx}, {sm.dy}); truth {-H[0, 2]}, {-H[1, 2]}")
 
 

@@ -218,7 +218,7 @@ def search(reg, net, k=4, with_network=True, iters=25):
     seeds = []
     for b in net.top(features(sw.scores), k):
         H = candidate_pose(reg, *bin_pose(b))
-        sm = reg.shift_map(H, return_map=False)
+        sm = reg.shift_map(H, want_map=False)
         seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
     Hs, sc = reg.refine_poses(np.array(seeds), iters)
     i = int(np.argmax(sc))
@@ -276,9 +276,9 @@ def dataset(reg, seeds, n=256):
 
 
 def _train_main(a):
-    from . import Registrar
+    from .engine import Engine
     t0 = time.perf_counter()
-    with Registrar(half=False) as reg:
+    with Engine(half=False) as reg:
         x, y = dataset(reg, range(a.train), a.n)
         xv, yv = dataset(reg, range(a.train, a.train + a.val), a.n)
     t_data = time.perf_counter() - t0
@@ -300,10 +300,10 @@ def _eval_main(a):
     """Held-out pairs: the plain full search (the reference of pose error), the coarse search
     alone and the coarse search with the network; success = corner RMS error ≤ 0.5 px against
     the planted pose; the wall time of each search with the images already loaded."""
-    from . import Registrar
+    from .engine import Engine
     net = Network.load(a.params)
     rows = []
-    with Registrar(half=False) as reg:
+    with Engine(half=False) as reg:
         for sd in range(a.first, a.first + a.pairs):
             m, f, Ht = make_pair(sd, a.n)
             reg.set_images(m, f, preprocess=False)
