@@ -464,7 +464,10 @@ def run_gpu(args, rank, ws, local):
                                         "stages_ms from event-instrumented maps",
                               "ms_per_map_instrumented": r.get("ms_per_map_instrumented")}),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel from a capture "
+                                           "of an earlier run of this command (profiles/traffic.json), not measured by this run",
+                         "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": b_launch, "launch_ms": t_launch,
                          "map_algorithmic_bytes": survey_bytes(r),
                          "map_frac": survey_bytes(r) / (ms * 1e-3) / 1e9 / hbm},

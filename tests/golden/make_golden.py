@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures in this folder from the reference tree (ZacharyVarley/zcmir).
 
-    python tests/golden/make_golden.py /path/to/zcmir
+    python tests/golden/make_golden.py --reference /path/to/zcmir   (or set ZCMIR_REFERENCE)
 
 Run once where the reference is checked out; the fixtures it writes are committed, and
 nothing at test time reads the reference tree.
@@ -108,4 +108,13 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+    import os
+
+    ap = argparse.ArgumentParser(description="ABI, settings and landsat-b fixtures from the reference's sources")
+    ap.add_argument("--reference", default=os.environ.get("ZCMIR_REFERENCE"),
+                    help="the zcmir checkout (default: $ZCMIR_REFERENCE)")
+    a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set ZCMIR_REFERENCE")
+    main(a.reference)

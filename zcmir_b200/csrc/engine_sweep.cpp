@@ -32,8 +32,8 @@ bool Engine::sweep_setup(const Mat3& H0, const SweepGrid& gv, int G, SweepOut& o
     const double fw = B.w, fh = B.h, mw = A.w, mh = A.h;
     const bool ladder = set.e("fft_sizes") != "compact";
     out = SweepOut{};
-    // canvas: a square around the fixed image, large enough for the moving image at the largest
-    // stretch (capped at twice the fixed size)
+    // the G×G canvas is a square centred on the fixed image, wide enough to hold the moving image
+    // under the candidate with the biggest singular value, but never over twice the fixed image
     const auto cm = map_pt(H0, (mw + 1) / 2, (mh + 1) / 2);
     double s_max = -INFINITY;
     for (double s : gv.sigmas)
@@ -71,7 +71,8 @@ bool Engine::sweep_setup(const Mat3& H0, const SweepGrid& gv, int G, SweepOut& o
                     c.gx0 = mcx[0], c.gy0 = mcy[0];
                     c.nx = (int)sweep_plane_len((unsigned)(mcx[1] - mcx[0] + Fx - 1), ladder);
                     c.ny = (int)sweep_plane_len((unsigned)(mcy[1] - mcy[0] + Fy - 1), ladder);
-                    // box-filter taps per cell side from the candidate's smallest stretch
+                    // taps per cell side: enough that the box filter samples the moving image at its finest
+                    // (the candidate's smaller singular value)
                     c.taps = (float)std::min(6.0, std::max(1.0, std::ceil(cell / (sv2(L)[1] * s0) - 1e-3)));
                     out.cands.push_back(c);
                 }
@@ -274,8 +275,9 @@ void Engine::sweep_make_peaks(SweepOut& out, int n_peak) {
             const uint32_t t = out.lane_idx[(size_t)ci * n_peak + k];
             if (!(v > 0) || (uint64_t)t >= (uint64_t)cd.nx * cd.ny) continue;
             if (k == 0) out.best[ci] = (float)v;
-            // lag (moving index − fixed index) in [−(F − 1), window − 1], then the moving
-            // image's canvas displacement gx0 + lag − fx0 cells; the correction is T(−d)
+            // the map index gives a lag between the moving and fixed windows, from −(F − 1) up to
+            // the moving window's width − 1; adding the windows' first cells turns it into the
+            // moving image's displacement on the canvas in cells, and the pose is corrected by T(−d)
             const int py = (int)(t / (uint32_t)cd.nx), px = (int)(t - (uint32_t)py * (uint32_t)cd.nx);
             const int wx = cd.nx - out.Fx + 1, wy = cd.ny - out.Fy + 1;
             const int lx = px < wx ? px : px - cd.nx, ly = py < wy ? py : py - cd.ny;
@@ -369,7 +371,8 @@ void Engine::sweep_settings(SweepGrid& gv, int& G, Mat3& H0) {
     const unsigned g = set.u("sw_grid");
     G = (g == 32 || g == 64 || g == 128 || g == 256) ? (int)g : 128;
     const double rot_deg = clampf(set.f("sw_rot"), 0, 180);
-    // a range wider than the circle is the circle; hi < lo runs through ±180° (170 → −170)
+    // a span past 360° is clamped to one turn; an upper end below the lower one wraps through
+    // ±180° (e.g. 170 to −170 covers 20° about 180°)
     const bool range = set.b("sw_rot_range");
     const double rot_lo = range ? clampf(set.f("sw_rot_lo"), -360, 360) : -rot_deg;
     double rot_hi = range ? clampf(set.f("sw_rot_hi"), -360, 360) : rot_deg;

@@ -37,8 +37,10 @@ inline std::vector<double> sweep_linspace(double lo, double hi, unsigned n0) {
     return out;
 }
 
-// The full circle is sampled without repeating ±180°; a partial range includes both ends.
-// Scales and stretches are log-spaced (stretch symmetric about 1), shears linear about 0.
+// Rotation samples: a 360° span takes n_theta equal steps from −180° (so −180° and +180°, the same
+// rotation, are not both taken); a narrower span puts samples on both of its end points. Scale and
+// stretch samples are geometric (stretch factors come in reciprocal pairs about 1); shear samples
+// are evenly spaced about 0.
 inline SweepGrid sweep_grid(const SweepGridOpts& o) {
     SweepGrid g;
     const unsigned nT = std::max(1u, o.n_theta);
@@ -74,7 +76,7 @@ inline Mat3 about_c(const std::array<double, 2>& c, const Lin2& L) {
     return {L[0], L[1], c[0] - L[0] * c[0] - L[1] * c[1], L[2], L[3], c[1] - L[2] * c[0] - L[3] * c[1], 0, 0, 1};
 }
 
-// singular values of a 2×2 (largest, smallest)
+// the 2×2 map's two singular values, the larger first
 inline std::array<double, 2> sv2(const Lin2& L) {
     const double a = L[0] * L[0] + L[2] * L[2], b = L[0] * L[1] + L[2] * L[3], d = L[1] * L[1] + L[3] * L[3];
     const double t = 0.5 * (a + d), r = std::sqrt(std::max(0.0, 0.25 * (a - d) * (a - d) + b * b));
@@ -148,7 +150,7 @@ inline std::vector<double> geo_amps(double a0, double ratio, unsigned n) {
     return out;
 }
 
-// Rotation (rad) and scale of H relative to H0 at moving point c (1-based).
+// How far H is turned (radians) and scaled from H0, read at moving-image point c (1-based).
 inline std::array<double, 2> sim_of(const Mat3& H, const Mat3& H0, double cx, double cy) {
     auto jac = [&](const Mat3& M) -> std::array<double, 4> {
         const double w = M[6] * cx + M[7] * cy + M[8];
