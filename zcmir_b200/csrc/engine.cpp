@@ -544,9 +544,11 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
         }
         return true;
     };
+    unsigned* fault = reinterpret_cast<unsigned*>(res + 24);  // the inverse columns' fault word
     auto lag0 = [&](const float* ga, const float* gb) {
         return cuda_ok(lag0_count(ga, gb, g.cw, g.ch, n00, st), "lag0") &&
-               cuda_ok(cudaMemsetAsync(best, 0, 8, st), "shift_map");
+               cuda_ok(cudaMemsetAsync(best, 0, 8, st), "shift_map") &&
+               cuda_ok(cudaMemsetAsync(fault, 0, 4, st), "shift_map");
     };
     auto rows_of = [&](int s, const float* grid) {
         return cuda_ok(forward_rows(grid, g, job.plan, job.row, (s == 0 ? half_a_ : half_b_).as<float2>(), st),
@@ -575,7 +577,8 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
             !lag0(ga, gb) || !rows_of(1, gb) || !cols_of(1))
             return false;
     }
-    if (!cuda_ok(inverse_columns(half_a_.as<float2>(), half_b_.as<float2>(), g, job.plan, job.col, q_.as<float2>(), st),
+    if (!cuda_ok(inverse_columns(half_a_.as<float2>(), half_b_.as<float2>(), g, job.plan, job.col, q_.as<float2>(), st,
+                                 1, 0, 0, 0, fault),
                  "inverse columns"))
         return false;
     rec(4);
@@ -637,8 +640,8 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     // with the tensor-memory row pass the map leaves in row chunks during the pass (copy_st_)
     const bool chunked = map && row_pass != "split" && rows_tmem_supported(job.g.nx, job.plan.n_corr);
     if (!run_map(job, profiling ? ev : nullptr, chunked ? map : nullptr)) return false;
-    unsigned char host[24];
-    if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 24, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
+    unsigned char host[28];
+    if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 28, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
     counts[2]++;
     if (map && !chunked) {
         if (!cuda_ok(cudaMemcpyAsync(map, map_.p, nn * 4, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
@@ -661,8 +664,13 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     }
     unsigned long long best;
     float zero;
+    unsigned fault;
     memcpy(&best, host, 8);
     memcpy(&zero, host + 8, 4);
+    memcpy(&fault, host + 24, 4);
+    if (fault)
+        return fail("shift_map: the inverse column pass gave up waiting for its operand copies (fault " +
+                    std::to_string(fault) + "); the map is not valid");
     map_result(job, best, zero, pair_area(), out);
     return true;
 }

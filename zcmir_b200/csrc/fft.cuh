@@ -27,11 +27,11 @@ struct LinePlan {
     const float2* tw;         // n twiddles e^{−2πi t/n}, t < n (device memory)
 };
 
-__host__ __device__ __forceinline__ int pad_idx(int i) { return i + (i >> 4); }
-__host__ __device__ __forceinline__ int padded_len(int n) { return n + (n >> 4) + 1; }
+__host__ __device__ __forceinline__ constexpr int pad_idx(int i) { return i + (i >> 4); }
+__host__ __device__ __forceinline__ constexpr int padded_len(int n) { return n + (n >> 4) + 1; }
 // pitch between lines stored side by side (column tiles): ≡ 4 (mod 16) points, so a half-warp
 // touching 4 lines × 4 consecutive points hits 16 distinct bank pairs
-__host__ __device__ __forceinline__ int line_pitch(int n) {
+__host__ __device__ __forceinline__ constexpr int line_pitch(int n) {
     const int p = padded_len(n);
     return p + ((4 - (p & 15)) & 15);
 }

@@ -78,10 +78,16 @@ cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev&
                          float2* half, cudaStream_t st, int batch = 1, size_t grid_stride = 0, size_t half_stride = 0);
 cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
                          cudaStream_t st, int batch = 1);
-// products and inverse column FFTs: Q[slot][ny][WP] (b_stride 0: one fixed side for every item)
+// products and inverse column FFTs: Q[slot][ny][WP] (b_stride 0: one fixed side for every item).
+// fault (nullable, device memory): 1 is or-ed into it if the TMA-fed pass (1024- and 2048-point
+// square maps, one item) gave up waiting for a copy, 2 if its staging was misaligned; its Q is
+// then not valid. ZCMIR_B200_INV_COLS=pipe selects the register-prefetch pass instead.
 cudaError_t inverse_columns(const float2* half_a, const float2* half_b, const MapGeom& g, const CorrPlanDev& plan,
                             const LinePlan& col, float2* Q, cudaStream_t st, int batch = 1, size_t a_stride = 0,
-                            size_t b_stride = 0, size_t q_stride = 0);
+                            size_t b_stride = 0, size_t q_stride = 0, unsigned* fault = nullptr);
+bool inverse_columns_tma_supported(const MapGeom& g, int batch);
+cudaError_t inverse_columns_tma(const float2* half_a, const float2* half_b, const MapGeom& g, const CorrPlanDev& plan,
+                                const float2* tw, float2* Q, cudaStream_t st, unsigned* fault);
 // inverse row FFTs fused with the per-shift score and the argmax: map (ny × nx f32), best key
 // (u64), zero-lag score (best and zero may be null); n00: one zero-lag overlap per item
 cudaError_t inverse_rows_score(const float2* Q, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& line,

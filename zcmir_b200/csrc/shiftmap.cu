@@ -13,6 +13,9 @@
 //      inverse row FFT, and the per-shift score in float64 with its argmax, without writing a
 //      correlation plane to memory. Rows longer than shared memory holds for all C correlations
 //      are split S ways by one decimation-in-frequency step (output shifts x ≡ s mod S).
+#include <cstdlib>
+#include <string>
+
 #include "passes.cuh"
 
 namespace zc {
@@ -206,7 +209,13 @@ cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan
 
 cudaError_t inverse_columns(const float2* ha, const float2* hb, const MapGeom& g, const CorrPlanDev& plan,
                             const LinePlan& col, float2* Q, cudaStream_t st, int batch, size_t a_stride,
-                            size_t b_stride, size_t q_stride) {
+                            size_t b_stride, size_t q_stride, unsigned* fault) {
+    static const bool pipe = [] {
+        const char* v = getenv("ZCMIR_B200_INV_COLS");
+        return v && std::string(v) == "pipe";
+    }();
+    if (!pipe && col.n == g.ny && inverse_columns_tma_supported(g, batch))
+        return inverse_columns_tma(ha, hb, g, plan, col.tw, Q, st, fault);
     PassArgs a = pass_args(g, plan, batch);
     a.half = const_cast<float2*>(ha);
     a.half_stride = a_stride;
