@@ -30,7 +30,10 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
  * and prior pose H0 (NULL: the pose zc_search would use). For every candidate (θ-major, then σ,
  * shear, stretch) its n_peak (1..16) best lane maxima — score in fixed pixels, map index
  * (0xffffffff: none) — into scores / idx (cap ≥ candidates × n_peak; both NULL: not returned).
- * batch: candidates per launch (0: from a 1 GB budget). shard / nshard: only the candidates in
+ * batch: candidates per launch (0: per plane class the size zcb_tune_sweep chose, else what a
+ * 1 GB budget holds, at most 128). The whole sweep's launches are captured once as a CUDA graph and
+ * replayed while their parameters are unchanged (ZCMIR_B200_SWEEP_GRAPH=0: stream-ordered
+ * launches). shard / nshard: only the candidates in
  * slots ≡ shard (mod nshard) of the plane-size order are mapped (one rank's share of a sweep
  * split across GPUs); the others' entries stay (0, 0xffffffff), so the shards' outputs merge by
  * a sum of scores and a minimum of indices. info[16]: [0] candidates, [1] cell (px),
@@ -40,6 +43,17 @@ int32_t zcb_settings_apply(const char* json, size_t len, char* out, size_t cap, 
  * (its sweep is internal to zc_search, src/search.zig:300-494). 0 / -1 with zc_error. */
 int32_t zcb_sweep(zc_engine* e, const double H0[9], uint32_t n_peak, uint32_t batch, uint32_t shard, uint32_t nshard,
                   float* scores, uint32_t* idx, size_t cap, double* info, size_t info_len);
+
+/* The sweep's autotuner: for every plane class (nx × ny) of a sweep with the engine's sw_*
+ * settings and images, times the whole sweep stream-ordered with candidate batches of 16, 32, …,
+ * 2048 (each class capped by its candidates and an 8 GB work-buffer budget) and keeps, per class,
+ * the batch with the least device time per candidate map; later sweeps (zcb_sweep batch 0,
+ * zc_search) use it. out (nullable, cap doubles; *used: the doubles written or needed), per class:
+ * nx, ny, candidates, chosen batch, its ms per candidate, k, then k pairs (batch, ms per
+ * candidate). Tuning grows the sweep's work buffers to the largest batch tried. No counterpart in
+ * the reference (whose tuning hooks, src/exports.zig:95-121, set workgroup shapes by hand).
+ * 0 / -1 with zc_error. */
+int32_t zcb_tune_sweep(zc_engine* e, double* out, size_t cap, size_t* used);
 
 /* zc_search from gathered lane maxima: scores / idx hold every candidate's 4 lane maxima (n =
  * candidates × 4, as zcb_sweep with n_peak 4 writes them, merged over shards); the engine's

@@ -86,6 +86,33 @@ def test_sweep_lane_peaks_match_oracle(small, exact, features):
     np.testing.assert_allclose(sw.scores, sw2.scores, rtol=1e-6, atol=0)
 
 
+def test_tuned_and_graph_sweeps_equal_the_stream_ordered_sweep(small, monkeypatch):
+    """zcb_tune_sweep picks a batch per plane class by timing; the sweep then runs with those
+    batches as one replay of a captured CUDA graph. The batch changes the launch shapes, not the
+    result, and a replay gives the lanes of a stream-ordered sweep."""
+    m, f, _ = small
+    settings = dict(half=False, sw_nth=12, sw_ns=3, sw_smin=0.8, sw_smax=1.25, sw_grid=64)
+    with zc.Engine(**settings) as eng:
+        eng.set_images(m, f, preprocess=False)
+        base = eng.sweep(n_peak=4, batch=5)
+        rows = eng.tune_sweep()
+        assert rows and sum(r["candidates"] for r in rows) == base.info["candidates"]
+        for r in rows:
+            assert r["batch"] in r["options"] and r["ms_per_map"] == min(r["options"].values())
+        tuned = eng.sweep(n_peak=4)
+        again = eng.sweep(n_peak=4)
+    np.testing.assert_array_equal(tuned.index, base.index)
+    np.testing.assert_allclose(tuned.scores, base.scores, rtol=1e-6, atol=0)
+    np.testing.assert_array_equal(again.index, tuned.index)
+    np.testing.assert_array_equal(again.scores, tuned.scores)
+    monkeypatch.setenv("ZCMIR_B200_SWEEP_GRAPH", "0")
+    with zc.Engine(**settings) as eng:
+        eng.set_images(m, f, preprocess=False)
+        plain = eng.sweep(n_peak=4, batch=5)
+    np.testing.assert_array_equal(plain.index, base.index)
+    np.testing.assert_array_equal(plain.scores, base.scores)
+
+
 @pytest.mark.slow
 def test_sweep_lane_peaks_full_size_sample():
     """The 512² sweep workload: 360 rotations × 9 scales = 3240 candidate maps on the 128-cell

@@ -83,6 +83,7 @@ Engine::Engine(int dev) : device(dev) {
 
 Engine::~Engine() {
     cudaStreamSynchronize(st);
+    if (sweep_exec_) cudaGraphExecDestroy(sweep_exec_);
     for (auto& s : side) {
         s.raw.release();
         s.work.release();

@@ -123,6 +123,9 @@ struct SweepOut {
     unsigned min_n = 0;
     int groups = 0, batches = 0, launches = 0;
     float ms = 0;                       // device time of the maps (CUDA events)
+    // per plane class (slot order): nx, ny, candidates, batch, device ms (stream-ordered runs only)
+    std::vector<std::array<double, 5>> classes;
+    bool graph = false;                 // the maps were one replay of a captured CUDA graph
 };
 
 // A pose and its score (the batched Gauss–Newton screen).
@@ -285,6 +288,19 @@ class Engine {
 
     // the rotation × scale sweep (engine_sweep.cpp): every candidate's map reduced to n_peak
     // peaks; batch 0 picks the batch from a memory budget
+    // Sweep batch sizes chosen by tune_sweep, per plane class: (nx, ny, correlations, exact).
+    std::map<std::array<int, 4>, int> sweep_tuned_;
+    // The sweep's launches captured as one CUDA graph, replayed while their parameters (the
+    // signature) are unchanged.
+    cudaGraphExec_t sweep_exec_ = nullptr;
+    std::vector<uint64_t> sweep_sig_;
+    int sweep_launches_ = 0;  // kernels one replay of sweep_exec_ launches
+    // while tuning: batch per plane class (nx, ny), stream-ordered launches timed per class
+    std::map<std::array<int, 2>, int> sweep_force_;
+    // time each candidate batch size per plane class of the current sweep settings, keep the
+    // fastest (rows of out: nx, ny, candidates, chosen batch, its ms per candidate, options,
+    // then (batch, ms per candidate) per option)
+    bool tune_sweep(double* out, size_t cap, size_t* used);
     bool sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
                     SweepOut& out, int batch = 0, int shard = 0, int nshard = 1);
     // the host half of a sweep: canvas, candidates, footprints, plane sizes and slot order

@@ -20,6 +20,7 @@ namespace {
 
 constexpr size_t kSweepBudget = 1ull << 30;  // device bytes of one batch's work buffers
 constexpr int kSweepMaxBatch = 128;
+constexpr size_t kTuneBudget = 8ull << 30;  // device bytes of one batch's work buffers while tuning
 
 size_t pitch_of(int nx) { return (size_t)((nx / 2 + 1) + 7) / 8 * 8; }
 
@@ -121,63 +122,75 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     fp[9] = (float)std::min(6.0, std::max(1.0, std::ceil(cell - 1e-3)));
     fp[10] = (float)fcx[0];
     fp[11] = (float)fcy[0];
-    // work buffers, sized once for the largest planes
-    int nx_max = 0, ny_max = 0;
-    size_t per_max = 0, fgrid = (size_t)5 * Fx * Fy;
+    // plane classes in slot order: [k0, k1) of the slots share one plane size
+    struct Cls {
+        int k0, k1, nx, ny, b, S;
+        LinePlan row, col, line;
+        const float2* tw;
+    };
+    std::vector<Cls> cls;
+    for (int k0 = 0; k0 < nm;) {
+        const int nx = out.cands[perm[k0]].nx, ny = out.cands[perm[k0]].ny;
+        int k1 = k0;
+        while (k1 < nm && out.cands[perm[k1]].nx == nx && out.cands[perm[k1]].ny == ny) ++k1;
+        cls.push_back(Cls{k0, k1, nx, ny, 0, 0, {}, {}, {}, nullptr});
+        k0 = k1;
+    }
     auto per_item = [&](int nx, int ny) {
         const size_t pstride = (size_t)ny * pitch_of(nx);
         return (size_t)5 * (nx - Fx + 1) * (ny - Fy + 1) * 4 + (size_t)(plan.n_real + plan.n_corr) * pstride * 8 +
                (size_t)nx * ny * 4;
     };
-    for (const SweepCand& c : out.cands) {
-        nx_max = std::max(nx_max, c.nx), ny_max = std::max(ny_max, c.ny);
-        per_max = std::max(per_max, per_item(c.nx, c.ny));
-    }
-    out.n = std::max(nx_max, ny_max);
-    int bmax = batch > 0 ? batch : (int)std::max<size_t>(1, std::min<size_t>(kSweepMaxBatch, kSweepBudget / per_max));
-    if (const char* v = getenv("ZCMIR_B200_SWEEP_BATCH"))
-        if (batch <= 0 && atoi(v) > 0) bmax = atoi(v);
+    // batch per class: the caller's, else the tuned one, else the environment's, else as many as
+    // the budget holds (at most kSweepMaxBatch)
+    int env_b = 0;
+    if (const char* v = getenv("ZCMIR_B200_SWEEP_BATCH")) env_b = std::max(0, atoi(v));
     size_t grid_max = 0, half_max = 0, q_max = 0, map_max = 0, fhalf_max = 0;
-    for (const SweepCand& c : out.cands) {
+    int bmax = 1;
+    for (Cls& c : cls) {
+        int b = batch;
+        if (!sweep_force_.empty()) {
+            const auto it = sweep_force_.find({c.nx, c.ny});
+            b = it != sweep_force_.end() ? it->second : b;
+        }
+        if (b <= 0) {
+            const auto it = sweep_tuned_.find({c.nx, c.ny, plan.n_corr, exact ? 1 : 0});
+            b = it != sweep_tuned_.end() ? it->second : 0;
+        }
+        if (b <= 0) b = env_b;
+        if (b <= 0) b = (int)std::max<size_t>(1, std::min<size_t>(kSweepMaxBatch, kSweepBudget / per_item(c.nx, c.ny)));
+        c.b = std::min(b, c.k1 - c.k0);
+        bmax = std::max(bmax, c.b);
         const size_t pstride = (size_t)c.ny * pitch_of(c.nx);
-        grid_max = std::max(grid_max, (size_t)5 * (c.nx - Fx + 1) * (c.ny - Fy + 1));
-        half_max = std::max(half_max, (size_t)plan.n_real * pstride);
-        q_max = std::max(q_max, (size_t)plan.n_corr * pstride);
-        map_max = std::max(map_max, (size_t)c.nx * c.ny);
+        grid_max = std::max(grid_max, (size_t)5 * (c.nx - Fx + 1) * (c.ny - Fy + 1) * c.b);
+        half_max = std::max(half_max, (size_t)plan.n_real * pstride * c.b);
+        q_max = std::max(q_max, (size_t)plan.n_corr * pstride * c.b);
+        map_max = std::max(map_max, (size_t)c.nx * c.ny * c.b);
         fhalf_max = std::max(fhalf_max, (size_t)plan.n_real * pstride);
+        out.n = std::max({out.n, c.nx, c.ny});
+        // line plans and twiddles now: nothing may allocate while the launches are captured
+        if (!line_plan(c.nx, c.row) || !line_plan(c.ny, c.col)) return false;
+        c.S = row_split(c.nx, plan.n_corr);
+        if (c.S == 0) return fail("sweep: a plane row of " + std::to_string(c.nx) + " does not fit the row pass");
+        if (!line_plan(c.nx / c.S, c.line)) return false;
+        c.tw = twiddles(c.nx);
+        if (!c.tw) return fail("sweep: twiddles: out of device memory");
     }
+    const size_t fgrid = (size_t)5 * Fx * Fy;
     const size_t na = (size_t)A.w * A.h, nb = (size_t)B.w * B.h;
     bool ok = cuda_ok(sw_il_[0].ensure(na * 20), "sweep") && cuda_ok(sw_il_[1].ensure(nb * 20), "sweep") &&
               cuda_ok(sw_poses_.ensure(poses.size() * 4), "sweep") && cuda_ok(sw_fgrid_.ensure(fgrid * 4), "sweep") &&
-              cuda_ok(sw_fhalf_.ensure(fhalf_max * 8), "sweep") &&
-              cuda_ok(sw_grid_.ensure(grid_max * 4 * bmax), "sweep") &&
-              cuda_ok(sw_half_.ensure(half_max * 8 * bmax), "sweep") && cuda_ok(sw_q_.ensure(q_max * 8 * bmax), "sweep") &&
-              cuda_ok(sw_map_.ensure(map_max * 4 * bmax), "sweep") && cuda_ok(sw_n0_.ensure((size_t)bmax * 8), "sweep") &&
+              cuda_ok(sw_fhalf_.ensure(fhalf_max * 8), "sweep") && cuda_ok(sw_grid_.ensure(grid_max * 4), "sweep") &&
+              cuda_ok(sw_half_.ensure(half_max * 8), "sweep") && cuda_ok(sw_q_.ensure(q_max * 8), "sweep") &&
+              cuda_ok(sw_map_.ensure(map_max * 4), "sweep") && cuda_ok(sw_n0_.ensure((size_t)bmax * 8), "sweep") &&
               cuda_ok(sw_ps_.ensure((size_t)std::max(nm, 1) * n_peak * 4), "sweep") &&
               cuda_ok(sw_pi_.ensure((size_t)std::max(nm, 1) * n_peak * 4), "sweep");
     if (!ok) return false;
     if (!cuda_ok(cudaMemcpyAsync(sw_poses_.p, poses.data(), poses.size() * 4, cudaMemcpyHostToDevice, st), "sweep"))
         return false;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
-    auto done = [&](bool r) {
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        return r;
-    };
     const SweepCanvas cv{(float)ox, (float)oy, (float)cell, G};
     const float4* ila = sw_il_[0].as<float4>();
     const float4* ilb = sw_il_[1].as<float4>();
-    int launches = 0;
-    if (!cuda_ok(sweep_interleave(A.stack.as<float>(), (int)na, sw_il_[0].as<float4>(), st), "sweep") ||
-        !cuda_ok(sweep_interleave(B.stack.as<float>(), (int)nb, sw_il_[1].as<float4>(), st), "sweep") ||
-        !cuda_ok(sweep_pack(ilb, B.w, B.h, sw_poses_.as<float>(), nm, 1, Fx, Fy, cv, nullptr, 0, 0, 0, 0,
-                            sw_fgrid_.as<float>(), nullptr, st),
-                 "sweep"))
-        return done(false);
-    launches += 3;
     out.min_n = (unsigned)std::max(12.0, std::floor(min_overlap * (fw * fh) / (cell * cell) + 0.5));
     CombineParams cp{};
     cp.exact = exact ? 1 : 0;
@@ -186,55 +199,149 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     cp.min_n = (float)out.min_n;
     cp.area = 1.0;
     cp.ridge = 1e-4;
-    for (int k0 = 0; k0 < nm;) {
-        const int nx = out.cands[perm[k0]].nx, ny = out.cands[perm[k0]].ny;
-        int k1 = k0;
-        while (k1 < nm && out.cands[perm[k1]].nx == nx && out.cands[perm[k1]].ny == ny) ++k1;
-        MapGeom gm{};
-        gm.nx = nx, gm.ny = ny, gm.WP = (int)pitch_of(nx);
-        gm.cw = nx - Fx + 1, gm.ch = ny - Fy + 1;
-        gm.W = gm.cw, gm.Hh = gm.ch;
-        MapGeom gf = gm;
-        gf.cw = Fx, gf.ch = Fy;
-        LinePlan row, col, line;
-        if (!line_plan(nx, row) || !line_plan(ny, col)) return done(false);
-        const int S = row_split(nx, plan.n_corr);
-        if (S == 0) return done(fail("sweep: a plane row of " + std::to_string(nx) + " does not fit the row pass"));
-        if (!line_plan(nx / S, line)) return done(false);
-        const float2* tw = twiddles(nx);
-        if (!tw) return done(fail("sweep: twiddles: out of device memory"));
-        cp.inv_nn = 1.0 / ((double)nx * (double)ny);
-        const size_t pstride = (size_t)ny * gm.WP;
-        const size_t wn = (size_t)gm.cw * gm.ch;
-        // the fixed window's spectra for this plane size
-        if (!cuda_ok(forward_rows(sw_fgrid_.as<float>(), gf, plan, row, sw_fhalf_.as<float2>(), st), "sweep") ||
-            !cuda_ok(forward_cols(sw_fhalf_.as<float2>(), gf, plan, col, st), "sweep"))
-            return done(false);
-        launches += 2;
-        for (int c0 = k0; c0 < k1; c0 += bmax) {
-            const int b = std::min(bmax, k1 - c0);
-            const size_t hs = (size_t)plan.n_real * pstride, qs = (size_t)plan.n_corr * pstride;
-            if (!cuda_ok(sweep_pack(ila, A.w, A.h, sw_poses_.as<float>(), c0, b, gm.cw, gm.ch, cv, sw_fgrid_.as<float>(),
-                                    fcx[0], fcy[0], Fx, Fy, sw_grid_.as<float>(), sw_n0_.as<double>(), st),
-                         "sweep") ||
-                !cuda_ok(forward_rows(sw_grid_.as<float>(), gm, plan, row, sw_half_.as<float2>(), st, b, 5 * wn, hs),
-                         "sweep") ||
-                !cuda_ok(forward_cols(sw_half_.as<float2>(), gm, plan, col, st, b), "sweep") ||
-                !cuda_ok(inverse_columns(sw_half_.as<float2>(), sw_fhalf_.as<float2>(), gm, plan, col,
-                                         sw_q_.as<float2>(), st, b, hs, 0, qs),
-                         "sweep") ||
-                !cuda_ok(inverse_rows_score(sw_q_.as<float2>(), gm, plan, line, S, tw, cp, sw_n0_.as<double>(),
-                                            sw_map_.as<float>(), nullptr, nullptr, st, b, qs, (size_t)nx * ny),
-                         "sweep") ||
-                !cuda_ok(sweep_peaks(sw_map_.as<float>(), nx, ny, (size_t)nx * ny, b, n_peak, c0, sw_ps_.as<float>(),
-                                     sw_pi_.as<uint32_t>(), st),
-                         "sweep"))
-                return done(false);
-            launches += 6;
-            out.batches++;
+    // per-class events (stream-ordered runs only: they time each plane class)
+    const bool use_graph = sweep_force_.empty() &&
+                           (!getenv("ZCMIR_B200_SWEEP_GRAPH") || atoi(getenv("ZCMIR_B200_SWEEP_GRAPH")) != 0);
+    std::vector<cudaEvent_t> cev;
+    if (!use_graph) {
+        cev.resize(cls.size() + 1);
+        for (auto& e : cev) cudaEventCreate(&e);
+    }
+    auto free_cev = [&] {
+        for (auto& e : cev) cudaEventDestroy(e);
+        cev.clear();
+    };
+    // every launch of the sweep's maps, in order; returns the launch count (−1 on an error)
+    auto enqueue = [&]() -> int {
+        int launches = 0;
+        if (!cuda_ok(sweep_interleave(A.stack.as<float>(), (int)na, sw_il_[0].as<float4>(), st), "sweep") ||
+            !cuda_ok(sweep_interleave(B.stack.as<float>(), (int)nb, sw_il_[1].as<float4>(), st), "sweep") ||
+            !cuda_ok(sweep_pack(ilb, B.w, B.h, sw_poses_.as<float>(), nm, 1, Fx, Fy, cv, nullptr, 0, 0, 0, 0,
+                                sw_fgrid_.as<float>(), nullptr, st),
+                     "sweep"))
+            return -1;
+        launches += 3;
+        for (size_t ci = 0; ci < cls.size(); ++ci) {
+            const Cls& c = cls[ci];
+            if (!cev.empty()) cudaEventRecord(cev[ci], st);
+            MapGeom gm{};
+            gm.nx = c.nx, gm.ny = c.ny, gm.WP = (int)pitch_of(c.nx);
+            gm.cw = c.nx - Fx + 1, gm.ch = c.ny - Fy + 1;
+            gm.W = gm.cw, gm.Hh = gm.ch;
+            MapGeom gf = gm;
+            gf.cw = Fx, gf.ch = Fy;
+            CombineParams cpc = cp;
+            cpc.inv_nn = 1.0 / ((double)c.nx * (double)c.ny);
+            const size_t pstride = (size_t)c.ny * gm.WP;
+            const size_t wn = (size_t)gm.cw * gm.ch;
+            // the fixed window's spectra for this plane size
+            if (!cuda_ok(forward_rows(sw_fgrid_.as<float>(), gf, plan, c.row, sw_fhalf_.as<float2>(), st), "sweep") ||
+                !cuda_ok(forward_cols(sw_fhalf_.as<float2>(), gf, plan, c.col, st), "sweep"))
+                return -1;
+            launches += 2;
+            for (int c0 = c.k0; c0 < c.k1; c0 += c.b) {
+                const int b = std::min(c.b, c.k1 - c0);
+                const size_t hs = (size_t)plan.n_real * pstride, qs = (size_t)plan.n_corr * pstride;
+                if (!cuda_ok(sweep_pack(ila, A.w, A.h, sw_poses_.as<float>(), c0, b, gm.cw, gm.ch, cv,
+                                        sw_fgrid_.as<float>(), fcx[0], fcy[0], Fx, Fy, sw_grid_.as<float>(),
+                                        sw_n0_.as<double>(), st),
+                             "sweep") ||
+                    !cuda_ok(forward_rows(sw_grid_.as<float>(), gm, plan, c.row, sw_half_.as<float2>(), st, b, 5 * wn, hs),
+                             "sweep") ||
+                    !cuda_ok(forward_cols(sw_half_.as<float2>(), gm, plan, c.col, st, b), "sweep") ||
+                    !cuda_ok(inverse_columns(sw_half_.as<float2>(), sw_fhalf_.as<float2>(), gm, plan, c.col,
+                                             sw_q_.as<float2>(), st, b, hs, 0, qs),
+                             "sweep") ||
+                    !cuda_ok(inverse_rows_score(sw_q_.as<float2>(), gm, plan, c.line, c.S, c.tw, cpc,
+                                                sw_n0_.as<double>(), sw_map_.as<float>(), nullptr, nullptr, st, b, qs,
+                                                (size_t)c.nx * c.ny),
+                             "sweep") ||
+                    !cuda_ok(sweep_peaks(sw_map_.as<float>(), c.nx, c.ny, (size_t)c.nx * c.ny, b, n_peak, c0,
+                                         sw_ps_.as<float>(), sw_pi_.as<uint32_t>(), st),
+                             "sweep"))
+                    return -1;
+                launches += 6;
+            }
         }
-        out.groups++;
-        k0 = k1;
+        if (!cev.empty()) cudaEventRecord(cev.back(), st);
+        return launches;
+    };
+    out.groups = (int)cls.size();
+    out.batches = 0;
+    for (const Cls& c : cls) out.batches += (c.k1 - c.k0 + c.b - 1) / c.b;
+    // the signature of everything the launches read from the host: pointers, sizes, the schedule
+    std::vector<uint64_t> sig;
+    if (use_graph) {
+        auto put = [&](uint64_t v) { sig.push_back(v); };
+        auto putd = [&](double v) {
+            uint64_t u;
+            std::memcpy(&u, &v, 8);
+            sig.push_back(u);
+        };
+        const void* ptrs[] = {A.stack.p, B.stack.p, sw_il_[0].p, sw_il_[1].p, sw_poses_.p, sw_fgrid_.p, sw_fhalf_.p,
+                              sw_grid_.p, sw_half_.p, sw_q_.p, sw_map_.p, sw_n0_.p, sw_ps_.p, sw_pi_.p};
+        for (const void* q : ptrs) put((uint64_t)(uintptr_t)q);
+        for (int v : {A.w, A.h, B.w, B.h, nm, n_peak, Fx, Fy, fcx[0], fcy[0], G, plan.n_real, plan.n_corr, exact ? 1 : 0,
+                      three ? 1 : 0, (int)out.min_n})
+            put((uint64_t)(int64_t)v);
+        putd(ox), putd(oy), putd(cell);
+        for (const Cls& c : cls)
+            for (uint64_t v : {(uint64_t)c.k0, (uint64_t)c.k1, (uint64_t)c.nx, (uint64_t)c.ny, (uint64_t)c.b,
+                               (uint64_t)c.S, (uint64_t)(uintptr_t)c.tw, (uint64_t)(uintptr_t)c.row.tw,
+                               (uint64_t)(uintptr_t)c.col.tw, (uint64_t)(uintptr_t)c.line.tw})
+                put(v);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto done = [&](bool r) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        free_cev();
+        return r;
+    };
+    int launches = 0;
+    out.graph = false;
+    if (use_graph) {
+        if (!sweep_exec_ || sig != sweep_sig_) {
+            // capture the launches once (nothing runs), instantiate, keep while the signature holds
+            if (sweep_exec_) {
+                cudaGraphExecDestroy(sweep_exec_);
+                sweep_exec_ = nullptr;
+            }
+            sweep_sig_.clear();
+            cudaGraph_t graph = nullptr;
+            const std::string err_before = err;
+            bool cap_ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            int n = -1;
+            if (cap_ok) {
+                n = enqueue();
+                const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+                cap_ok = n >= 0 && ce == cudaSuccess && graph &&
+                         cudaGraphInstantiate(&sweep_exec_, graph, 0) == cudaSuccess;
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (cap_ok) {
+                sweep_sig_ = sig;
+                sweep_launches_ = n;
+            } else {
+                cudaGetLastError();  // a refused capture is not this call's error: run stream-ordered
+                err = err_before;
+                if (sweep_exec_) cudaGraphExecDestroy(sweep_exec_);
+                sweep_exec_ = nullptr;
+            }
+        }
+        if (sweep_exec_) {
+            cudaEventRecord(e0, st);
+            if (!cuda_ok(cudaGraphLaunch(sweep_exec_, st), "sweep")) return done(false);
+            launches = sweep_launches_;
+            out.graph = true;
+        }
+    }
+    if (!out.graph) {
+        cudaEventRecord(e0, st);
+        launches = enqueue();
+        if (launches < 0) return done(false);
     }
     cudaEventRecord(e1, st);
     std::vector<float> ps((size_t)nm * n_peak);
@@ -244,6 +351,13 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
         !cuda_ok(cudaStreamSynchronize(st), "sweep"))
         return done(false);
     cudaEventElapsedTime(&out.ms, e0, e1);
+    out.classes.clear();
+    for (size_t ci = 0; ci < cls.size(); ++ci) {
+        float cms = -1.f;
+        if (!cev.empty()) cudaEventElapsedTime(&cms, cev[ci], cev[ci + 1]);
+        out.classes.push_back({(double)cls[ci].nx, (double)cls[ci].ny, (double)(cls[ci].k1 - cls[ci].k0),
+                               (double)cls[ci].b, (double)cms});
+    }
     out.launches = launches;
     counts[0] += launches;
     counts[1]++;
@@ -391,6 +505,78 @@ void Engine::sweep_settings(SweepGrid& gv, int& G, Mat3& H0) {
     gv = sweep_grid(o);
     const double lw = side[0].w, lh = side[0].h, rw = side[1].w, rh = side[1].h;
     H0 = set.b("sw_rel") ? H : translate((rw - lw) / 2, (rh - lh) / 2);
+}
+
+bool Engine::tune_sweep(double* out, size_t cap, size_t* used) {
+    if (!search_check()) return false;
+    SweepGrid gv;
+    int G;
+    Mat3 H0;
+    sweep_settings(gv, G, H0);
+    const bool exact = set.b("exact");
+    const double min_ov = std::min(0.5, std::max(0.0, set.f("min_overlap")));
+    const CorrPlanDev plan = corr_plan_dev(exact, side[0].mode == 1);
+    SweepOut probe;
+    if (!sweep_setup(H0, gv, G, probe)) return false;
+    // the plane classes and what one candidate's work buffers take
+    std::map<std::array<int, 2>, int> members;
+    for (const SweepCand& c : probe.cands) members[{c.nx, c.ny}]++;
+    auto per_item = [&](int nx, int ny) {
+        const size_t pstride = (size_t)ny * pitch_of(nx);
+        return (size_t)5 * (nx - probe.Fx + 1) * (ny - probe.Fy + 1) * 4 +
+               (size_t)(plan.n_real + plan.n_corr) * pstride * 8 + (size_t)nx * ny * 4;
+    };
+    static const int kOptions[] = {16, 32, 64, 128, 256, 512, 1024, 2048};
+    std::map<std::array<int, 2>, std::vector<std::pair<int, double>>> timed;  // class → (batch, ms per map)
+    struct Restore {
+        std::map<std::array<int, 2>, int>& f;
+        ~Restore() { f.clear(); }
+    } restore{sweep_force_};
+    for (int b : kOptions) {
+        sweep_force_.clear();
+        bool any = false;
+        for (const auto& kv : members) {
+            const size_t cap_b = std::max<size_t>(1, kTuneBudget / per_item(kv.first[0], kv.first[1]));
+            const int eb = (int)std::min<size_t>({(size_t)b, cap_b, (size_t)kv.second});
+            sweep_force_[kv.first] = eb;
+            const auto& seen = timed[kv.first];
+            if (std::none_of(seen.begin(), seen.end(), [&](const std::pair<int, double>& p) { return p.first == eb; }))
+                any = true;
+        }
+        if (!any) continue;
+        SweepOut r;
+        // one untimed run (buffers, caches), then the timed one
+        if (!sweep_maps(H0, gv, G, exact, 4, min_ov, r) || !sweep_maps(H0, gv, G, exact, 4, min_ov, r)) return false;
+        for (const auto& c : r.classes) {
+            const std::array<int, 2> key{(int)c[0], (int)c[1]};
+            auto& seen = timed[key];
+            if (std::none_of(seen.begin(), seen.end(), [&](const std::pair<int, double>& p) { return p.first == (int)c[3]; }))
+                seen.push_back({(int)c[3], c[4] / std::max(1.0, c[2])});
+        }
+    }
+    size_t n = 0;
+    auto put = [&](double v) {
+        if (out && n < cap) out[n] = v;
+        ++n;
+    };
+    std::string msg = "tune_sweep";
+    for (const auto& kv : timed) {
+        if (kv.second.empty()) continue;
+        const auto best = *std::min_element(kv.second.begin(), kv.second.end(),
+                                            [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+                                                return a.second < b.second;
+                                            });
+        sweep_tuned_[{kv.first[0], kv.first[1], plan.n_corr, exact ? 1 : 0}] = best.first;
+        put(kv.first[0]), put(kv.first[1]), put(members[kv.first]), put(best.first), put(best.second);
+        put((double)kv.second.size());
+        for (const auto& p : kv.second) put(p.first), put(p.second);
+        char b[96];
+        snprintf(b, sizeof b, "  %d×%d: batch %d (%.4f ms per map)", kv.first[0], kv.first[1], best.first, best.second);
+        msg += b;
+    }
+    log_event(msg);
+    if (used) *used = n;
+    return true;
 }
 
 bool Engine::search_check() {

@@ -27,9 +27,15 @@ inline bool fixed_line(int n) {
         if (v == n) return true;
     return false;
 }
-// threads per line of the row pass's policy for length L (FixedLine<L, L/8>, or the generic plan's)
+// threads per line of the row pass's compile-time lines: N/8 (8 points a thread), raised to 32
+// where N/8 is below 32 and does not divide it, so no short line shares a warp with part of
+// another (lines of 24 threads straddled warps: shared-memory bank conflicts between the two
+// lines' slots)
+__host__ __device__ constexpr int row_tpl(int n) { return (n / 8 >= 32 || 32 % (n / 8) == 0) ? n / 8 : 32; }
+// threads per line of the row pass's policy for length L (FixedLine<L, row_tpl(L)>, or the
+// generic plan's)
 inline int row_tl(int L) {
-    if (fixed_line(L)) return L / 8;
+    if (fixed_line(L)) return row_tpl(L);
     int tl = (L + 15) / 16;
     return ((tl + 31) / 32) * 32;
 }
@@ -558,7 +564,7 @@ cudaError_t run_fixed(Pass p, const float2* tw, const PassArgs& a, cudaStream_t 
         case Pass::FwdRows: return run_pass<Pass::FwdRows, FixedLine<N, N / 16>, SPLIT>(FixedLine<N, N / 16>{tw}, a, st);
         case Pass::FwdCols: return run_pass<Pass::FwdCols, FixedLine<N, N / 16>, SPLIT>(FixedLine<N, N / 16>{tw}, a, st);
         case Pass::InvCols: return run_pass<Pass::InvCols, FixedLine<N, N / 16>, SPLIT>(FixedLine<N, N / 16>{tw}, a, st);
-        default: return run_pass<Pass::Rows, FixedLine<N, N / 8>, SPLIT>(FixedLine<N, N / 8>{tw}, a, st);
+        default: return run_pass<Pass::Rows, FixedLine<N, row_tpl(N)>, SPLIT>(FixedLine<N, row_tpl(N)>{tw}, a, st);
     }
 }
 

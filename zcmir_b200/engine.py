@@ -432,6 +432,22 @@ class Engine:
             raise EngineError(f"sweep: the engine swept {int(d['candidates'])} candidates, expected {nc}")
         return SweepOut(sc, ix, d)
 
+    def tune_sweep(self) -> list:
+        """zcb_tune_sweep: the sweep's batch size per plane class, chosen by timing; one dict per
+        class (nx, ny, candidates, batch, ms_per_map, options: {batch: ms per map})."""
+        used = ctypes.c_size_t()
+        self.call("zcb_tune_sweep", None, 0, ctypes.byref(used))
+        buf = np.zeros(max(used.value, 1))
+        self.call("zcb_tune_sweep", _f64(buf), buf.size, ctypes.byref(used))
+        out, i = [], 0
+        while i + 6 <= used.value:
+            nx, ny, cnt, b, ms, k = buf[i:i + 6]
+            opts = {int(buf[i + 6 + 2 * j]): float(buf[i + 7 + 2 * j]) for j in range(int(k))}
+            out.append({"nx": int(nx), "ny": int(ny), "candidates": int(cnt), "batch": int(b), "ms_per_map": float(ms),
+                        "options": opts})
+            i += 6 + 2 * int(k)
+        return out
+
     def search_lanes(self, scores, index) -> SearchOut:
         """zcb_search_lanes: the search finished from (gathered) lane maxima."""
         sc = np.ascontiguousarray(scores, np.float32).ravel()
