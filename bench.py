@@ -141,6 +141,29 @@ def stage_bytes(p):
     }
 
 
+def sweep_work(tuned, Fx, Fy):
+    """(bytes, flops) of one whole sweep: per candidate of plane nx × ny (window cw × ch = nx − Fx + 1
+    × ny − Fy + 1, P = 15 real planes, C = 45 correlations) the bytes each pass reads and writes once
+    (pack → window stacks, forward rows → half spectra, columns in place, inverse columns → the
+    correlations' spectra, rows → map, peaks ← map) and the FP32 flops of the survey's counting rule
+    (moving side's forward FFT over its rows and columns, 23 inverse 2-D FFTs, products, score)."""
+    P, C, NC = 15, 45, 8
+    total_b = total_f = 0.0
+    for r in tuned:
+        nx, ny, k = r["nx"], r["ny"], r["candidates"]
+        cw, ch = nx - Fx + 1, ny - Fy + 1
+        half = (nx // 2 + 1) * 8
+        win = 5 * cw * ch * 4
+        b = (win + (win + P * ch * half) + (P * ch * half + P * ny * half) + (P * ny * half + C * ny * half)
+             + (C * ny * half + nx * ny * 4) + nx * ny * 4)
+        lx, ly = np.log2(nx), np.log2(ny)
+        f = (NC * 5 * (nx * lx * ch + ny * ly * nx) + ((C + 1) // 2) * 5 * nx * ny * np.log2(nx * ny)
+             + 10 * C * nx * ny + 300 * nx * ny)
+        total_b += k * b
+        total_f += k * f
+    return total_b, total_f
+
+
 def survey_bytes(p):
     """The whole map's compulsory HBM bytes (both stacks read, both sides' half spectra written and
     read once, the map written)."""
@@ -210,16 +233,18 @@ def run_sweep(reg_cls, args, barrier, dist, torch, ws):
     m, f = (m16 / 65535.0).astype(np.float32), (f16 / 65535.0).astype(np.float32)
     reg = reg_cls(**SWEEP_SETTINGS)
     reg.set_images(m, f, preprocess=False)
+    # the batch of every plane class chosen by the engine's autotuner (timed here, untimed below)
+    tuned = reg.tune_sweep()
     # N > 1: the candidates split across the ranks (strong scaling of one sweep)
     shard, nshard = (dist.get_rank(), ws) if dist else (0, 1)
     for _ in range(args.warmup):
-        reg.sweep(n_peak=4, batch=128, shard=shard, nshard=nshard)
+        reg.sweep(n_peak=4, shard=shard, nshard=nshard)
     barrier()
     with Clocks(torch.cuda.current_device()) as clk:
-        ms = [reg.sweep(n_peak=4, batch=128, shard=shard, nshard=nshard).info["ms"] for _ in range(args.steps)]
+        ms = [reg.sweep(n_peak=4, shard=shard, nshard=nshard).info["ms"] for _ in range(args.steps)]
     barrier()
     ms_step = float(np.mean(ms))
-    info = reg.sweep(n_peak=4, batch=128, shard=shard, nshard=nshard).info
+    info = reg.sweep(n_peak=4, shard=shard, nshard=nshard).info
     if dist:
         t = torch.tensor([ms_step], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -252,8 +277,22 @@ def run_sweep(reg_cls, args, barrier, dist, torch, ws):
     for x, y in [(1, 1), (512, 1), (512, 512), (1, 512)]:
         a, b = r.H @ [x, y, 1.0], H @ [x, y, 1.0]
         corner = max(corner, float(np.hypot(*(a[:2] / a[2] - b[:2] / b[2]))))
+    sb, sf = sweep_work(tuned, int(info["Fx"]), int(info["Fy"]))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    achieved = sb / nshard / (ms_step * 1e-3) / 1e9
     out = {"metric": "sweep poses/s", "value": info["candidates"] / (ms_step * 1e-3), "unit": "poses/s",
            "ms_per_step": ms_step, "scaling": "strong",
+           "tuned": [{k: r[k] for k in ("nx", "ny", "candidates", "batch", "ms_per_map")} for r in tuned],
+           "timing": "CUDA events around one replay of the sweep's captured CUDA graph",
+           "roofline": {"bound": "hbm", "kernel": "all sweep passes", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                        "frac": achieved / hbm, "traffic": None,
+                        "algorithmic_bytes_per_sweep": sb,
+                        "what": "bytes every pass of this decomposition reads and writes once per candidate "
+                                "(window stacks, half spectra, correlation spectra, maps), summed over the 3240",
+                        "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                        "fp32_flops_per_sweep": sf, "fp32_tflops": sf / nshard / (ms_step * 1e-3) / 1e12,
+                        "fp32_frac_of_nominal_75_tflops": sf / nshard / (ms_step * 1e-3) / 75e12},
            "config": dict(SWEEP_CONFIG, parallelism=f"candidates split over {ws} GPU(s), lane peaks all-reduced"),
            "launches_per_step": int(info["launches"]), "clocks": clk.summary(), "plane_sizes": int(info["groups"]), "batches": int(info["batches"]),
            "e2e": {"value": 1.0 / e2e_s, "unit": "searches/s", "seconds_per_search": e2e_s,

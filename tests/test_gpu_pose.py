@@ -169,3 +169,24 @@ def test_climb_roto_scale_hop(golden):
     assert "roto-scale hop" in labels, labels
     assert any("roto-scale hop+" in t for t in logs), logs
     assert corner_dist(r.H, H, mw, mh) < 1.0, corner_dist(r.H, H, mw, mh)
+
+
+def test_tune_parts_changes_the_launch_shape_not_the_scores():
+    """zc_tune_parts (the reference's knobs of its per-pixel sum kernels, src/exports.zig:115-121)
+    sets the pose kernels' pixels per thread and blocks per pose: the sums are added in another
+    order, so the scores agree within the pose tests' 1e-5; the defaults are put back after."""
+    from zcmir_b200 import _native
+
+    m, f, H = synth.pair_similarity(n=256, seed=7)
+    lib = _native.load()
+    with zc.Engine(half=False) as eng:
+        eng.set_images(m, f, preprocess=False)
+        ref = eng.score(H)
+        try:
+            for knobs in ((64, 0, 0, 0), (4, 0, 0, 0), (16, 600, 0, 0), (16, 1, 0, 8)):
+                lib.zc_tune_parts(*knobs)
+                s = eng.score(H)
+                assert abs(s.mean - ref.mean) <= 1e-5 * abs(ref.mean), (knobs, s, ref)
+        finally:
+            lib.zc_tune_parts(16, 1, 0, 4096)
+        assert abs(eng.score(H).mean - ref.mean) <= 1e-9 * abs(ref.mean)

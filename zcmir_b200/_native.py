@@ -90,6 +90,7 @@ SIGS = {
     "zc_ffd_gradient": ([P, f64p, f64p, f64p, SZ], I32),
     "zc_displacement": ([P, f32p, SZ], I32),
     "zc_result_sizes": ([u32p], None),
+    "zc_tune_parts": ([U32, U32, U32, U32], None),
     "zcb_bench_maps": ([P, f64p, U32, U32, U32, U32, f64p, SZ], I32),
     "zcb_score_static": ([P, f64p, U32, f64p], I32),
     "zcb_stack_maps": ([P, U32, ctypes.POINTER(f32p), u32p, u32p, f64p, U32, U32, ctypes.POINTER(ShiftResult), f64p], I32),

@@ -272,7 +272,13 @@ int32_t zc_bench_moments(zc_engine* e, uint32_t n_poses, uint32_t iters) {
     });
 }
 
-void zc_tune_parts(uint32_t, uint32_t, uint32_t, uint32_t) {}
+// The reference's knobs of its per-pixel sum kernels (src/exports.zig:115-121) mapped onto this
+// build's pose kernels: pixels per thread, the least blocks per pose (fill_wg), the most blocks
+// per pose (tg_cap); tg_px (the reference's pixels per tile group) has no counterpart, since a
+// warp here always takes an 8 × 4 tile. 0 keeps a knob's value.
+void zc_tune_parts(uint32_t px_per_thread, uint32_t fill_wg, uint32_t /*tg_px*/, uint32_t tg_cap) {
+    zc::pose_tune(px_per_thread, fill_wg, tg_cap);
+}
 
 int32_t zc_compile_wgsl(zc_engine*, const char*, size_t, const char*, size_t, char*, size_t) {
     return -1;  // "unsupported here" (python/zcmir/__init__.py:315-325)

@@ -177,6 +177,10 @@ struct PoseFfd {
 };
 // the 45 sums of n poses of one direction (a sampled at H⁻¹x for every b pixel x); hinv: n
 // inverse poses (f32, row-major); sums: n × 45 float64 (zeroed here)
+// The pose kernels' launch shape (zc_tune_parts): pixels per thread, the least and the most
+// blocks per pose (0 keeps the current value). It changes the order of the cross-block sums, so
+// scores move within their float32 rounding.
+void pose_tune(unsigned px_per_thread, unsigned min_blocks, unsigned max_blocks);
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
                          const PoseFfd& ffd = {});
 // score (float64) and the 102 gradient coefficients (f32) of each pose's sums

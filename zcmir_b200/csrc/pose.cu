@@ -8,6 +8,7 @@
 // features bilinearly at H⁻¹(x + 1) − 1, weighted by a 2-px ramp inside a's valid border. Blocks
 // of pose p sum their pixels in float32 per thread, then float64 across the block, and add into
 // the pose's float64 sums.
+#include <atomic>
 #include <algorithm>
 
 #include "common.cuh"
@@ -885,11 +886,17 @@ __global__ void __launch_bounds__(256) k_pose_ffd_cells(const float4* __restrict
 // wave, or b a whole number of waves) — a wave and a few blocks would take two waves' time. The
 // count depends on the image alone, never on how many poses share the launch, so a pose's sums
 // (and score) are the same whatever batch it is scored in.
+// zc_tune_parts' knobs (0 keeps the default): pixels per thread (16), the least and the most
+// blocks per pose (none, 4096)
+std::atomic<unsigned> g_px_per_thread{16}, g_min_blocks{0}, g_max_blocks{4096};
+
 int pose_blocks(size_t pixels, int slots) {
-    const size_t by_work = std::max<size_t>(1, (pixels + 256 * 16 - 1) / (256 * 16));
+    const size_t ppt = std::max(1u, g_px_per_thread.load(std::memory_order_relaxed));
+    const size_t by_work = std::max<size_t>(1, (pixels + 256 * ppt - 1) / (256 * ppt));
     const size_t sl = (size_t)std::max(slots, 1);
-    const size_t b = by_work >= sl ? sl * (by_work / sl) : sl / ((sl + by_work - 1) / by_work);
-    return (int)std::max<size_t>(1, std::min<size_t>(b, 4096));
+    size_t b = by_work >= sl ? sl * (by_work / sl) : sl / ((sl + by_work - 1) / by_work);
+    b = std::max<size_t>(b, g_min_blocks.load(std::memory_order_relaxed));
+    return (int)std::max<size_t>(1, std::min<size_t>(b, std::max(1u, g_max_blocks.load(std::memory_order_relaxed))));
 }
 
 // resident blocks of 256 threads of kernel k across the GPU
@@ -910,6 +917,12 @@ __global__ void k_feat_interleave(const float* __restrict__ feat, int n, float4*
         out[i] = make_float4(feat[i], feat[(size_t)n + i], feat[2 * (size_t)n + i], feat[3 * (size_t)n + i]);
 }
 }  // namespace
+
+void pose_tune(unsigned px_per_thread, unsigned min_blocks, unsigned max_blocks) {
+    if (px_per_thread) g_px_per_thread = std::min(px_per_thread, 4096u);
+    if (min_blocks) g_min_blocks = std::min(min_blocks, 4096u);
+    if (max_blocks) g_max_blocks = std::min(max_blocks, 4096u);
+}
 
 cudaError_t interleave_features(const float* feat, int n, float4* out, cudaStream_t st) {
     const int blocks = std::min((n + 255) / 256, 148 * 8);
