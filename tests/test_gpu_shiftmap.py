@@ -250,3 +250,53 @@ def test_bench_maps_graph_replay_leaves_the_map_unchanged(c1_pair):
     assert not any("graph replay unavailable" in t for t in ev), ev
     assert (after.dx, after.dy, after.peak_index) == (before.dx, before.dy, before.peak_index)
     np.testing.assert_array_equal(after.map, before.map)
+
+
+def test_maps_reuse_each_sides_spectra(c1_pair):
+    """A side's canvas and half spectra are built once and reused by the next map whose canvas,
+    plan and (for the moving side) canvas pose are the same: the calibrated map after the
+    uncalibrated one at the same pose, the map at a pose that keeps the moving image inside the
+    fixed frame (the fixed side is reused). Every reused map equals the map of a fresh engine,
+    value for value, and launches fewer kernels; new images, a roto-scale map in between and new
+    feature settings rebuild what they must."""
+    m, f, _ = c1_pair
+    c = 128.5
+    T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
+    a = np.deg2rad(1.5)
+    inside = T(c, c) @ np.array([[0.96 * np.cos(a), -0.96 * np.sin(a), 0], [0.96 * np.sin(a), 0.96 * np.cos(a), 0],
+                                 [0, 0, 1]]) @ T(-c, -c)
+
+    def fresh(H, **kw):
+        with zc.Engine(half=False) as e:
+            e.set_images(m, f, preprocess=False)
+            return e.shift_map(H, cap=1024, **kw)
+
+    with zc.Engine(half=False) as eng:
+        eng.set_images(m, f, preprocess=False)
+        first = eng.shift_map(np.eye(3), exact=True, calibrated=False, cap=1024)
+        eng.gpu_counts()
+        again = eng.shift_map(np.eye(3), exact=True, calibrated=True, cap=1024)
+        n_both = eng.gpu_counts()["launches"]
+        moved = eng.shift_map(inside, exact=True, calibrated=True, cap=1024)
+        n_fixed = eng.gpu_counts()["launches"]
+        eng.rs_map(np.eye(3), want_maps=False)
+        eng.gpu_counts()
+        after_rs = eng.shift_map(inside, exact=True, calibrated=True, cap=1024)
+        n_none = eng.gpu_counts()["launches"]
+        assert n_both < n_fixed < n_none, (n_both, n_fixed, n_none)
+        np.testing.assert_array_equal(first.map, fresh(np.eye(3), exact=True, calibrated=False).map)
+        np.testing.assert_array_equal(again.map, fresh(np.eye(3), exact=True, calibrated=True).map)
+        ref_moved = fresh(inside, exact=True, calibrated=True)
+        np.testing.assert_array_equal(moved.map, ref_moved.map)
+        np.testing.assert_array_equal(after_rs.map, ref_moved.map)
+        # new images and new feature settings: both sides rebuilt
+        eng.set_images(f, m, preprocess=False)
+        swapped = eng.shift_map(np.eye(3), exact=True, calibrated=True, cap=1024)
+        with zc.Engine(half=False) as e2:
+            e2.set_images(f, m, preprocess=False)
+            np.testing.assert_array_equal(swapped.map, e2.shift_map(np.eye(3), exact=True, calibrated=True, cap=1024).map)
+        eng.configure(smi_features="three")
+        three = eng.shift_map(np.eye(3), exact=True, calibrated=True, cap=1024)
+        with zc.Engine(half=False, smi_features="three") as e3:
+            e3.set_images(f, m, preprocess=False)
+            np.testing.assert_array_equal(three.map, e3.shift_map(np.eye(3), exact=True, calibrated=True, cap=1024).map)

@@ -24,6 +24,7 @@ cudaError_t DevBuf::ensure(size_t bytes) {
         return e;
     }
     cap = want;
+    ++gen;
     return cudaSuccess;
 }
 
@@ -72,6 +73,7 @@ CorrPlanDev corr_plan_dev(bool exact, bool three) {
 
 Engine::Engine(int dev) : device(dev) {
     if (const char* v = getenv("ZCMIR_B200_ROW_PASS")) row_pass = v;
+    if (const char* v = getenv("ZCMIR_B200_SPECTRA_CACHE")) spectra_cache_ = atoi(v) != 0;
     cudaSetDevice(dev);
     cudaGetDeviceProperties(&prop, dev);
     // priorities: side 1's feature build (st2_) highest, so it is not starved by side 0's passes
@@ -259,6 +261,7 @@ bool Engine::build_stream(int s, cudaStream_t& bs) {
 
 bool Engine::build_side(int s) {
     Side& sd = side[s];
+    sd.ver = ++build_counter_;
     const size_t n = (size_t)sd.w * sd.h;
     cudaStream_t bs = st;
     if (!build_stream(s, bs)) return false;
@@ -559,23 +562,65 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
         return cuda_ok(forward_cols((s == 0 ? half_a_ : half_b_).as<float2>(), g, job.plan, job.col, st),
                        "forward columns");
     };
+    // Each side's canvas, grid and half spectra depend on its feature build, the canvas frame and
+    // plan, the buffers they live in and, for the moving side, the canvas pose: with the same key
+    // as the last map that built them, they are still in the buffers and are reused.
+    auto side_key = [&](int s) {
+        std::vector<uint64_t> k;
+        const DevBuf &cv = s == 0 ? canvas_a_ : canvas_b_, &gd = s == 0 ? grid_a_ : grid_b_,
+                     &hf = s == 0 ? half_a_ : half_b_;
+        for (const DevBuf* b : {&cv, &gd, &hf}) k.push_back((uint64_t)(uintptr_t)b->p), k.push_back(b->gen);
+        for (int v : {s, side[s].mode, (int)side[s].half, g.W, g.Hh, g.ox, g.oy, g.cw, g.ch, g.nx, g.ny, g.WP,
+                      (int)job.identity_grid, job.plan.n_real})
+            k.push_back((uint64_t)(int64_t)v);
+        k.push_back(side[s].ver);
+        for (int i = 0; i < job.plan.n_real; ++i) k.push_back((uint64_t)job.plan.planes[i]);
+        if (s == 0) {
+            for (int i = 0; i < 9; ++i) {
+                uint64_t u;
+                memcpy(&u, &job.Hc[i], 8);
+                k.push_back(u);
+            }
+            k.push_back(okdet ? 1 : 0);
+        }
+        return k;
+    };
+    const bool use_cache = spectra_cache_ && !spectra_cache_off_;
+    std::vector<uint64_t> key[2] = {side_key(0), side_key(1)};
+    const bool have[2] = {use_cache && key[0] == spec_key_[0], use_cache && key[1] == spec_key_[1]};
+    // a kept side still needs its grid for the zero-lag overlap (its canvas is still in place)
+    auto kept_grid = [&](int s, const float*& grid) {
+        grid = (s == 0 ? canvas_a_ : canvas_b_).as<float>();
+        if (!job.identity_grid) grid = (s == 0 ? grid_a_ : grid_b_).as<float>();
+        return true;
+    };
+    auto side_canvas = [&](int s, const float*& grid) { return have[s] ? kept_grid(s, grid) : canvas_side(s, grid); };
+    auto side_rows = [&](int s, const float* grid) { return have[s] || rows_of(s, grid); };
+    auto side_cols = [&](int s) {
+        if (have[s]) return true;
+        if (!cols_of(s)) return false;
+        spec_key_[s] = key[s];
+        return true;
+    };
+    for (int s = 0; s < 2; ++s)
+        if (!have[s]) spec_key_[s].clear();  // until this side's passes are queued
     const float *ga = nullptr, *gb = nullptr;
     if (!join_side(0)) return false;
     if (ev) {
         // in stage order, so each stage's events bracket its own passes
         if (!join_side(1)) return false;
         rec(0);
-        if (!canvas_side(0, ga) || !canvas_side(1, gb) || !lag0(ga, gb)) return false;
+        if (!side_canvas(0, ga) || !side_canvas(1, gb) || !lag0(ga, gb)) return false;
         rec(1);
-        if (!rows_of(0, ga) || !rows_of(1, gb)) return false;
+        if (!side_rows(0, ga) || !side_rows(1, gb)) return false;
         rec(2);
-        if (!cols_of(0) || !cols_of(1)) return false;
+        if (!side_cols(0) || !side_cols(1)) return false;
         rec(3);
     } else {
         // side 0's passes first: they need only its own build, so they run while side 1's build
         // (on a stream of its own) may still be going; then the wait for it and side 1's passes
-        if (!canvas_side(0, ga) || !rows_of(0, ga) || !cols_of(0) || !join_side(1) || !canvas_side(1, gb) ||
-            !lag0(ga, gb) || !rows_of(1, gb) || !cols_of(1))
+        if (!side_canvas(0, ga) || !side_rows(0, ga) || !side_cols(0) || !join_side(1) || !side_canvas(1, gb) ||
+            !lag0(ga, gb) || !side_rows(1, gb) || !side_cols(1))
             return false;
     }
     if (!cuda_ok(inverse_columns(half_a_.as<float2>(), half_b_.as<float2>(), g, job.plan, job.col, q_.as<float2>(), st,
@@ -625,7 +670,8 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
                         "inverse rows"))
         return false;
     rec(5);
-    counts[0] += job.identity_grid ? 10 : 12;
+    counts[0] += (job.identity_grid ? 10 : 12) - (have[0] ? (job.identity_grid ? 3 : 4) : 0) -
+                 (have[1] ? (job.identity_grid ? 3 : 4) : 0);
     return true;
 }
 
@@ -761,6 +807,12 @@ double Engine::graph_maps(MapJob& job, unsigned warmup, unsigned steps, size_t f
 bool Engine::bench_maps(const Mat3& Hm, unsigned flags, unsigned cap, unsigned warmup, unsigned steps, double* out,
                         size_t out_len) {
     if (out_len < 16) return fail("bench_maps: output needs 16 doubles");
+    // every timed map builds both sides' spectra: the benchmark times whole maps
+    struct NoReuse {
+        bool& f;
+        explicit NoReuse(bool& x) : f(x) { f = true; }
+        ~NoReuse() { f = false; }
+    } no_reuse(spectra_cache_off_);
     MapJob job;
     if (!plan_map(Hm, (flags & 1) != 0, (flags & 2) != 0, cap, 0.0, job)) return false;
     // an L2 flush between timed maps: write a buffer larger than the 126 MB L2

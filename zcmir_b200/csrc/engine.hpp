@@ -23,6 +23,7 @@ namespace zc {
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
+    uint64_t gen = 0;  // bumped by every (re)allocation: contents from before it are gone
     cudaError_t ensure(size_t bytes);
     void release();
     template <class T>
@@ -76,6 +77,7 @@ struct Side {
     int mode = -1;
     bool half = false;
     std::string bake;  // the preprocessing settings the work image was made with
+    uint64_t ver = 0;  // which build the feature planes come from (unique per engine)
 };
 
 // Scores (and optionally the symmetric gradient and Gauss–Newton matrix) at one pose.
@@ -295,6 +297,17 @@ class Engine {
     cudaGraphExec_t sweep_exec_ = nullptr;
     std::vector<uint64_t> sweep_sig_;
     int sweep_launches_ = 0;  // kernels one replay of sweep_exec_ launches
+    // What the map's canvas / grid / half-spectrum buffers of each side hold (empty: nothing
+    // known): a map whose side has the same key reuses them instead of rebuilding that side's
+    // canvas and forward transforms. Cleared by every other user of those buffers.
+    std::array<std::vector<uint64_t>, 2> spec_key_;
+    bool spectra_cache_ = true;     // ZCMIR_B200_SPECTRA_CACHE=0 at creation: always rebuild
+    bool spectra_cache_off_ = false;  // set while a benchmark times whole maps
+    uint64_t build_counter_ = 0;
+    void forget_spectra() {
+        spec_key_[0].clear();
+        spec_key_[1].clear();
+    }
     // while tuning: batch per plane class (nx, ny), stream-ordered launches timed per class
     std::map<std::array<int, 2>, int> sweep_force_;
     // time each candidate batch size per plane class of the current sweep settings, keep the

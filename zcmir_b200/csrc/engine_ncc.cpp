@@ -90,6 +90,7 @@ bool Engine::ncc_shift_map(const Mat3& H, zc_shift_result* out, float* map, size
     if (!tw) return fail("shift_map: twiddles: out of device memory");
     const size_t cn = (size_t)g.W * g.Hh, gn = (size_t)g.cw * g.ch;
     const size_t hs = (size_t)g.ny * g.WP * sizeof(float2);
+    forget_spectra();  // this map writes the map path's canvas and spectrum buffers
     bool ok = cuda_ok(canvas_a_.ensure(cn * 4), "shift_map") && cuda_ok(canvas_b_.ensure(cn * 4), "shift_map") &&
               cuda_ok(grid_a_.ensure(gn * 20), "shift_map") && cuda_ok(grid_b_.ensure(gn * 20), "shift_map") &&
               cuda_ok(half_a_.ensure(hs), "shift_map") && cuda_ok(half_b_.ensure(hs), "shift_map") &&

@@ -75,6 +75,7 @@ bool Engine::rs_map_one(const Mat3& H, const double c[2], double r0_opt, double 
     const size_t cn = (size_t)fr.w * fr.h, gn = (size_t)p.n_th * p.n_lam, nn = (size_t)p.n * p.n;
     const size_t hs = (size_t)plan.n_real * g.ny * g.WP * sizeof(float2);
     const size_t qs = (size_t)plan.n_corr * g.ny * g.WP * sizeof(float2);
+    forget_spectra();  // this map writes the map path's canvas and spectrum buffers
     bool ok = cuda_ok(canvas_a_.ensure(cn * 20), "rs_map") && cuda_ok(canvas_b_.ensure(cn * 20), "rs_map") &&
               cuda_ok(grid_a_.ensure(gn * 20), "rs_map") && cuda_ok(grid_b_.ensure(gn * 20), "rs_map") &&
               cuda_ok(half_a_.ensure(hs), "rs_map") && cuda_ok(half_b_.ensure(hs), "rs_map") &&
