@@ -141,6 +141,39 @@ def stage_bytes(p):
     }
 
 
+def reuse_maps(reg, torch, args):
+    """Maps through the public call (features resident, map left on the device) when a side's
+    spectra are still in place: the moving image turned and shrunk about its centre so it stays
+    inside the fixed frame (the fixed side's canvas and spectra reused, the moving side's rebuilt
+    at every new pose), and the calibrated map right after the uncalibrated one at one pose (both
+    sides reused). Wall time per map, each call synchronised; not the headline, which rebuilds
+    both sides in every timed map."""
+    c = 512.5
+    T = lambda x, y: np.array([[1, 0, x], [0, 1, y], [0, 0, 1.0]])
+
+    def pose(k):
+        a, s = np.deg2rad(0.2 * (k % 7 + 1)), 0.97 - 0.001 * (k % 5)
+        return T(c, c) @ np.array([[s * np.cos(a), -s * np.sin(a), 0], [s * np.sin(a), s * np.cos(a), 0], [0, 0, 1]]) @ T(-c, -c)
+
+    n = max(5, args.steps // 2)
+    for k in range(3):
+        reg.shift_map(pose(k), exact=True, calibrated=True, cap=2048, want_map=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(n):
+        reg.shift_map(pose(k + 3), exact=True, calibrated=True, cap=2048, want_map=False)
+    fixed_s = (time.perf_counter() - t0) / n
+    both_s = 0.0
+    for k in range(n):
+        reg.shift_map(pose(100 + k), exact=True, calibrated=False, cap=2048, want_map=False)
+        t1 = time.perf_counter()
+        reg.shift_map(pose(100 + k), exact=True, calibrated=True, cap=2048, want_map=False)
+        both_s += time.perf_counter() - t1
+    both_s /= n
+    return {"fixed_side_reused_maps_s": 1.0 / fixed_s, "both_sides_reused_maps_s": 1.0 / both_s,
+            "timing": "wall clock per synchronised shift_map call, map not copied back"}
+
+
 def sweep_work(tuned, Fx, Fy):
     """(bytes, flops) of one whole sweep: per candidate of plane nx × ny (window cw × ch = nx − Fx + 1
     × ny − Fy + 1, P = 15 real planes, C = 45 correlations) the bytes each pass reads and writes once
@@ -320,13 +353,14 @@ def run_proposal(reg_cls, m, f, H, reps=3):
         for _ in range(reps + 1):
             reg.pose = np.eye(3)
             t0 = time.perf_counter()
+            fb = False
             if name == "plain":
                 Hs, maps = P._with(reg, P.fine_settings(), reg.search).H, P.FINE_NTH * P.FINE_NS
             else:
                 r = P.search(reg, net, with_network=name == "proposal")
-                Hs, maps = r["H"], r["maps"]
+                Hs, maps, fb = r["H"], r["maps"], r["fallback"]
             ts.append(time.perf_counter() - t0)
-        out[name] = {"seconds_per_search": float(np.mean(ts[1:])), "maps": maps,
+        out[name] = {"seconds_per_search": float(np.mean(ts[1:])), "maps": maps, "plain_sweep_fallback": fb,
                      "corner_rms_px": P.corner_rms(np.asarray(Hs), H, mw, mh)}
     reg.close()
     return out
@@ -453,6 +487,7 @@ def run_gpu(args, rank, ws, local):
     reg.configure(smi_features="three")
     r28 = reg.bench_maps(np.eye(3), flags=3, cap=2048, warmup=1, steps=max(3, args.steps // 2))
     reg.configure(smi_features="laplacian")
+    reuse = reuse_maps(reg, torch, args)
 
     # e2e: the public API from pinned host buffers, map back into pinned host memory
     pm = torch.empty(m.shape, dtype=torch.float32, pin_memory=True).numpy()
@@ -501,7 +536,8 @@ def run_gpu(args, rank, ws, local):
                               "stages_ms": r["stages_ms"],
                               "timing": "CUDA events around replays of one captured CUDA graph of the map's passes; "
                                         "stages_ms from event-instrumented maps",
-                              "ms_per_map_instrumented": r.get("ms_per_map_instrumented")}),
+                              "ms_per_map_instrumented": r.get("ms_per_map_instrumented"),
+                              "spectra_reuse": reuse}),
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel from a capture "

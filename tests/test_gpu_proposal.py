@@ -90,10 +90,34 @@ def test_trained_network_gains_over_the_landscape_alone():
             reg.pose = np.eye(3)
             out = P.search(reg, net)
             ep.append(P.corner_rms(out["H"], Ht, mw, mh))
-            assert out["maps"] == 112
+            assert out["maps"] == 113 + (3240 if out["fallback"] else 0)
             reg.pose = np.eye(3)
             keep = {k: reg.settings[k] for k in P.fine_settings()}
             reg.configure(**P.fine_settings())
             er.append(P.corner_rms(reg.search().H, Ht, mw, mh))
             reg.configure(**keep)
     assert np.median(ep) <= np.median(er) + 0.2, (ep, er)
+
+
+def test_plain_sweep_fallback_when_the_network_misleads():
+    """An untrained network proposes cells that refine to less SMI than the coarse sweep's own
+    best candidate: the search then falls back to the plain full sweep, and lands where the plain
+    search lands."""
+    import zcmir_b200 as zc
+    bad = P.Network(seed=123)
+    with zc.Engine(half=False) as reg:
+        used = []
+        for sd in range(200_010, 200_013):
+            m, f, Ht = P.make_pair(sd)
+            reg.set_images(m, f, preprocess=False)
+            mh, mw = m.shape
+            reg.pose = np.eye(3)
+            out = P.search(reg, bad)
+            used.append(out["fallback"])
+            if out["fallback"]:
+                assert out["maps"] == 113 + 3240
+                reg.pose = np.eye(3)
+                plain = P._with(reg, P.fine_settings(), reg.search)
+                assert out["score"] >= plain.score * (1 - 1e-6)
+                assert P.corner_rms(out["H"], Ht, mw, mh) <= P.corner_rms(plain.H, Ht, mw, mh) + 0.2
+        assert any(used), used

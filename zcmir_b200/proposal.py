@@ -203,29 +203,46 @@ def landscape(reg):
     return features(sw.scores), sw
 
 
-def search(reg, net, k=4, with_network=True, iters=25):
+def coarse_pose(reg, c):
+    """The pose of coarse sweep candidate c (θ-major over 36 rotations × 3 scales)."""
+    it, js = divmod(int(c), COARSE_NS)
+    sigma = math.exp(math.log(S_MIN) + (math.log(S_MAX) - math.log(S_MIN)) * js / (COARSE_NS - 1))
+    return candidate_pose(reg, -180.0 + 360.0 * it / COARSE_NTH, sigma)
+
+
+def search(reg, net, k=4, with_network=True, iters=25, fallback=True):
     """The proposal search on the pair loaded in reg from its current pose. Both forms map the
     coarse 36 × 3 grid. Without the network, the coarse search: the coarse sweep's peaks screened
     and climbed (the plain search's own steps on the coarse grid). With it, the network's top-k
-    cells of the plain sweep's fine grid, each placed by one shift map and refined by
-    Gauss–Newton together. The result becomes the pose when it beats the current one. Returns
-    dict(H, score, maps)."""
+    cells of the plain sweep's fine grid and the coarse sweep's own best candidate, each placed by
+    one shift map and refined by Gauss–Newton together; when the coarse candidate ends with the
+    higher pair score (the network's seeds refined to less SMI than the sweep's own best), the
+    plain full search runs as the fallback and the better of the two is kept. The result becomes
+    the pose when it beats the current one. Returns dict(H, score, maps, fallback)."""
     cur = reg.score().mean
     if not with_network:
         r = _with(reg, coarse_settings(), lambda: reg.search_lanes(*_lanes(reg.sweep())))
-        return dict(H=np.asarray(r.H), score=r.score, maps=COARSE_NTH * COARSE_NS)
+        return dict(H=np.asarray(r.H), score=r.score, maps=COARSE_NTH * COARSE_NS, fallback=False)
     sw = _with(reg, coarse_settings(), reg.sweep)
+    starts = [candidate_pose(reg, *bin_pose(b)) for b in net.top(features(sw.scores), k)]
+    starts.append(coarse_pose(reg, int(np.argmax(sw.scores[:, 0]))))
     seeds = []
-    for b in net.top(features(sw.scores), k):
-        H = candidate_pose(reg, *bin_pose(b))
+    for H in starts:
         sm = reg.shift_map(H, want_map=False)
         seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
     Hs, sc = reg.refine_poses(np.array(seeds), iters)
     i = int(np.argmax(sc))
     best_H, best_s = np.asarray(Hs[i]), float(sc[i])
-    if best_s > cur + max(1e-6 * abs(cur), 1e-12):
-        reg.pose = best_H
-    return dict(H=best_H, score=best_s, maps=COARSE_NTH * COARSE_NS + len(seeds))
+    maps = COARSE_NTH * COARSE_NS + len(seeds)
+    used_fallback = fallback and float(sc[-1]) > float(np.max(sc[:-1]))
+    if used_fallback:
+        reg.pose = np.eye(3)
+        r = _with(reg, fine_settings(), reg.search)
+        maps += FINE_NTH * FINE_NS
+        if r.score > best_s:
+            best_H, best_s = np.asarray(r.H), float(r.score)
+    reg.pose = best_H if best_s > cur + max(1e-6 * abs(cur), 1e-12) else reg.pose
+    return dict(H=best_H, score=best_s, maps=maps, fallback=used_fallback)
 
 
 def _lanes(sw):
@@ -314,16 +331,19 @@ def _eval_main(a):
                 t0 = time.perf_counter()
                 if name == "plain":
                     H, maps = _with(reg, fine_settings(), reg.search).H, FINE_NTH * FINE_NS
+                    fb = False
                 else:
                     out = search(reg, net, k=a.k, with_network=name == "proposal")
-                    H, maps = out["H"], out["maps"]
-                r[name] = dict(err=corner_rms(H, Ht, mw, mh), s=time.perf_counter() - t0, maps=maps)
+                    H, maps, fb = out["H"], out["maps"], out["fallback"]
+                r[name] = dict(err=corner_rms(H, Ht, mw, mh), s=time.perf_counter() - t0, maps=maps, fallback=fb)
             rows.append(r)
     summ = {}
     for name in ("plain", "coarse", "proposal"):
         e = np.array([r[name]["err"] for r in rows])
         summ[name] = dict(success=float(np.mean(e <= 0.5)), median_err=float(np.median(e)),
-                          s_per_search=float(np.mean([r[name]["s"] for r in rows])), maps=rows[0][name]["maps"])
+                          s_per_search=float(np.mean([r[name]["s"] for r in rows])),
+                          maps_mean=float(np.mean([r[name]["maps"] for r in rows])),
+                          fallbacks=int(sum(r[name]["fallback"] for r in rows)))
     print(json.dumps({"pairs": a.pairs, "first_seed": a.first, "k": a.k, "summary": summ,
                       "errors": {n: [round(r[n]["err"], 3) for r in rows] for n in ("plain", "coarse", "proposal")}}))
 
