@@ -190,3 +190,34 @@ def test_tune_parts_changes_the_launch_shape_not_the_scores():
         finally:
             lib.zc_tune_parts(16, 1, 0, 4096)
         assert abs(eng.score(H).mean - ref.mean) <= 1e-9 * abs(ref.mean)
+
+
+def test_device_refine_equals_the_host_loop(monkeypatch):
+    """The batched Gauss–Newton refine (zcb_refine_poses, and the search's screening and final
+    refines) runs on the device by default; ZCMIR_B200_GN=host runs the same loop on the host.
+    The device kernels restate the host's float64 pose algebra without fused multiply-adds, so
+    both take the same steps: the poses and scores agree to the last few bits (the pose sums are
+    float64 atomics across blocks, added in whatever order the blocks finish)."""
+    m, f, H = synth.pair_similarity(n=256, seed=7)
+    rng = np.random.default_rng(3)
+    starts = [_near(H, th=rng.uniform(-4, 4), s=rng.uniform(0.97, 1.03), t=rng.uniform(-3, 3, 2)) for _ in range(8)]
+
+    def run():
+        with zc.Engine(half=False, sw_nth=72, sw_ns=3) as eng:
+            eng.set_images(m, f, preprocess=False)
+            poses, scores = eng.refine_poses(starts, iters=12)
+            s = eng.search()
+        return poses, scores, s
+
+    dp, ds, dsr = run()
+    monkeypatch.setenv("ZCMIR_B200_GN", "host")
+    hp, hs, hsr = run()
+    np.testing.assert_allclose(ds, hs, rtol=1e-9, atol=0)
+    np.testing.assert_allclose(dp, hp, rtol=0, atol=1e-9 * np.abs(hp).max())
+    np.testing.assert_allclose(dsr.H, hsr.H, rtol=0, atol=1e-9 * np.abs(hsr.H).max())
+    assert abs(dsr.score - hsr.score) <= 1e-9 * abs(hsr.score)
+    # every start climbed: no score below its start's
+    with zc.Engine(half=False) as eng:
+        eng.set_images(m, f, preprocess=False)
+        s0 = np.array([eng.score(h).mean for h in starts])
+    assert np.all(ds >= s0 - 1e-9 * np.abs(s0)), (ds, s0)

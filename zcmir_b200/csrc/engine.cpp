@@ -125,6 +125,8 @@ Engine::~Engine() {
         b->release();
     pose_in_pin_.release();
     pose_out_pin_.release();
+    gn_pin_.release();
+    for (DevBuf* b : {&gn_H_, &gn_Htry_, &gn_valid_, &gn_active_, &gn_cur_}) b->release();
     for (auto& kv : tw_) cudaFree(kv.second);
     for (cudaEvent_t e : chunk_ev_)
         if (e) cudaEventDestroy(e);

@@ -308,6 +308,9 @@ class Engine {
         spec_key_[0].clear();
         spec_key_[1].clear();
     }
+    // the batched Gauss–Newton refine's device state (gn_batch_dev)
+    DevBuf gn_H_, gn_Htry_, gn_valid_, gn_active_, gn_cur_;
+    PinnedBuf gn_pin_;
     // while tuning: batch per plane class (nx, ny), stream-ordered launches timed per class
     std::map<std::array<int, 2>, int> sweep_force_;
     // time each candidate batch size per plane class of the current sweep settings, keep the
@@ -326,6 +329,10 @@ class Engine {
     bool search_lanes(const float* scores, const uint32_t* idx, size_t n, zc_search_result* out);
     bool search_check();
     // Gauss–Newton on many poses at once (src/search.zig gnBatch)
+    // gn_batch run on the device (gn_device.cu): no host round trip inside a batch of
+    // iterations; one read of the poses' moved flags per batch (ZCMIR_B200_GN=host: the host loop)
+    bool gn_batch_dev(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
+                      std::vector<ScoredPose>& out);
     bool gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
                   std::vector<ScoredPose>& out);
     // zc_match without keypoints: the SMI sweep search from the images' centres aligned gives

@@ -21,6 +21,7 @@ namespace {
 constexpr size_t kSweepBudget = 1ull << 30;  // device bytes of one batch's work buffers
 constexpr int kSweepMaxBatch = 128;
 constexpr size_t kTuneBudget = 8ull << 30;  // device bytes of one batch's work buffers while tuning
+constexpr int kMom = 45, kCoef = 102, kGrad = 44;  // per pose: moment sums, coefficients, tangent sums
 
 size_t pitch_of(int nx) { return (size_t)((nx / 2 + 1) + 7) / 8 * 8; }
 
@@ -406,8 +407,115 @@ void Engine::sweep_make_peaks(SweepOut& out, int n_peak) {
     }
 }
 
+// gn_batch with the loop on the device: per iteration the poses' inverse maps, their moments,
+// coefficients and tangent sums (masked to the poses still moving), then one warp per pose builds
+// the candidates (k_gn_propose), the candidates are scored, and k_gn_select keeps the first that
+// beats each pose's score. The host reads the moved flags once per kGnBatch iterations, to stop
+// when no pose moves; the iterations past the last move only launch masked-out kernels.
+bool Engine::gn_batch_dev(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
+                          std::vector<ScoredPose>& out) {
+    out.clear();
+    if (Hs.empty()) return true;
+    if (!need_images() || !metric_ok("score")) return false;
+    const bool homog = set.e("group") == "homography", sym = set.b("symmetric"), exact = set.b("exact");
+    const Side &A = side[0], &B = side[1];
+    GnAmps ga{};
+    ga.n = (int)amps.size();
+    for (int k = 0; k < ga.n; ++k) ga.v[k] = amps[k];
+    const int n = (int)Hs.size(), nd = sym ? 2 : 1;
+    const GnDims d{n, ga.n + 5, n_keys(homog), homog ? 1 : 0, sym ? 1 : 0, A.w, A.h, B.w, B.h};
+    const size_t nt = (size_t)n * d.T, mt = (size_t)nd * nt, m = (size_t)nd * n;
+    const size_t act_b = (size_t)(n + 15) / 16 * 16;
+    bool ok = cuda_ok(gn_H_.ensure((size_t)n * 9 * 8), "refine") && cuda_ok(gn_Htry_.ensure(nt * 9 * 8), "refine") &&
+              cuda_ok(gn_valid_.ensure(nt), "refine") && cuda_ok(gn_active_.ensure(act_b), "refine") &&
+              cuda_ok(gn_cur_.ensure((size_t)n * 8), "refine") && cuda_ok(pose_hinv_.ensure(mt * 9 * 4), "refine") &&
+              cuda_ok(pose_sums_.ensure(mt * kMom * 8), "refine") &&
+              cuda_ok(pose_coef_.ensure(mt * kCoef * 4), "refine") && cuda_ok(pose_score_.ensure(mt * 8), "refine") &&
+              cuda_ok(pose_tsum_.ensure(m * kGrad * 8), "refine") && cuda_ok(pose_gens_.ensure(2 * 72 * 4), "refine") &&
+              cuda_ok(gn_pin_.ensure((size_t)n * 9 * 8 + (size_t)n * 8 + act_b + 2 * 72 * 4), "refine");
+    if (!ok) return false;
+    // page-locked staging: poses (f64), scores (f64), moved flags, generators (f32)
+    double* hH = gn_pin_.as<double>();
+    double* hcur = hH + (size_t)n * 9;
+    unsigned char* hact = reinterpret_cast<unsigned char*>(hcur + n);
+    float* hgens = reinterpret_cast<float*>(hact + act_b);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 9; ++k) hH[(size_t)i * 9 + k] = Hs[i][k];
+    const auto gf = generators(homog, B.w, B.h), gi = generators(homog, A.w, A.h);
+    for (int k = 0; k < 8; ++k)
+        for (int e = 0; e < 9; ++e) {
+            hgens[k * 9 + e] = (float)gf[k][e];
+            hgens[72 + k * 9 + e] = (float)gi[k][e];
+        }
+    double* H = gn_H_.as<double>();
+    double* Ht = gn_Htry_.as<double>();
+    double* cur = gn_cur_.as<double>();
+    unsigned char* act = gn_active_.as<unsigned char>();
+    unsigned char* valid = gn_valid_.as<unsigned char>();
+    float* dh = pose_hinv_.as<float>();
+    float* dg = pose_gens_.as<float>();
+    double* sums = pose_sums_.as<double>();
+    double* tsum = pose_tsum_.as<double>();
+    double* score = pose_score_.as<double>();
+    float* coef = pose_coef_.as<float>();
+    std::vector<double> ninf((size_t)n, -INFINITY);
+    if (!cuda_ok(cudaMemcpyAsync(H, hH, (size_t)n * 9 * 8, cudaMemcpyHostToDevice, st), "refine") ||
+        !cuda_ok(cudaMemcpyAsync(dg, hgens, 2 * 72 * 4, cudaMemcpyHostToDevice, st), "refine") ||
+        !cuda_ok(cudaMemsetAsync(act, 1, (size_t)n, st), "refine"))
+        return false;
+    std::copy(ninf.begin(), ninf.end(), hcur);
+    if (!cuda_ok(cudaMemcpyAsync(cur, hcur, (size_t)n * 8, cudaMemcpyHostToDevice, st), "refine")) return false;
+    counts[2] += 3;
+    const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
+        pb{B.feat.as<float>(), B.feat4.as<float4>(), B.w, B.h};
+    constexpr unsigned kGnBatch = 4;
+    for (unsigned it = 0; it < iters && !cancel; ++it) {
+        // the poses: moments, coefficients, gradient and Gauss–Newton sums
+        ok = cuda_ok(gn_hinv(H, n, d.sym, dh, st), "refine") &&
+             cuda_ok(pose_moments(pa, pb, dh, n, sums, st, {}, act), "refine") &&
+             (!sym || cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, {}, act), "refine")) &&
+             cuda_ok(pose_coefs(sums, (int)m, exact, coef, score, st), "refine") &&
+             cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, true, tsum, st, {}, act), "refine") &&
+             (!sym || cuda_ok(pose_tangent(pb, pa, dh + (size_t)n * 9, coef + (size_t)n * kCoef, dg + 72, n, true,
+                                           tsum + (size_t)n * kGrad, st, {}, act),
+                              "refine")) &&
+             // the candidates, then their scores
+             cuda_ok(gn_propose(d, ga, H, sums, score, tsum, act, cur, Ht, valid, st), "refine") &&
+             cuda_ok(gn_hinv(Ht, (int)nt, d.sym, dh, st), "refine") &&
+             cuda_ok(pose_moments(pa, pb, dh, (int)nt, sums, st, {}, valid), "refine") &&
+             (!sym ||
+              cuda_ok(pose_moments(pb, pa, dh + nt * 9, (int)nt, sums + nt * kMom, st, {}, valid), "refine")) &&
+             cuda_ok(pose_coefs(sums, (int)mt, exact, coef, score, st), "refine") &&
+             cuda_ok(gn_select(d, score, valid, Ht, H, cur, act, st), "refine");
+        if (!ok) return false;
+        counts[0] += 5 + 2 * nd + 2 + nd + 2;
+        if ((it + 1) % kGnBatch != 0 || it + 1 == iters) continue;
+        // stop once no pose moved in the last iteration
+        if (!cuda_ok(cudaMemcpyAsync(hact, act, (size_t)n, cudaMemcpyDeviceToHost, st), "refine") ||
+            !cuda_ok(cudaStreamSynchronize(st), "refine"))
+            return false;
+        counts[2]++, counts[3]++;
+        if (std::none_of(hact, hact + n, [](unsigned char a) { return a != 0; })) break;
+    }
+    if (!cuda_ok(cudaMemcpyAsync(hH, H, (size_t)n * 9 * 8, cudaMemcpyDeviceToHost, st), "refine") ||
+        !cuda_ok(cudaMemcpyAsync(hcur, cur, (size_t)n * 8, cudaMemcpyDeviceToHost, st), "refine") ||
+        !cuda_ok(cudaStreamSynchronize(st), "refine"))
+        return false;
+    counts[1]++, counts[2] += 2, counts[3]++;
+    out.resize(n);
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < 9; ++k) out[i].H[k] = hH[(size_t)i * 9 + k];
+        out[i].score = hcur[i];
+    }
+    return true;
+}
+
 bool Engine::gn_batch(const std::vector<Mat3>& Hs, unsigned iters, const std::vector<double>& amps,
                       std::vector<ScoredPose>& cur) {
+    // the device loop, unless a live spline moves the samples (its directions are per pose on the
+    // host) or ZCMIR_B200_GN=host asks for the host loop
+    const char* gv = std::getenv("ZCMIR_B200_GN");
+    if (!(gv && std::string(gv) == "host") && !ffd_live() && amps.size() <= 16) return gn_batch_dev(Hs, iters, amps, cur);
     const bool homog = set.e("group") == "homography";
     const int nk = n_keys(homog);
     const double rw = side[1].w, rh = side[1].h;

@@ -181,14 +181,39 @@ struct PoseFfd {
 // blocks per pose (0 keeps the current value). It changes the order of the cross-block sums, so
 // scores move within their float32 rounding.
 void pose_tune(unsigned px_per_thread, unsigned min_blocks, unsigned max_blocks);
+// mask (nullable, n bytes): poses with a zero byte are skipped (their sums stay 0)
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
-                         const PoseFfd& ffd = {});
+                         const PoseFfd& ffd = {}, const unsigned char* mask = nullptr);
 // score (float64) and the 102 gradient coefficients (f32) of each pose's sums
 cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, double* score, cudaStream_t st);
 // tangent sums per pose: 8 gradient + 36 Gauss–Newton (upper triangle) float64 (zeroed here);
 // gens: 8 generators (9 f32 each) in b's pixel coordinates
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
-                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd = {});
+                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd = {},
+                         const unsigned char* mask = nullptr);
+// ── the batched Gauss–Newton refine on the device (gn_device.cu) ──
+struct GnDims {
+    int n;        // poses
+    int T;        // candidates per pose: the step ladder's then the 5 Gauss–Newton multiples
+    int nk;       // tangent keys (8 homography, 6 affine)
+    int homog, sym;
+    double mw, mh, fw, fh;  // moving and fixed image sizes
+};
+struct GnAmps {
+    int n;         // unit-ascent step lengths (≤ 16)
+    double v[16];
+};
+// inverse maps of n poses H (n × 9 float64) for the pose kernels: forward rows 0..n−1, the
+// inverse direction's n..2n−1 when sym
+cudaError_t gn_hinv(const double* H, int n, int sym, float* hinv, cudaStream_t st);
+// per active pose: its pair score into cur, its candidates into Htry (n × T × 9) and valid
+cudaError_t gn_propose(const GnDims& d, const GnAmps& amps, const double* H, const double* sums, const double* score,
+                       const double* tsum, const unsigned char* active, double* cur, double* Htry,
+                       unsigned char* valid, cudaStream_t st);
+// per active pose: the first candidate (in order) that beats the score so far becomes the pose;
+// a pose that did not move becomes inactive. tscore: the candidates' scores (forward, then inverse)
+cudaError_t gn_select(const GnDims& d, const double* tscore, const unsigned char* valid, const double* Htry, double* H,
+                      double* cur, unsigned char* active, cudaStream_t st);
 // ∂score/∂(control points cp0 .. cp0 + 15) of pose 0 of one direction from its coefficients:
 // out[32] float64 (x then y per point; zeroed here)
 cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef,

@@ -49,9 +49,10 @@ inline Coords vee(const Mat3& A0, bool homog) {
 inline Mat3 expm3(const Mat3& A) {
     double nrm = 0;
     for (double v : A) nrm = std::max(nrm, std::fabs(v));
+    // halvings until the norm is at most 0.5 (at most 10), counted exactly
     int s = 0;
-    if (nrm > 0.5) s = (int)std::min(10.0, std::max(0.0, std::ceil(std::log2(nrm / 0.5))));
-    const double sc = std::pow(0.5, s);
+    for (double v = nrm; v > 0.5 && s < 10; v *= 0.5) ++s;
+    const double sc = std::ldexp(1.0, -s);
     Mat3 B;
     for (int i = 0; i < 9; ++i) B[i] = A[i] * sc;
     Mat3 T = mat_identity(), P = mat_identity();

@@ -176,11 +176,12 @@ template <bool FFD>
 __global__ void __launch_bounds__(256, FFD ? 2 : 3) k_pose_moments(const float4* __restrict__ fa, int aw, int ah,
                                                       const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, double* __restrict__ sums,
-                                                      PoseFfd ffd) {
+                                                      PoseFfd ffd, const unsigned char* __restrict__ mask) {
     __shared__ float Hs[9];
     __shared__ float red[8][kMom];
     __shared__ float cps[2 * kFfdMax * kFfdMax];
     const int pose = blockIdx.y;
+    if (mask && !mask[pose]) return;  // a pose nobody reads (its sums stay 0)
     if (threadIdx.x < 9) Hs[threadIdx.x] = hinv[pose * 9 + threadIdx.x];
     const FfdView fv = ffd_view(ffd, cps, pose);
     __syncthreads();
@@ -396,11 +397,12 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__
                                                       const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, const float* __restrict__ coef,
                                                       const float* __restrict__ gens, int hess, double* __restrict__ out,
-                                                      PoseFfd ffd) {
+                                                      PoseFfd ffd, const unsigned char* __restrict__ mask) {
     __shared__ float Hs[9], Mk[8][9], cf[kCoef];
     __shared__ float red[8][kGrad];
     __shared__ float cps[2 * kFfdMax * kFfdMax];
     const int pose = blockIdx.y;
+    if (mask && !mask[pose]) return;  // a pose nobody reads (its sums stay 0)
     if (threadIdx.x < 9) Hs[threadIdx.x] = hinv[pose * 9 + threadIdx.x];
     for (int k = threadIdx.x; k < kCoef; k += blockDim.x) cf[k] = coef[pose * kCoef + k];
     const FfdView fv = ffd_view(ffd, cps, pose);
@@ -931,15 +933,15 @@ cudaError_t interleave_features(const float* feat, int n, float4* out, cudaStrea
 }
 
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
-                         const PoseFfd& ffd) {
+                         const PoseFfd& ffd, const unsigned char* mask) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(sums, 0, (size_t)n * kMom * sizeof(double), st);
     static const int sl_s = pose_slots(k_pose_moments<true>), sl_p = pose_slots(k_pose_moments<false>);
     dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
-        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd);
+        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask);
     else
-        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd);
+        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask);
     return cudaGetLastError();
 }
 
@@ -967,15 +969,17 @@ cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, doubl
 }
 
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
-                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd) {
+                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd, const unsigned char* mask) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, (size_t)n * kGrad * sizeof(double), st);
     static const int sl_s = pose_slots(k_pose_tangent<true>), sl_p = pose_slots(k_pose_tangent<false>);
     dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
-        k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
+        k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd,
+                                                mask);
     else
-        k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd);
+        k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out,
+                                                 ffd, mask);
     return cudaGetLastError();
 }
 
