@@ -195,9 +195,9 @@ def test_tune_parts_changes_the_launch_shape_not_the_scores():
 def test_device_refine_equals_the_host_loop(monkeypatch):
     """The batched Gauss–Newton refine (zcb_refine_poses, and the search's screening and final
     refines) runs on the device by default; ZCMIR_B200_GN=host runs the same loop on the host.
-    The device kernels restate the host's float64 pose algebra without fused multiply-adds, so
-    both take the same steps: the poses and scores agree to the last few bits (the pose sums are
-    float64 atomics across blocks, added in whatever order the blocks finish)."""
+    The device kernels restate the host's float64 pose algebra without fused multiply-adds, and
+    the pose kernels add their blocks' totals in block order, so both take the same steps: the
+    poses and scores are equal bit for bit."""
     m, f, H = synth.pair_similarity(n=256, seed=7)
     rng = np.random.default_rng(3)
     starts = [_near(H, th=rng.uniform(-4, 4), s=rng.uniform(0.97, 1.03), t=rng.uniform(-3, 3, 2)) for _ in range(8)]
@@ -212,12 +212,37 @@ def test_device_refine_equals_the_host_loop(monkeypatch):
     dp, ds, dsr = run()
     monkeypatch.setenv("ZCMIR_B200_GN", "host")
     hp, hs, hsr = run()
-    np.testing.assert_allclose(ds, hs, rtol=1e-9, atol=0)
-    np.testing.assert_allclose(dp, hp, rtol=0, atol=1e-9 * np.abs(hp).max())
-    np.testing.assert_allclose(dsr.H, hsr.H, rtol=0, atol=1e-9 * np.abs(hsr.H).max())
-    assert abs(dsr.score - hsr.score) <= 1e-9 * abs(hsr.score)
+    np.testing.assert_array_equal(ds, hs)
+    np.testing.assert_array_equal(dp, hp)
+    np.testing.assert_array_equal(dsr.H, hsr.H)
+    assert dsr.score == hsr.score
     # every start climbed: no score below its start's
     with zc.Engine(half=False) as eng:
         eng.set_images(m, f, preprocess=False)
         s0 = np.array([eng.score(h).mean for h in starts])
     assert np.all(ds >= s0 - 1e-9 * np.abs(s0)), (ds, s0)
+
+
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_pose_sums_are_the_same_in_any_batch(symmetric):
+    """A pose's moment and tangent sums are added across its blocks in block order, not by
+    atomics: one step of the refine from a pose gives the same pose and score bit for bit whether
+    the pose is refined alone, first in a batch of 12 or last in it, and the moments of a pose
+    are the same on every call."""
+    m, f, H = synth.pair_similarity(n=256, seed=7)
+    rng = np.random.default_rng(11)
+    starts = [_near(H, th=rng.uniform(-4, 4), s=rng.uniform(0.97, 1.03), t=rng.uniform(-3, 3, 2)) for _ in range(12)]
+    with zc.Engine(half=False, symmetric=symmetric) as eng:
+        eng.set_images(m, f, preprocess=False)
+        alone = [eng.refine_poses([h], iters=1) for h in (starts[0], starts[-1])]
+        p, s = eng.refine_poses(starts, iters=1)
+        pr, sr = eng.refine_poses(starts[::-1], iters=1)
+        mom = [eng.moments(starts[3]) for _ in range(3)]
+    np.testing.assert_array_equal(alone[0][0][0], p[0])
+    assert alone[0][1][0] == s[0]
+    np.testing.assert_array_equal(alone[1][0][0], p[-1])
+    assert alone[1][1][0] == s[-1]
+    np.testing.assert_array_equal(pr[::-1], p)
+    np.testing.assert_array_equal(sr[::-1], s)
+    np.testing.assert_array_equal(mom[0], mom[1])
+    np.testing.assert_array_equal(mom[0], mom[2])

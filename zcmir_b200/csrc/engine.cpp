@@ -110,7 +110,7 @@ Engine::~Engine() {
     }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
-                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &sw_il_[0], &sw_il_[1], &sw_poses_,
+                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &pose_part_, &pose_ticket_, &sw_il_[0], &sw_il_[1], &sw_poses_,
                       &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
     for (auto& s : stack_) {

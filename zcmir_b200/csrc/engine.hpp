@@ -362,6 +362,9 @@ class Engine {
     int prio_lo_ = 0, prio_hi_ = 0;     // the device's stream priority range
     DevBuf canvas_a_, canvas_b_, grid_a_, grid_b_, half_a_, half_b_, q_, map_, res_, flush_;
     DevBuf pose_hinv_, pose_sums_, pose_coef_, pose_score_, pose_tsum_, pose_gens_;
+    // the pose kernels' per-block totals and per-pose tickets (their sums added in block order)
+    DevBuf pose_part_, pose_ticket_;
+    bool pose_red(int n, PoseRed& r);
     DevBuf rs_fwd_, rs_inv_, rs_map_;
     DevBuf pp_rgba_, pp_clahe_, pp_tmp_, pp_mm_;
     std::vector<Side> stack_;

@@ -110,14 +110,17 @@ bool Engine::ffd_gradient(const Mat3& H, double* score, double* grad, size_t len
     double* out = ffd_out_.as<double>();
     ok = cuda_ok(cudaMemcpyAsync(ffd_dev_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st), "ffd_gradient") &&
          cuda_ok(cudaMemcpyAsync(dh, hinv, sizeof hinv, cudaMemcpyHostToDevice, st), "ffd_gradient");
+    PoseRed rd;
+    ok = ok && pose_red(1, rd);
     for (int d = 0; ok && d < nd; ++d) {
         const PoseSide &a = d ? pb : pa, &b = d ? pa : pb;
         const PoseFfd& f = d ? fi : ff;
-        ok = cuda_ok(pose_moments(a, b, dh + 9 * d, 1, sums + kMom * d, st, f), "ffd_gradient") &&
+        ok = cuda_ok(pose_moments(a, b, dh + 9 * d, 1, sums + kMom * d, st, f, nullptr, rd), "ffd_gradient") &&
              cuda_ok(pose_coefs(sums + kMom * d, 1, exact, coef + kCoef * d, pose_score_.as<double>() + d, st),
                      "ffd_gradient");
         for (int c = 0; ok && c < nchunk; ++c)
-            ok = cuda_ok(pose_ffd_grad(a, b, dh + 9 * d, coef + kCoef * d, f, 16 * c, out + ((size_t)d * nchunk + c) * 32, st),
+            ok = cuda_ok(pose_ffd_grad(a, b, dh + 9 * d, coef + kCoef * d, f, 16 * c, out + ((size_t)d * nchunk + c) * 32, st,
+                                       rd),
                          "ffd_gradient");
     }
     if (!ok) return false;

@@ -48,6 +48,21 @@ std::string json_str(const std::string& t) {
 
 void Engine::log_event(const std::string& text) { events.push_back("{\"kind\":\"log\",\"text\":" + json_str(text) + "}"); }
 
+// scratch for n poses per launch onto either side: the pose kernels then add each pose's
+// block totals in block order (the same sums on every run, in any batch); fresh tickets are zeroed
+bool Engine::pose_red(int n, PoseRed& r) {
+    const size_t px = std::max((size_t)side[0].w * side[0].h, (size_t)side[1].w * side[1].h);
+    const uint64_t gen = pose_ticket_.gen;
+    if (!cuda_ok(pose_part_.ensure(pose_red_need(px, n) * sizeof(double)), "pose sums") ||
+        !cuda_ok(pose_ticket_.ensure((size_t)std::max(n, 1) * sizeof(unsigned)), "pose sums"))
+        return false;
+    if (pose_ticket_.gen != gen && !cuda_ok(cudaMemsetAsync(pose_ticket_.p, 0, pose_ticket_.cap, st), "pose sums"))
+        return false;
+    r = PoseRed{pose_part_.as<double>(), pose_ticket_.as<unsigned>(), pose_part_.cap / sizeof(double),
+                pose_ticket_.cap / sizeof(unsigned)};
+    return true;
+}
+
 bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::vector<PoseEval>& out,
                         bool forward_only, const float* pose_cps) {
     if (!need_images()) return false;
@@ -98,15 +113,18 @@ bool Engine::eval_poses(const std::vector<Mat3>& Hs, bool grad, bool hess, std::
     // a live spline moves the samples of both directions (src/pair.zig:127-150)
     PoseFfd ff, fi;
     if (!(pose_cps ? ffd_pose_dirs(pose_cps, n, ff, fi) : ffd_dirs(ff, fi))) return false;
-    if (!cuda_ok(pose_moments(pa, pb, dh, n, sums, st, ff), "moments")) return false;
-    if (sym && !cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, fi), "moments"))
+    PoseRed rd;
+    if (!pose_red(n, rd)) return false;
+    if (!cuda_ok(pose_moments(pa, pb, dh, n, sums, st, ff, nullptr, rd), "moments")) return false;
+    if (sym &&
+        !cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, fi, nullptr, rd), "moments"))
         return false;
     if (!cuda_ok(pose_coefs(sums, (int)m, exact, coef, pose_score_.as<double>(), st), "score")) return false;
     counts[0] += nd + 1;
     if (grad) {
-        if (!cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, hess, tsum, st, ff), "gradient")) return false;
+        if (!cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, hess, tsum, st, ff, nullptr, rd), "gradient")) return false;
         if (sym && !cuda_ok(pose_tangent(pb, pa, dh + (size_t)n * 9, coef + (size_t)n * kCoef, dg + 72, n, hess,
-                                         tsum + (size_t)n * kGrad, st, fi),
+                                         tsum + (size_t)n * kGrad, st, fi, nullptr, rd),
                             "gradient"))
             return false;
         counts[0] += nd;

@@ -468,23 +468,25 @@ bool Engine::gn_batch_dev(const std::vector<Mat3>& Hs, unsigned iters, const std
     counts[2] += 3;
     const PoseSide pa{A.feat.as<float>(), A.feat4.as<float4>(), A.w, A.h},
         pb{B.feat.as<float>(), B.feat4.as<float4>(), B.w, B.h};
+    PoseRed rd;
+    if (!pose_red((int)nt, rd)) return false;
     constexpr unsigned kGnBatch = 4;
     for (unsigned it = 0; it < iters && !cancel; ++it) {
         // the poses: moments, coefficients, gradient and Gauss–Newton sums
         ok = cuda_ok(gn_hinv(H, n, d.sym, dh, st), "refine") &&
-             cuda_ok(pose_moments(pa, pb, dh, n, sums, st, {}, act), "refine") &&
-             (!sym || cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, {}, act), "refine")) &&
+             cuda_ok(pose_moments(pa, pb, dh, n, sums, st, {}, act, rd), "refine") &&
+             (!sym || cuda_ok(pose_moments(pb, pa, dh + (size_t)n * 9, n, sums + (size_t)n * kMom, st, {}, act, rd), "refine")) &&
              cuda_ok(pose_coefs(sums, (int)m, exact, coef, score, st), "refine") &&
-             cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, true, tsum, st, {}, act), "refine") &&
+             cuda_ok(pose_tangent(pa, pb, dh, coef, dg, n, true, tsum, st, {}, act, rd), "refine") &&
              (!sym || cuda_ok(pose_tangent(pb, pa, dh + (size_t)n * 9, coef + (size_t)n * kCoef, dg + 72, n, true,
-                                           tsum + (size_t)n * kGrad, st, {}, act),
+                                           tsum + (size_t)n * kGrad, st, {}, act, rd),
                               "refine")) &&
              // the candidates, then their scores
              cuda_ok(gn_propose(d, ga, H, sums, score, tsum, act, cur, Ht, valid, st), "refine") &&
              cuda_ok(gn_hinv(Ht, (int)nt, d.sym, dh, st), "refine") &&
-             cuda_ok(pose_moments(pa, pb, dh, (int)nt, sums, st, {}, valid), "refine") &&
+             cuda_ok(pose_moments(pa, pb, dh, (int)nt, sums, st, {}, valid, rd), "refine") &&
              (!sym ||
-              cuda_ok(pose_moments(pb, pa, dh + nt * 9, (int)nt, sums + nt * kMom, st, {}, valid), "refine")) &&
+              cuda_ok(pose_moments(pb, pa, dh + nt * 9, (int)nt, sums + nt * kMom, st, {}, valid, rd), "refine")) &&
              cuda_ok(pose_coefs(sums, (int)mt, exact, coef, score, st), "refine") &&
              cuda_ok(gn_select(d, score, valid, Ht, H, cur, act, st), "refine");
         if (!ok) return false;

@@ -175,6 +175,18 @@ struct PoseFfd {
     int source = 0;
     int stride = 0;  // floats between poses' control points (0: one set for every pose)
 };
+// How a pose's blocks add their float64 totals. With part set, each block stores its totals in
+// part and the pose's last block to finish adds them in block order, so the sums are the same on
+// every run and in every batch; ticket: one counter per pose of the launch, zero before it (each
+// is put back to zero). Without part: float64 atomics, in the order the blocks finish.
+struct PoseRed {
+    double* part = nullptr;
+    unsigned* ticket = nullptr;
+    size_t cap = 0;      // doubles at part
+    size_t tickets = 0;  // counters at ticket
+};
+// doubles of PoseRed::part any pose kernel needs for n poses onto an image of `pixels` pixels
+size_t pose_red_need(size_t pixels, int n);
 // the 45 sums of n poses of one direction (a sampled at H⁻¹x for every b pixel x); hinv: n
 // inverse poses (f32, row-major); sums: n × 45 float64 (zeroed here)
 // The pose kernels' launch shape (zc_tune_parts): pixels per thread, the least and the most
@@ -183,14 +195,14 @@ struct PoseFfd {
 void pose_tune(unsigned px_per_thread, unsigned min_blocks, unsigned max_blocks);
 // mask (nullable, n bytes): poses with a zero byte are skipped (their sums stay 0)
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
-                         const PoseFfd& ffd = {}, const unsigned char* mask = nullptr);
+                         const PoseFfd& ffd = {}, const unsigned char* mask = nullptr, const PoseRed& red = {});
 // score (float64) and the 102 gradient coefficients (f32) of each pose's sums
 cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, double* score, cudaStream_t st);
 // tangent sums per pose: 8 gradient + 36 Gauss–Newton (upper triangle) float64 (zeroed here);
 // gens: 8 generators (9 f32 each) in b's pixel coordinates
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
                          int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd = {},
-                         const unsigned char* mask = nullptr);
+                         const unsigned char* mask = nullptr, const PoseRed& red = {});
 // ── the batched Gauss–Newton refine on the device (gn_device.cu) ──
 struct GnDims {
     int n;        // poses
@@ -217,7 +229,7 @@ cudaError_t gn_select(const GnDims& d, const double* tscore, const unsigned char
 // ∂score/∂(control points cp0 .. cp0 + 15) of pose 0 of one direction from its coefficients:
 // out[32] float64 (x then y per point; zeroed here)
 cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef,
-                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st);
+                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st, const PoseRed& red = {});
 // the spline's Gauss–Newton terms per lattice cell of pose 0 of one direction (its coefficients
 // with a positive semi-definite Q): per cell and chunk 332 float32 sums (100 symmetric basis
 // pairs × K_xx, K_xy, K_yy, then 16 taps × ∇_x, ∇_y); nch chunks per cell

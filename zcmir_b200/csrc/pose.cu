@@ -6,8 +6,9 @@
 //
 // One direction warps image a (moving) onto image b (fixed): every b pixel x samples a's
 // features bilinearly at H⁻¹(x + 1) − 1, weighted by a 2-px ramp inside a's valid border. Blocks
-// of pose p sum their pixels in float32 per thread, then float64 across the block, and add into
-// the pose's float64 sums.
+// of pose p sum their pixels in float32 per thread, then float64 across the block; the pose's
+// blocks' totals are added in block order by the last of them to finish (block_add).
+#include <array>
 #include <atomic>
 #include <algorithm>
 
@@ -23,6 +24,43 @@ constexpr int kMom = 45, kCoef = 102, kG0 = 40, kQ0 = 85, kGrad = 44;
 __device__ __forceinline__ int tri4(int i, int j) {
     const int a = min(i, j), b = max(i, j);
     return a * 4 - (a * (a + 1)) / 2 + b;
+}
+
+// The block's k ≤ 48 float64 totals (thread t < k holds total t; the others pass anything) added
+// into out[0 .. k) of this pose. With r.part: every block stores its totals at
+// part[(pose · blocks + block) · k], then the pose's last block to finish (the old value of its
+// ticket is blocks − 1) adds them in a fixed order — group g of ⌊256 / k⌋ threads takes blocks
+// g, g + groups, …, and thread t adds the groups' totals 0, 1, … — and puts the ticket back to
+// 0. Every thread of the block calls it. Without r.part: float64 atomics.
+__device__ void block_add(double s, int k, double* __restrict__ out, const PoseRed& r, int pose) {
+    const int t = threadIdx.x, nblk = gridDim.x;
+    if (!r.part) {
+        if (t < k) atomicAdd(&out[t], s);
+        return;
+    }
+    __shared__ int last;
+    __shared__ double grp[8][48];
+    double* part = r.part + (size_t)pose * nblk * k;
+    if (t < k) part[(size_t)blockIdx.x * k + t] = s;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&r.ticket[pose], 1u) == (unsigned)(nblk - 1);
+    __syncthreads();
+    if (!last) return;  // uniform over the block
+    __threadfence();
+    const int ng = min((int)blockDim.x / k, 8), g = t / k, e = t - g * k;
+    if (g < ng) {
+        double a = 0.0;
+        for (int b = g; b < nblk; b += ng) a += __ldcg(&part[(size_t)b * k + e]);
+        grp[g][e] = a;
+    }
+    __syncthreads();
+    if (t < k) {
+        double a = 0.0;
+        for (int q = 0; q < ng; ++q) a += grp[q][t];
+        out[t] = a;
+    }
+    if (t == 0) r.ticket[pose] = 0;
 }
 
 // (w, ∂w/∂fx, ∂w/∂fy) of the border taper at (fx, fy) in a w×h image
@@ -176,7 +214,7 @@ template <bool FFD>
 __global__ void __launch_bounds__(256, FFD ? 2 : 3) k_pose_moments(const float4* __restrict__ fa, int aw, int ah,
                                                       const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, double* __restrict__ sums,
-                                                      PoseFfd ffd, const unsigned char* __restrict__ mask) {
+                                                      PoseFfd ffd, const unsigned char* __restrict__ mask, PoseRed rd) {
     __shared__ float Hs[9];
     __shared__ float red[8][kMom];
     __shared__ float cps[2 * kFfdMax * kFfdMax];
@@ -236,11 +274,10 @@ __global__ void __launch_bounds__(256, FFD ? 2 : 3) k_pose_moments(const float4*
         if (lane == 0) red[w][k] = v;
     }
     __syncthreads();
-    if (threadIdx.x < kMom) {
-        double s = 0.0;
+    double s = 0.0;
+    if (threadIdx.x < kMom)
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += (double)red[i][threadIdx.x];
-        atomicAdd(&sums[pose * kMom + threadIdx.x], s);
-    }
+    block_add(s, kMom, sums + (size_t)pose * kMom, rd, pose);
 }
 
 // scoreFromMoments (src/moments.zig:91-172) in float64, one thread per pose: the score and the
@@ -397,7 +434,7 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__
                                                       const float4* __restrict__ fb, int bw, int bh,
                                                       const float* __restrict__ hinv, const float* __restrict__ coef,
                                                       const float* __restrict__ gens, int hess, double* __restrict__ out,
-                                                      PoseFfd ffd, const unsigned char* __restrict__ mask) {
+                                                      PoseFfd ffd, const unsigned char* __restrict__ mask, PoseRed rd) {
     __shared__ float Hs[9], Mk[8][9], cf[kCoef];
     __shared__ float red[8][kGrad];
     __shared__ float cps[2 * kFfdMax * kFfdMax];
@@ -530,11 +567,10 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__
         if (lane == 0) red[w][8 + k] = v;
     }
     __syncthreads();
-    if (threadIdx.x < kGrad) {
-        double s = 0.0;
+    double s = 0.0;
+    if (threadIdx.x < kGrad)
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += (double)red[i][threadIdx.x];
-        atomicAdd(&out[pose * kGrad + threadIdx.x], s);
-    }
+    block_add(s, kGrad, out + (size_t)pose * kGrad, rd, pose);
 }
 
 // ∂score/∂(control points cp0 .. cp0 + 15) of pose 0 (smi.wgsl ffd_grad 1275-1417): per valid
@@ -545,7 +581,7 @@ __global__ void __launch_bounds__(256) k_pose_tangent(const float4* __restrict__
 __global__ void __launch_bounds__(256) k_pose_ffd_grad(const float4* __restrict__ fa, int aw, int ah,
                                                        const float4* __restrict__ fb, int bw, int bh,
                                                        const float* __restrict__ hinv, const float* __restrict__ coef,
-                                                       PoseFfd ffd, int cp0, double* __restrict__ out) {
+                                                       PoseFfd ffd, int cp0, double* __restrict__ out, PoseRed rd) {
     __shared__ float Hs[9], cf[kCoef];
     __shared__ float red[8][32];
     __shared__ float cps[2 * kFfdMax * kFfdMax];
@@ -656,11 +692,10 @@ __global__ void __launch_bounds__(256) k_pose_ffd_grad(const float4* __restrict_
         if (lane == 0) red[w][k] = v;
     }
     __syncthreads();
-    if (threadIdx.x < 32) {
-        double s = 0.0;
+    double s = 0.0;
+    if (threadIdx.x < 32)
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += (double)red[i][threadIdx.x];
-        atomicAdd(&out[threadIdx.x], s);
-    }
+    block_add(s, 32, out, rd, 0);
 }
 
 // The spline's Gauss–Newton terms of one lattice cell (smi.wgsl ffd_cells 2065-2264): block =
@@ -932,16 +967,37 @@ cudaError_t interleave_features(const float* feat, int n, float4* out, cudaStrea
     return cudaGetLastError();
 }
 
+namespace {
+// resident blocks of each pose kernel: moments (spline, plain), tangent (spline, plain), ffd_grad
+const std::array<int, 5>& kernel_slots() {
+    static const std::array<int, 5> sl{pose_slots(k_pose_moments<true>), pose_slots(k_pose_moments<false>),
+                                       pose_slots(k_pose_tangent<true>), pose_slots(k_pose_tangent<false>),
+                                       pose_slots(k_pose_ffd_grad)};
+    return sl;
+}
+// part must hold n poses × blocks × k totals and ticket n counters
+bool red_fits(const PoseRed& r, int n, int blocks, int k) {
+    return !r.part || (r.ticket && r.tickets >= (size_t)n && r.cap >= (size_t)n * blocks * k);
+}
+}  // namespace
+
+size_t pose_red_need(size_t pixels, int n) {
+    int b = 1;
+    for (int sl : kernel_slots()) b = std::max(b, pose_blocks(pixels, sl));
+    return (size_t)std::max(n, 1) * b * kMom;
+}
+
 cudaError_t pose_moments(const PoseSide& a, const PoseSide& b, const float* hinv, int n, double* sums, cudaStream_t st,
-                         const PoseFfd& ffd, const unsigned char* mask) {
+                         const PoseFfd& ffd, const unsigned char* mask, const PoseRed& red) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
+    if (n <= 0) return cudaSuccess;
+    dim3 g(pose_blocks((size_t)b.w * b.h, kernel_slots()[ffd.cps ? 0 : 1]), n);
+    if (!red_fits(red, n, (int)g.x, kMom)) return cudaErrorInvalidValue;
     cudaMemsetAsync(sums, 0, (size_t)n * kMom * sizeof(double), st);
-    static const int sl_s = pose_slots(k_pose_moments<true>), sl_p = pose_slots(k_pose_moments<false>);
-    dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
-        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask);
+        k_pose_moments<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask, red);
     else
-        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask);
+        k_pose_moments<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, sums, ffd, mask, red);
     return cudaGetLastError();
 }
 
@@ -954,12 +1010,12 @@ cudaError_t pose_ffd_cells(const PoseSide& a, const PoseSide& b, const float* hi
 }
 
 cudaError_t pose_ffd_grad(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef,
-                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st) {
+                          const PoseFfd& ffd, int cp0, double* out, cudaStream_t st, const PoseRed& red) {
     if (!ffd.cps || ffd.g < 2 || ffd.g > kFfdMax) return cudaErrorInvalidValue;
+    const int blocks = pose_blocks((size_t)b.w * b.h, kernel_slots()[4]);
+    if (!red_fits(red, 1, blocks, 32)) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, 32 * sizeof(double), st);
-    static const int sl = pose_slots(k_pose_ffd_grad);
-    k_pose_ffd_grad<<<pose_blocks((size_t)b.w * b.h, sl), 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef,
-                                                                       ffd, cp0, out);
+    k_pose_ffd_grad<<<blocks, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, ffd, cp0, out, red);
     return cudaGetLastError();
 }
 
@@ -969,17 +1025,19 @@ cudaError_t pose_coefs(const double* sums, int n, bool exact, float* coef, doubl
 }
 
 cudaError_t pose_tangent(const PoseSide& a, const PoseSide& b, const float* hinv, const float* coef, const float* gens,
-                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd, const unsigned char* mask) {
+                         int n, bool hess, double* out, cudaStream_t st, const PoseFfd& ffd, const unsigned char* mask,
+                         const PoseRed& red) {
     if (ffd.cps && (ffd.g < 2 || ffd.g > kFfdMax)) return cudaErrorInvalidValue;
+    if (n <= 0) return cudaSuccess;
+    dim3 g(pose_blocks((size_t)b.w * b.h, kernel_slots()[ffd.cps ? 2 : 3]), n);
+    if (!red_fits(red, n, (int)g.x, kGrad)) return cudaErrorInvalidValue;
     cudaMemsetAsync(out, 0, (size_t)n * kGrad * sizeof(double), st);
-    static const int sl_s = pose_slots(k_pose_tangent<true>), sl_p = pose_slots(k_pose_tangent<false>);
-    dim3 g(pose_blocks((size_t)b.w * b.h, ffd.cps ? sl_s : sl_p), n);
     if (ffd.cps)
         k_pose_tangent<true><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out, ffd,
-                                                mask);
+                                                mask, red);
     else
         k_pose_tangent<false><<<g, 256, 0, st>>>(a.feat4, a.w, a.h, b.feat4, b.w, b.h, hinv, coef, gens, hess ? 1 : 0, out,
-                                                 ffd, mask);
+                                                 ffd, mask, red);
     return cudaGetLastError();
 }
 
