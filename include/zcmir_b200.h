@@ -88,6 +88,15 @@ int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, con
  * stream of its own is waited for on the engine's stream. 0 / -1. */
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out);
 
+/* Precision study of the FFT's small-radix stage (no counterpart in the reference): with pieces 1,
+ * 2 or 3, the shift maps' forward column FFTs (zc_shift_map and the settings map) run their first
+ * stage — radix 16, which the column length must start with — on the tensor cores, every FP32
+ * input and DFT coefficient split into `pieces` BF16 parts and the stage summed from their
+ * products (1, 3 or 6) in FP32; the other stages stay FP32. The stage needs one more buffer as
+ * large as a side's half spectra and an extra pass, so it is slower than the default; 0 (the
+ * default) puts the FP32 stage back. Other values: −1 with zc_error. 0 / −1. */
+int32_t zcb_set_dft_stage(zc_engine* e, uint32_t pieces);
+
 /* Gauss–Newton from each of n poses (Hs, row-major 3×3 each) at once for `iters` steps of the
  * search's batched screen (src/search.zig gnBatch: a step only where it raises the pair score),
  * the final poses into Hout and their scores into scores: the seeds of a search that starts from

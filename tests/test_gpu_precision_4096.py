@@ -10,10 +10,14 @@ planted lag; at every lag where neither side floors the score, the GPU score is 
 map's peak, and within 1e-3 of its own value where the overlap is at least 20 %; both sides floor
 the same lags (the 8 %-of-zero-lag floor) except within 1 % of it. The float32-centring score of
 the exact sums is reported beside it (no bound: it is the alternative this build does not take).
+So are maps whose forward column FFTs run their first (radix-16) stage on the tensor cores with
+each FP32 value split into 3, 2 or 1 BF16 pieces (zcb_set_dft_stage): for 3 and 2 pieces the
+argmax is the planted lag and every score within 1e-4 of the peak; 1 piece is reported only.
 
 With ZCMIR_B200_STUDY_OUT set, the per-lag table is written there as JSON."""
 import json
 import os
+import time
 
 import numpy as np
 import pytest
@@ -43,10 +47,23 @@ def lags(rng, planted):
 def test_precision_study_4096():
     m, f, H = synth.pair_segmented(n=N, seed=4, max_shift=800)
     planted = (int(-H[0, 2]), int(-H[1, 2]))
+    tc, tc_ms = {}, {}
     with zc.Engine(half=False) as reg:
         reg.set_images(m, f, preprocess=False)
         sm = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=8192)
         fa, fb = reg.features(0), reg.features(1)
+        # the forward column FFTs' first stage on the tensor cores, 3, 2 and 1 BF16 pieces; each
+        # map timed whole on its second run (the first allocates the stage's buffer)
+        for p in (0, 3, 2, 1):
+            reg.set_dft_stage(p)
+            for _ in range(2):
+                t0 = time.perf_counter()
+                r = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=8192)
+                tc_ms[p] = (time.perf_counter() - t0) * 1e3
+            tc[p] = r
+        reg.set_dft_stage(0)
+    # the FP32 map does not depend on the stage runs between
+    np.testing.assert_array_equal(tc[0].map, sm.map)
     assert (sm.n, sm.ny, sm.cw, sm.ch) == (8192, 8192, N, N)
     assert (sm.dx, sm.dy) == planted
     # at the identity pose of two equal images the canvas planes are the stacks themselves, at
@@ -75,12 +92,27 @@ def test_precision_study_4096():
     assert err_peak[both].max() <= 1e-4, err_peak[both].max()
     big = both & (overlap >= 0.2)
     assert err_own[big].max() <= 1e-3, err_own[big].max()
+    # the tensor-core stage: argmax and error against float64 at the same lags
+    small = both & (overlap < 0.1)
+    tc_rows = {}
+    for p in (3, 2, 1):
+        g = np.array([tc[p].map[ty % tc[p].ny, tx % tc[p].n] for tx, ty in L], np.float64)
+        bp = (g != 0) & (s64 != 0)
+        ep = np.abs(g - s64) / peak
+        eo = np.where(bp, np.abs(g - s64) / np.maximum(np.abs(s64), 1e-300), 0.0)
+        tc_rows[p] = {"argmax": [tc[p].dx, tc[p].dy], "max_err_of_peak": float(ep[bp].max()),
+                      "max_err_rel_overlap_ge_20pct": float(eo[bp & (overlap >= 0.2)].max()),
+                      "max_err_rel_overlap_lt_10pct": float(eo[bp & (overlap < 0.1)].max()) if (bp & (overlap < 0.1)).any() else None,
+                      "floored_lags": int((g == 0).sum()), "map_ms": tc_ms[p], "values": g.tolist()}
+    for p in (3, 2):
+        assert (tc[p].dx, tc[p].dy) == planted, p
+        assert tc_rows[p]["max_err_of_peak"] <= 1e-4, (p, tc_rows[p]["max_err_of_peak"])
     out = os.environ.get("ZCMIR_B200_STUDY_OUT")
     if out:
         rows = [{"lag": [int(tx), int(ty)], "overlap": float(o), "fp64": float(a), "gpu": float(g), "fp32_centring": float(b),
-                 "gpu_err_of_peak": float(e), "gpu_err_rel": float(r), "fp32_centring_err_rel": float(q)}
-                for (tx, ty), o, a, g, b, e, r, q in zip(L, overlap, s64, gpu, s32, err_peak, err_own, err32)]
-        small = both & (overlap < 0.1)
+                 "gpu_err_of_peak": float(e), "gpu_err_rel": float(r), "fp32_centring_err_rel": float(q),
+                 "bf16x3": tc_rows[3]["values"][i], "bf16x2": tc_rows[2]["values"][i], "bf16x1": tc_rows[1]["values"][i]}
+                for i, ((tx, ty), o, a, g, b, e, r, q) in enumerate(zip(L, overlap, s64, gpu, s32, err_peak, err_own, err32))]
         summary = {
             "image": N, "fft": sm.n, "lags": len(L), "peak": peak, "argmax_gpu": [sm.dx, sm.dy], "planted": list(planted),
             "gpu_max_err_of_peak": float(err_peak[both].max()),
@@ -89,6 +121,8 @@ def test_precision_study_4096():
             "fp32_centring_max_err_rel_overlap_ge_20pct": float(err32[big].max()),
             "fp32_centring_max_err_rel_overlap_lt_10pct": float(err32[small].max()) if small.any() else None,
             "floored_lags_gpu": int((gpu == 0).sum()), "floored_lags_fp64": int((s64 == 0).sum()),
+            "fp32_map_ms": tc_ms[0],
+            "tensor_core_stage": {f"bf16x{p}": {k: v for k, v in r.items() if k != "values"} for p, r in tc_rows.items()},
         }
         with open(out, "w") as fh:
             json.dump({"summary": summary, "rows": rows}, fh, indent=1)

@@ -110,7 +110,7 @@ Engine::~Engine() {
     }
     for (DevBuf* b : {&fs_stats_, &fs_hist_, &fs_wt_, &fs_acfpart_, &fs_acf_, &rank_tmp_, &canvas_a_, &canvas_b_,
                       &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_, &flush_, &pose_hinv_, &pose_sums_,
-                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &pose_part_, &pose_ticket_, &sw_il_[0], &sw_il_[1], &sw_poses_,
+                      &pose_coef_, &pose_score_, &pose_tsum_, &pose_gens_, &pose_part_, &pose_ticket_, &dft_scratch_, &sw_il_[0], &sw_il_[1], &sw_poses_,
                       &sw_fgrid_, &sw_fhalf_, &sw_grid_, &sw_half_, &sw_q_, &sw_map_, &sw_n0_, &sw_ps_, &sw_pi_})
         b->release();
     for (auto& s : stack_) {
@@ -560,9 +560,19 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
         return cuda_ok(forward_rows(grid, g, job.plan, job.row, (s == 0 ? half_a_ : half_b_).as<float2>(), st),
                        "forward rows");
     };
+    unsigned* fault_tc = reinterpret_cast<unsigned*>(res + 28);  // the tensor-core stage's fault word
+    if (dft_pieces_ && !cuda_ok(cudaMemsetAsync(fault_tc, 0, 4, st), "shift_map")) return false;
     auto cols_of = [&](int s) {
-        return cuda_ok(forward_cols((s == 0 ? half_a_ : half_b_).as<float2>(), g, job.plan, job.col, st),
-                       "forward columns");
+        float2* half = (s == 0 ? half_a_ : half_b_).as<float2>();
+        if (dft_pieces_) {
+            if (job.col.radix[0] != 16 || (g.ny / 16) % 4 != 0)
+                return fail("dft stage: the column length " + std::to_string(g.ny) + " does not start with radix 16");
+            return cuda_ok(dft_scratch_.ensure(hs), "dft stage") &&
+                   cuda_ok(forward_cols_tc(half, dft_scratch_.as<float2>(), g, job.plan, job.col, dft_pieces_, fault_tc,
+                                           st),
+                           "forward columns (tensor-core stage)");
+        }
+        return cuda_ok(forward_cols(half, g, job.plan, job.col, st), "forward columns");
     };
     // Each side's canvas, grid and half spectra depend on its feature build, the canvas frame and
     // plan, the buffers they live in and, for the moving side, the canvas pose: with the same key
@@ -689,8 +699,8 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     // with the tensor-memory row pass the map leaves in row chunks during the pass (copy_st_)
     const bool chunked = map && row_pass != "split" && rows_tmem_supported(job.g.nx, job.plan.n_corr);
     if (!run_map(job, profiling ? ev : nullptr, chunked ? map : nullptr)) return false;
-    unsigned char host[28];
-    if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 28, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
+    unsigned char host[32];
+    if (!cuda_ok(cudaMemcpyAsync(host, res_.p, 32, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
     counts[2]++;
     if (map && !chunked) {
         if (!cuda_ok(cudaMemcpyAsync(map, map_.p, nn * 4, cudaMemcpyDeviceToHost, st), "shift_map")) return false;
@@ -720,6 +730,9 @@ bool Engine::shift_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap
     if (fault)
         return fail("shift_map: the inverse column pass gave up waiting for its operand copies (fault " +
                     std::to_string(fault) + "); the map is not valid");
+    memcpy(&fault, host + 28, 4);
+    if (dft_pieces_ && fault)
+        return fail("shift_map: the tensor-core column stage gave up waiting for its products; the map is not valid");
     map_result(job, best, zero, pair_area(), out);
     return true;
 }
@@ -751,6 +764,14 @@ void Engine::map_result(const MapJob& job, unsigned long long best, float zero, 
         r.dy = (double)ly * ((double)g.Hh / (double)g.ch);
     }
     *out = r;
+}
+
+bool Engine::set_dft_stage(unsigned pieces) {
+    if (pieces > 3) return fail("set_dft_stage: pieces must be 0 (FP32), 1, 2 or 3");
+    if ((int)pieces != dft_pieces_) forget_spectra();  // kept spectra were made with the other stage
+    dft_pieces_ = (int)pieces;
+    if (!pieces) dft_scratch_.release();
+    return true;
 }
 
 bool Engine::shift_map_settings(const Mat3& Hm, zc_shift_result* out, float* map, size_t map_len) {

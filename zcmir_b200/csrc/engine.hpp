@@ -317,6 +317,10 @@ class Engine {
     // fastest (rows of out: nx, ny, candidates, chosen batch, its ms per candidate, options,
     // then (batch, ms per candidate) per option)
     bool tune_sweep(double* out, size_t cap, size_t* used);
+    // the forward column FFTs' first stage on the tensor cores in `pieces` BF16 parts (0: FP32)
+    bool set_dft_stage(unsigned pieces);
+    int dft_pieces_ = 0;
+    DevBuf dft_scratch_;
     bool sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, int n_peak, double min_overlap,
                     SweepOut& out, int batch = 0, int shard = 0, int nshard = 1);
     // the host half of a sweep: canvas, candidates, footprints, plane sizes and slot order

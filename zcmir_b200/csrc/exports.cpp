@@ -461,6 +461,10 @@ int32_t zcb_tune_sweep(zc_engine* e, double* out, size_t cap, size_t* used) {
     return guarded(e, "tune_sweep", [&] { return e->tune_sweep(out, cap, used); });
 }
 
+int32_t zcb_set_dft_stage(zc_engine* e, uint32_t pieces) {
+    return guarded(e, "set_dft_stage", [&] { return e->set_dft_stage(pieces); });
+}
+
 int32_t zcb_score_static(zc_engine* e, const double* Hs, uint32_t n, double* out) {
     // allocates no device memory: the scratch is a file-scope array (score_static.cu)
     return guarded(e, "score_static", [&] { return e->score_static(Hs, n, out); });

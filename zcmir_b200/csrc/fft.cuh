@@ -25,6 +25,7 @@ struct LinePlan {
     int radix[kMaxStages];    // radix of each stage, in order
     int tl;                   // threads per line (each stage's butterflies fit in tl·16/R)
     const float2* tw;         // n twiddles e^{−2πi t/n}, t < n (device memory)
+    int s0 = 0;               // first stage run: stages before it were applied by another pass
 };
 
 __host__ __device__ __forceinline__ constexpr int pad_idx(int i) { return i + (i >> 4); }
@@ -234,7 +235,8 @@ __device__ __noinline__ void fft_stage(float2* __restrict__ buf, const float2* _
 template <bool INV>
 __device__ __forceinline__ void line_fft(float2* __restrict__ buf, const LinePlan& p, int t) {
     int Ns = 1;
-    for (int s = 0; s < p.nst; ++s) {
+    for (int s = 0; s < p.s0; ++s) Ns *= p.radix[s];
+    for (int s = p.s0; s < p.nst; ++s) {
         const int R = p.radix[s];
         switch (R) {
             case 16: fft_stage<16, 1, INV>(buf, p.tw, p.n, Ns, t, p.tl); break;

@@ -78,6 +78,17 @@ cudaError_t forward_rows(const float* grid, const MapGeom& g, const CorrPlanDev&
                          float2* half, cudaStream_t st, int batch = 1, size_t grid_stride = 0, size_t half_stride = 0);
 cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
                          cudaStream_t st, int batch = 1);
+// the column FFTs on the run-time line plan whatever the length (col.s0: the stage to start at)
+cudaError_t forward_cols_generic(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
+                                 cudaStream_t st);
+// The column FFTs with their first stage (radix 16) on the tensor cores (dft_tc.cu): each FP32
+// input and each DFT coefficient split into `pieces` (1 to 3) BF16 parts, the stage a sum of
+// BF16 products (1, 3 or 6) accumulated in FP32 in tensor memory; then the other
+// stages in FP32 (forward_cols_generic from stage 1). scratch: as large as the half spectra;
+// the result is copied back into half. fault (device word): 1 or-ed in if a wait on the tensor
+// cores gave up. Needs col.radix[0] == 16.
+cudaError_t forward_cols_tc(float2* half, float2* scratch, const MapGeom& g, const CorrPlanDev& plan,
+                            const LinePlan& col, int pieces, unsigned* fault, cudaStream_t st);
 // products and inverse column FFTs: Q[slot][ny][WP] (b_stride 0: one fixed side for every item).
 // fault (nullable, device memory): 1 is or-ed into it if the TMA-fed pass (1024- and 2048-point
 // square maps, one item) gave up waiting for a copy, 2 if its staging was misaligned; its Q is

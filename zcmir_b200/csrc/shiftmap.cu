@@ -207,6 +207,13 @@ cudaError_t forward_cols(float2* half, const MapGeom& g, const CorrPlanDev& plan
     return dispatch_pass(Pass::FwdCols, col, a, st);
 }
 
+cudaError_t forward_cols_generic(float2* half, const MapGeom& g, const CorrPlanDev& plan, const LinePlan& col,
+                                 cudaStream_t st) {
+    PassArgs a = pass_args(g, plan, 1);
+    a.half = half;
+    return run_pass<Pass::FwdCols, GenericLine, true>(GenericLine{col}, a, st);
+}
+
 cudaError_t inverse_columns(const float2* ha, const float2* hb, const MapGeom& g, const CorrPlanDev& plan,
                             const LinePlan& col, float2* Q, cudaStream_t st, int batch, size_t a_stride,
                             size_t b_stride, size_t q_stride, unsigned* fault) {

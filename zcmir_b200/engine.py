@@ -456,6 +456,11 @@ class Engine:
         self.call("zcb_search_lanes", _f32(sc), _u32(ix), sc.size, ctypes.byref(r))
         return self._search_out(r)
 
+    def set_dft_stage(self, pieces: int):
+        """zcb_set_dft_stage: the maps' forward column FFTs run their first (radix-16) stage on the
+        tensor cores in `pieces` (1 to 3) BF16 parts per FP32 value; 0 puts the FP32 stage back."""
+        self.call("zcb_set_dft_stage", int(pieces))
+
     def refine_poses(self, Hs, iters=25):
         """zcb_refine_poses: Gauss–Newton from every pose together → (poses (n, 3, 3), scores)."""
         a = np.ascontiguousarray(np.asarray(Hs, np.float64).reshape(-1, 9))

@@ -1,13 +1,16 @@
 """Run a few shift maps, or sweeps, of a workload for a profiler (ncu) to capture.
 
     python -m zcmir_b200.profile_map [--n 1024] [--cap 2048] [--maps 2] [--features laplacian]
+                                     [--dft-stage 0] [--stages]
     python -m zcmir_b200.profile_map --sweep [--n 512] [--maps 1] [--nth 360] [--ns 9] [--batch 0]
     python -m zcmir_b200.profile_map --search [--n 512] [--maps 1]
 
 Maps: builds the seeded segmented pair (zcmir_b200.synth.pair_segmented) at n², uploads it, then
 runs `--maps` maps at the identity pose (exact, calibrated) through the C ABI, printing the plan
 and the peak. Each map launches, in order: warp_stack, paste_stack, lag0, fwd_rows ×2, cols ×2,
-inv_cols, inv_rows.
+inv_cols, inv_rows. --dft-stage P (1–3): the forward column FFTs' first stage on the tensor
+cores in P BF16 pieces (zcb_set_dft_stage; cols ×2 become k_dft16_tc, cols, copy per side).
+--stages: per-stage device times of the maps after the first (CUDA events, zc_profile_report).
 
 Sweeps (--sweep): the seeded similarity pair (zcmir_b200.synth.pair_similarity) at n², then
 `--maps` sweeps of nth rotations × ns scales in [0.8, 1.25] on a 128² canvas (3240 candidate maps
@@ -40,6 +43,8 @@ def main():
     ap.add_argument("--nth", type=int, default=360)
     ap.add_argument("--ns", type=int, default=9)
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--dft-stage", type=int, default=0)
+    ap.add_argument("--stages", action="store_true")
     a = ap.parse_args()
     if a.search:
         n = a.n or 512
@@ -68,9 +73,15 @@ def main():
     m, f, H = synth.pair_segmented(n=n, seed=1, max_shift=min(200, n // 5))
     with zc.Engine(half=False, smi_features=a.features) as reg:
         reg.set_images(m, f, preprocess=False)
-        for _ in range(a.maps):
+        reg.set_dft_stage(a.dft_stage)
+        for i in range(a.maps):
+            if a.stages and i == 1:
+                reg.profile_report()  # drop the first map's times
+                reg.profile(True)
             sm = reg.shift_map(np.eye(3), exact=True, calibrated=True, cap=a.cap, want_map=False)
         print(f"n {sm.n}x{sm.ny} grid {sm.cw}x{sm.ch} peak {sm.peak:.3f} at ({sm.dx}, {sm.dy}); truth {-H[0, 2]}, {-H[1, 2]}")
+        if a.stages:
+            print(reg.profile_report(), end="")
 
 
 if __name__ == "__main__":
