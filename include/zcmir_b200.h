@@ -72,6 +72,21 @@ int32_t zcb_search_lanes(zc_engine* e, const float* scores, const uint32_t* idx,
 int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, const uint32_t* w, const uint32_t* h,
                        const double* priors, uint32_t flags, uint32_t cap, zc_shift_result* out, double* ms);
 
+/* zcb_stack_maps in two parts, for the combined launch. zcb_stack_load takes the same stack
+ * (slices, sizes, priors, flags, cap): it builds every slice's features and plans the n − 1 maps,
+ * allocating what they need, and runs no map. zcb_sweep_stack then runs the sweep of the engine's
+ * image pair (as zcb_sweep with the current sw_* settings, all candidates, the tuned batches;
+ * H0 NULL: the settings' start pose) and the loaded stack's maps as two branches of ONE CUDA
+ * graph (captured on the first call, kept while the sweep's schedule, the stack and their buffers
+ * are unchanged), launched once: scores/idx/cap/info as zcb_sweep (info[2] is the device time of
+ * the whole launch, info[12] its kernel count), stack_out[0 .. n − 2] as zcb_stack_maps's out
+ * (n_out ≥ n − 1). The stack stays loaded across calls. No counterpart in the reference. 0 / -1
+ * with zc_error. */
+int32_t zcb_stack_load(zc_engine* e, uint32_t n, const float* const* images, const uint32_t* w, const uint32_t* h,
+                       const double* priors, uint32_t flags, uint32_t cap);
+int32_t zcb_sweep_stack(zc_engine* e, const double H0[9], uint32_t n_peak, float* scores, uint32_t* idx, size_t cap,
+                        double* info, size_t info_len, zc_shift_result* stack_out, size_t n_out);
+
 /* Scores of n poses (Hs: n row-major 3×3 maps, each as zc_score's H) into out[3n], per pose the
  * mean, forward and inverse score exactly as zc_score writes them, allocating no device memory.
  * No counterpart in the reference (whose only pose score is zc_score, src/exports.zig:417). For

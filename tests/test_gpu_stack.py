@@ -66,3 +66,37 @@ def test_stack_maps_errors():
             reg.stack_maps([np.zeros((64, 64), np.float32)])
         with pytest.raises(RuntimeError, match="BadImage"):
             reg.stack_maps([np.zeros((64, 64), np.float32), np.zeros((4, 64), np.float32)])
+
+
+def test_sweep_and_stack_in_one_launch(stack):
+    """zcb_stack_load + zcb_sweep_stack: the sweep of the engine's pair and the stack's maps as two
+    branches of one CUDA graph, launched once. Each branch computes what it computes alone: the
+    lane maxima equal zcb_sweep's, the stack's results equal zcb_stack_maps's, bit for bit; the
+    graph is captured once and replayed while nothing changes; a plain sweep or shift map after it
+    is unaffected."""
+    slices, _ = stack
+    m, f, _ = synth.pair_similarity(n=256, seed=5)
+    with zc.Engine(half=False, sw_nth=36, sw_ns=3, sw_grid=64) as reg:
+        reg.set_images(m, f, preprocess=False)
+        alone = reg.sweep(n_peak=4)
+        maps, _ = reg.stack_maps(slices, exact=True, calibrated=False, cap=1024)
+        with pytest.raises(zc.EngineError, match="load a stack"):
+            zc.Engine(half=False).sweep_stack()
+        reg.stack_load(slices, exact=True, calibrated=False, cap=1024)
+        for rep in range(3):
+            sw, st = reg.sweep_stack(n_peak=4)
+            np.testing.assert_array_equal(sw.scores, alone.scores)
+            np.testing.assert_array_equal(sw.index, alone.index)
+            assert len(st) == len(maps)
+            for a, b in zip(st, maps):
+                assert (a.peak_index, a.dx, a.dy) == (b.peak_index, b.dx, b.dy)
+                assert a.peak == b.peak
+            assert sw.info["ms"] > 0
+            # every kernel of both branches, each launched by the one replay
+            assert sw.info["launches"] > alone.info["launches"]
+        again = reg.sweep(n_peak=4)
+        np.testing.assert_array_equal(again.scores, alone.scores)
+        one = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=512, want_map=False)
+        reg.set_images(m, f, preprocess=False)
+        ref = reg.shift_map(np.eye(3), exact=True, calibrated=False, cap=512, want_map=False)
+        assert (one.peak_index, one.peak) == (ref.peak_index, ref.peak)

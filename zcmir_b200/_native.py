@@ -98,6 +98,8 @@ SIGS = {
     "zcb_search_lanes": ([P, f32p, u32p, SZ, ctypes.POINTER(SearchResult)], I32),
     "zcb_tune_sweep": ([P, f64p, SZ, ctypes.POINTER(SZ)], I32),
     "zcb_set_dft_stage": ([P, U32], I32),
+    "zcb_stack_load": ([P, U32, ctypes.POINTER(f32p), u32p, u32p, f64p, U32, U32], I32),
+    "zcb_sweep_stack": ([P, f64p, U32, f32p, u32p, SZ, f64p, SZ, ctypes.POINTER(ShiftResult), SZ], I32),
     "zcb_refine_poses": ([P, f64p, U32, U32, f64p, f64p], I32),
     "zcb_prop_nparams": ([], SZ),
     "zcb_prop_error": ([ctypes.c_char_p, SZ], SZ),

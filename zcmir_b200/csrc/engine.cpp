@@ -131,6 +131,9 @@ Engine::~Engine() {
     for (cudaEvent_t e : chunk_ev_)
         if (e) cudaEventDestroy(e);
     if (copy_st_) cudaStreamDestroy(copy_st_);
+    if (branch_st_) cudaStreamDestroy(branch_st_);
+    for (cudaEvent_t e : {fork_ev_, join_ev_})
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(st);
 }
 
@@ -512,7 +515,7 @@ bool Engine::plan_map(const Mat3& Hm, bool exact, bool calibrated, unsigned cap,
     return true;
 }
 
-bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
+bool Engine::map_buffers(const MapJob& job) {
     const MapGeom& g = job.g;
     const size_t cn = (size_t)g.W * g.Hh, gn = (size_t)g.cw * g.ch;
     const size_t hs = (size_t)job.plan.n_real * g.ny * g.WP * sizeof(float2);
@@ -523,7 +526,14 @@ bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
               cuda_ok(res_.ensure(64), "shift_map");
     if (ok && !job.identity_grid)
         ok = cuda_ok(grid_a_.ensure(gn * 20), "shift_map") && cuda_ok(grid_b_.ensure(gn * 20), "shift_map");
-    if (!ok) return false;
+    if (ok && dft_pieces_) ok = cuda_ok(dft_scratch_.ensure(hs), "dft stage");
+    return ok;
+}
+
+bool Engine::run_map(MapJob& job, cudaEvent_t* ev, float* host_map) {
+    const MapGeom& g = job.g;
+    const size_t hs = (size_t)job.plan.n_real * g.ny * g.WP * sizeof(float2);
+    if (!map_buffers(job)) return false;
     auto rec = [&](int i) {
         if (ev) cudaEventRecord(ev[i], st);
     };

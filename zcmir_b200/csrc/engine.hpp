@@ -246,6 +246,26 @@ class Engine {
     // against slice k − 1 (fixed) at priors[k − 1] for k = 1..n−1; ms: device time of it all
     bool stack_maps(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,
                     bool calibrated, unsigned cap, zc_shift_result* out, float* ms);
+    // the stack in parts: stack_load uploads the slices, builds their features and plans the
+    // n − 1 maps (every buffer the maps use allocated, every build and autocorrelation finished,
+    // so the maps can be captured); stack_enqueue queues the maps on `st` with each result key
+    // copied into stack_res_ (returns the launches, −1 on an error); stack_collect reads the
+    // keys back into out[0 .. n − 2]
+    bool stack_load(int n, const float* const* images, const int* ws, const int* hs, const Mat3* priors, bool exact,
+                    bool calibrated, unsigned cap);
+    int stack_enqueue();
+    bool stack_collect(zc_shift_result* out);
+    // the buffers run_map uses for a job, allocated now
+    bool map_buffers(const MapJob& job);
+    std::vector<MapJob> stack_jobs_;
+    std::vector<double> stack_areas_;
+    uint64_t stack_gen_ = 0;  // bumped by every stack_load (the combined graph's signature)
+    // the sweep of the current pair and the loaded stack's maps as two branches of one CUDA graph,
+    // launched once (engine_sweep.cpp)
+    bool sweep_stack(const Mat3& H0, int n_peak, SweepOut& sw, zc_shift_result* stack_out, size_t n_out);
+    bool sweep_with_stack_ = false;  // set while sweep_stack runs sweep_maps
+    cudaStream_t branch_st_ = nullptr;  // the stack's branch while the combined graph is captured
+    cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
     // benchmark: warmup + steps maps at H (device-resident inputs), per-step CUDA-event times
     // ms per map of `steps` replays of one captured CUDA graph of job's passes (an L2 flush
     // before each); -1 when the capture or its replay is refused

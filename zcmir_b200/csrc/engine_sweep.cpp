@@ -201,8 +201,8 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
     cp.area = 1.0;
     cp.ridge = 1e-4;
     // per-class events (stream-ordered runs only: they time each plane class)
-    const bool use_graph = sweep_force_.empty() &&
-                           (!getenv("ZCMIR_B200_SWEEP_GRAPH") || atoi(getenv("ZCMIR_B200_SWEEP_GRAPH")) != 0);
+    const bool use_graph = sweep_with_stack_ || (sweep_force_.empty() && (!getenv("ZCMIR_B200_SWEEP_GRAPH") ||
+                                                                         atoi(getenv("ZCMIR_B200_SWEEP_GRAPH")) != 0));
     std::vector<cudaEvent_t> cev;
     if (!use_graph) {
         cev.resize(cls.size() + 1);
@@ -291,6 +291,12 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
                                (uint64_t)c.S, (uint64_t)(uintptr_t)c.tw, (uint64_t)(uintptr_t)c.row.tw,
                                (uint64_t)(uintptr_t)c.col.tw, (uint64_t)(uintptr_t)c.line.tw})
                 put(v);
+        // with the stack's branch: the loaded stack and every buffer its maps use
+        put(sweep_with_stack_ ? stack_gen_ : 0);
+        if (sweep_with_stack_)
+            for (const DevBuf* b : {&canvas_a_, &canvas_b_, &grid_a_, &grid_b_, &half_a_, &half_b_, &q_, &map_, &res_,
+                                    &stack_res_, &dft_scratch_})
+                put((uint64_t)(uintptr_t)b->p), put(b->gen);
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
@@ -316,7 +322,22 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
             bool cap_ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess;
             int n = -1;
             if (cap_ok) {
+                int ns = 0;
+                if (sweep_with_stack_) {
+                    // the stack's maps on a second branch (their own buffers), forked from and
+                    // joined back into the capture, so the two run side by side in one launch
+                    cap_ok = cudaEventRecord(fork_ev_, st) == cudaSuccess &&
+                             cudaStreamWaitEvent(branch_st_, fork_ev_, 0) == cudaSuccess;
+                    std::swap(st, branch_st_);
+                    ns = cap_ok ? stack_enqueue() : -1;
+                    std::swap(st, branch_st_);
+                    if (ns > 0) counts[0] -= (uint32_t)ns;  // captured, not launched: counted per replay
+                }
                 n = enqueue();
+                if (sweep_with_stack_)
+                    cap_ok = cap_ok && cudaEventRecord(join_ev_, branch_st_) == cudaSuccess &&
+                             cudaStreamWaitEvent(st, join_ev_, 0) == cudaSuccess;
+                n = (n < 0 || ns < 0 || !cap_ok) ? -1 : n + ns;
                 const cudaError_t ce = cudaStreamEndCapture(st, &graph);
                 cap_ok = n >= 0 && ce == cudaSuccess && graph &&
                          cudaGraphInstantiate(&sweep_exec_, graph, 0) == cudaSuccess;
@@ -325,6 +346,12 @@ bool Engine::sweep_maps(const Mat3& H0, const SweepGrid& gv, int G, bool exact, 
             if (cap_ok) {
                 sweep_sig_ = sig;
                 sweep_launches_ = n;
+            } else if (sweep_with_stack_) {
+                cudaGetLastError();
+                if (sweep_exec_) cudaGraphExecDestroy(sweep_exec_);
+                sweep_exec_ = nullptr;
+                return done(fail("sweep_stack: the combined graph could not be captured" +
+                                 (err.empty() ? std::string() : ": " + err)));
             } else {
                 cudaGetLastError();  // a refused capture is not this call's error: run stream-ordered
                 err = err_before;
@@ -615,6 +642,31 @@ void Engine::sweep_settings(SweepGrid& gv, int& G, Mat3& H0) {
     gv = sweep_grid(o);
     const double lw = side[0].w, lh = side[0].h, rw = side[1].w, rh = side[1].h;
     H0 = set.b("sw_rel") ? H : translate((rw - lw) / 2, (rh - lh) / 2);
+}
+
+bool Engine::sweep_stack(const Mat3& H0, int n_peak, SweepOut& sw, zc_shift_result* stack_out, size_t n_out) {
+    if (stack_jobs_.empty()) return fail("sweep_stack: load a stack first (zcb_stack_load)");
+    if (!stack_out || n_out < stack_jobs_.size())
+        return fail("sweep_stack: the stack's results need " + std::to_string(stack_jobs_.size()) + " entries");
+    if (!branch_st_ && !cuda_ok(cudaStreamCreateWithFlags(&branch_st_, cudaStreamNonBlocking), "sweep_stack")) return false;
+    for (cudaEvent_t* e : {&fork_ev_, &join_ev_})
+        if (!*e && !cuda_ok(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "sweep_stack")) return false;
+    // the engine pair's builds joined and autocorrelations read: the capture may not wait on them
+    if (!need_images() || !join_side(0) || !join_side(1) || !finish_acf()) return false;
+    SweepGrid gv;
+    int G;
+    Mat3 Hd;
+    sweep_settings(gv, G, Hd);
+    (void)Hd;
+    const double min_ov = std::min(0.5, std::max(0.0, set.f("min_overlap")));
+    struct Flag {
+        bool& f;
+        explicit Flag(bool& x) : f(x) { f = true; }
+        ~Flag() { f = false; }
+    } with_stack(sweep_with_stack_);
+    const bool ran = sweep_maps(H0, gv, G, set.b("exact"), n_peak, min_ov, sw, 0, 0, 1);
+    forget_spectra();  // the stack's branch wrote the map path's canvas and spectrum buffers
+    return ran && stack_collect(stack_out);
 }
 
 bool Engine::tune_sweep(double* out, size_t cap, size_t* used) {

@@ -457,6 +457,44 @@ int32_t zcb_stack_maps(zc_engine* e, uint32_t n, const float* const* images, con
     });
 }
 
+int32_t zcb_stack_load(zc_engine* e, uint32_t n, const float* const* images, const uint32_t* w, const uint32_t* h,
+                       const double* priors, uint32_t flags, uint32_t cap) {
+    return guarded(e, "stack_load", [&] {
+        if (n > 0 && (!w || !h)) return e->fail("stack_load: null sizes");
+        std::vector<int> ws(n), hs(n);
+        for (uint32_t i = 0; i < n; ++i) ws[i] = (int)w[i], hs[i] = (int)h[i];
+        std::vector<zc::Mat3> pr;
+        if (priors)
+            for (uint32_t k = 0; k + 1 < n; ++k) pr.push_back(mat(priors + 9 * k));
+        return e->stack_load((int)n, images, ws.data(), hs.data(), priors ? pr.data() : nullptr, (flags & 1) != 0,
+                             (flags & 2) != 0, cap);
+    });
+}
+
+int32_t zcb_sweep_stack(zc_engine* e, const double H0p[9], uint32_t n_peak, float* scores, uint32_t* idx, size_t cap,
+                        double* info, size_t info_len, zc_shift_result* stack_out, size_t n_out) {
+    return guarded(e, "sweep_stack", [&] {
+        if (info_len < 16 || !info) return e->fail("sweep_stack: info needs 16 entries");
+        zc::SweepGrid gv;
+        int G;
+        zc::Mat3 Hd;
+        e->sweep_settings(gv, G, Hd);
+        zc::SweepOut r;
+        if (!e->sweep_stack(H0p ? mat(H0p) : Hd, (int)n_peak, r, stack_out, n_out)) return false;
+        const size_t n = r.lane_score.size();
+        if (scores && idx) {
+            if (cap < n) return e->fail("sweep_stack: BufferTooSmall");
+            std::copy(r.lane_score.begin(), r.lane_score.end(), scores);
+            std::copy(r.lane_idx.begin(), r.lane_idx.end(), idx);
+        }
+        const double v[16] = {(double)r.cands.size(), r.cell, (double)r.ms, (double)r.G, (double)r.Fx, (double)r.Fy,
+                              (double)r.fx0, (double)r.fy0, (double)r.min_n, (double)r.n, (double)r.groups,
+                              (double)r.batches, (double)r.launches, r.ox, r.oy, (double)r.peaks.size()};
+        std::copy(v, v + 16, info);
+        return true;
+    });
+}
+
 int32_t zcb_tune_sweep(zc_engine* e, double* out, size_t cap, size_t* used) {
     return guarded(e, "tune_sweep", [&] { return e->tune_sweep(out, cap, used); });
 }

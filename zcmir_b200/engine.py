@@ -393,6 +393,36 @@ class Engine:
                   int(bool(exact)) + 2 * int(bool(calibrated)), int(cap), res, ctypes.byref(ms))
         return [MapResult(x) for x in res], ms.value
 
+    def stack_load(self, slices, priors=None, *, exact=True, calibrated=False, cap=0):
+        """zcb_stack_load: the stack's features built and its maps planned, for sweep_stack."""
+        imgs = [gray32(s) for s in slices]
+        n = len(imgs)
+        if n < 2:
+            raise ValueError("a stack needs at least 2 slices")
+        ptrs = (N.f32p * n)(*[_f32(g) for g in imgs])
+        w = np.array([g.shape[1] for g in imgs], np.uint32)
+        h = np.array([g.shape[0] for g in imgs], np.uint32)
+        pr = None if priors is None else np.ascontiguousarray(np.asarray(priors, np.float64).reshape(n - 1, 9))
+        self.call("zcb_stack_load", n, ptrs, _u32(w), _u32(h), None if pr is None else _f64(pr),
+                  int(bool(exact)) + 2 * int(bool(calibrated)), int(cap))
+        self._stack_n = n
+
+    def sweep_stack(self, H0=None, n_peak=4):
+        """zcb_sweep_stack: the sweep of the engine's pair and the loaded stack's maps as two
+        branches of one CUDA graph, launched once → (SweepOut, [MapResult] of the stack)."""
+        n = getattr(self, "_stack_n", 0)
+        if n < 2:
+            raise EngineError("sweep_stack: load a stack first (stack_load)")
+        nc = self.sweep_size()
+        sc = np.zeros((nc, n_peak), np.float32)
+        ix = np.zeros((nc, n_peak), np.uint32)
+        info = np.zeros(len(SWEEP_INFO))
+        res = (N.ShiftResult * (n - 1))()
+        h = None if H0 is None else _pose9(H0)
+        self.call("zcb_sweep_stack", None if h is None else _f64(h), n_peak, _f32(sc), _u32(ix), sc.size, _f64(info),
+                  info.size, res, n - 1)
+        return SweepOut(sc, ix, dict(zip(SWEEP_INFO, map(float, info)))), [MapResult(x) for x in res]
+
     # optimisation
     def climb(self) -> ClimbOut:
         r = N.ClimbResult()
