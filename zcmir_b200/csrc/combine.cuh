@@ -1,5 +1,5 @@
-// The per-shift SMI score in float64 (the reference's combine_cell, shaders/smi.wgsl:825-915),
-// shared by the row-pass kernels.
+// The per-shift SMI score, centred and whitened in float64 (the reference's combine_cell,
+// shaders/smi.wgsl:825-915), shared by the row-pass kernels.
 #pragma once
 
 #include "kernels.hpp"
@@ -43,8 +43,9 @@ __device__ __forceinline__ double lag0_units(const CombineParams& cp, double n00
     return cp.lp_dlam != 0.0 ? n00 * cp.lp_dlam * cp.lp_dth : n00;
 }
 
-// Per-shift score (smi.wgsl:825-915, combine_cell) in float64 with every index known at compile
-// time (NF features, exact or global whitening, calibrated or not), so the 4×4 algebra stays in
+// Per-shift score (smi.wgsl:825-915, combine_cell): centring, ridge, Cholesky factors and the
+// whitened norm in float64, the calibrated map's Wilson–Hilferty transform in float32; every
+// index known at compile time (NF features, exact or global whitening, calibrated or not), so the 4×4 algebra stays in
 // registers. `get(slot)` returns this shift's (unscaled) sum of the plan's slot `slot`; the
 // slots follow the plan (NF = 3 drops the fourth feature's correlations), and every slot passed
 // to it is a compile-time constant. Each Cholesky pivot is inverted once (rsqrt) and the
@@ -148,14 +149,17 @@ __device__ __forceinline__ float combine_smi(G&& get, const CombineParams& p, do
     }
     double score = n * acc;
     if (CALIB) {
-        constexpr double q = NF;
-        const double v = fmin(acc, q - 1e-4);
-        const double fv = (neff - q - 1.0) / q * v / (q - v);
-        const double d1 = q * q, d2 = q * (neff - q - 1.0);
-        const double a = 2.0 / (9.0 * d1), b = 2.0 / (9.0 * d2);
-        const double cc = cbrt(fmax(fv, 0.0));
-        const double z = ((1.0 - b) * cc - (1.0 - a)) / sqrt(b * cc * cc + a);
-        score = fmax(z, 0.0);
+        // the Wilson–Hilferty transform of the whitened statistic in float32: the float64 steps
+        // are the centring and the Cholesky factors above; this tail only rescales their result
+        constexpr float q = NF;
+        const float v = fminf((float)acc, q - 1e-4f);
+        const float nq = (float)neff - q - 1.0f;
+        const float fv = nq * v / (q * (q - v));
+        constexpr float a = 2.0f / (9.0f * q * q);
+        const float b = 2.0f / (9.0f * q * nq);
+        const float cc = cbrtf(fmaxf(fv, 0.0f));
+        const float z = ((1.0f - b) * cc - (1.0f - a)) * rsqrtf(b * cc * cc + a);
+        score = fmaxf(z, 0.0f);
     }
     return (score == score) ? (float)score : 0.f;
 }

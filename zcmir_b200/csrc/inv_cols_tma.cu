@@ -1,12 +1,15 @@
 // The map's inverse-column pass for 1024- and 2048-point columns, fed by TMA.
 //
 // Per item (column tile of TX columns, correlation slot k) the pass forms the products
-// A_ca[k] · conj(B_cb[k]) over the whole tile and inverse-FFTs its columns into Q[k]. One
-// 512-thread block per SM walks the items, correlation fastest (so the blocks running together
-// share the two sides' tiles in L2). Both operand tiles (N rows × TX complex columns each) arrive
-// in shared memory by TMA: one thread issues N/256 box loads per side on an mbarrier, and the
-// next item's copies are issued as soon as the current item's first butterflies have read the
-// staging buffer, so they land while the rest of the transform runs. No thread spends registers
+// A_ca[k] · conj(B_cb[k]) over the whole tile and inverse-FFTs its columns into Q[k]. The
+// correlations are walked in runs that share one operand plane (make_units: the 45 of the full
+// plan in 10 runs of 4–5), and one 512-thread block per SM walks the (column tile, run) units,
+// run fastest (so the blocks running together share the tile's planes in L2). Both operand tiles
+// (N rows × TX complex columns each) arrive in shared memory by TMA: one thread issues N/256
+// box loads per side on an mbarrier. Within a run only the streamed side's tile is copied again,
+// so a column tile costs 55 tile copies out of L2 instead of 90. The next item's copies are
+// issued as soon as the current item's first butterflies have read the staging buffers, so they
+// land while the rest of the transform runs. No thread spends registers
 // or load instructions on the operands, and the twiddles of every stage after the first, which
 // depend only on a thread's place in its line, are read once per block into registers rather
 // than once per item.
@@ -182,15 +185,67 @@ template <int N>
 struct InvColsShape {
     static constexpr int TL = N / 16;          // threads per line
     static constexpr int TX = 512 / TL;        // columns per item
-    static constexpr size_t stage_bytes = (size_t)2 * N * TX * sizeof(float2);
-    static constexpr size_t smem = stage_bytes + (size_t)TX * line_pitch(N) * sizeof(float2) + 16;
+    static constexpr size_t tile_bytes = (size_t)N * TX * sizeof(float2);
+    static constexpr size_t smem = 2 * tile_bytes + (size_t)TX * line_pitch(N) * sizeof(float2) + 16;
 };
+
+// Runs of correlations that share one operand plane: unit u keeps side side[u]'s plane res[u]
+// resident in shared memory while its n[u] correlations k[u][·] stream the other side's plane.
+constexpr int kUnitMax = 5;
+constexpr int kMaxUnits = 48;
+struct InvUnits {
+    int count;
+    signed char side[kMaxUnits];  // 0: side A's plane stays, 1: side B's
+    signed char n[kMaxUnits];
+    signed char k[kMaxUnits][kUnitMax];
+};
+
+// Cover the plan's correlations with runs sharing an operand: repeatedly take the plane (of
+// either side) shared by the most correlations left, and cut its correlations into runs of at
+// most kUnitMax of nearly equal length. The 45-correlation plan gives 10 runs (plane 1 of A:
+// 15 in 3 runs, plane 1 of B: 14 in 3, then A's f_i planes: 4 runs of 4), so a column tile
+// loads 55 operand tiles instead of 90.
+bool make_units(const CorrPlanDev& plan, InvUnits& u) {
+    u = InvUnits{};
+    bool left[45] = {};
+    int n_left = plan.n_corr;
+    for (int c = 0; c < plan.n_corr; ++c) left[c] = true;
+    while (n_left > 0) {
+        int best_side = 0, best_plane = -1, best_n = 0;
+        for (int sd = 0; sd < 2; ++sd)
+            for (int pl = 0; pl < plan.n_real; ++pl) {
+                int cnt = 0;
+                for (int c = 0; c < plan.n_corr; ++c)
+                    if (left[c] && (sd == 0 ? plan.ca[c] : plan.cb[c]) == pl) ++cnt;
+                if (cnt > best_n) best_side = sd, best_plane = pl, best_n = cnt;
+            }
+        if (best_n == 0) return false;
+        const int runs = (best_n + kUnitMax - 1) / kUnitMax;
+        int c = 0;
+        for (int r = 0; r < runs; ++r) {
+            if (u.count >= kMaxUnits) return false;
+            const int len = best_n / runs + (r < best_n % runs ? 1 : 0);
+            const int ui = u.count++;
+            u.side[ui] = (signed char)best_side;
+            u.n[ui] = (signed char)len;
+            for (int i = 0; i < len; ++i) {
+                while (!(left[c] && (best_side == 0 ? plan.ca[c] : plan.cb[c]) == best_plane)) ++c;
+                u.k[ui][i] = (signed char)c;
+                left[c] = false;
+                ++c;
+            }
+            n_left -= len;
+        }
+    }
+    return true;
+}
 
 template <int N>
 __global__ void __launch_bounds__(512, 1) k_inv_cols_tma(const __grid_constant__ CUtensorMap map_a,
                                                          const __grid_constant__ CUtensorMap map_b, CorrPlanDev plan,
+                                                         const __grid_constant__ InvUnits units,
                                                          const float2* __restrict__ tw, int ncols,
-                                                         float2* __restrict__ Q, size_t pstride, int WP, int nitems,
+                                                         float2* __restrict__ Q, size_t pstride, int WP, int nwork,
                                                          unsigned* __restrict__ fault) {
     using SH = InvColsShape<N>;
     constexpr int TL = SH::TL, TX = SH::TX, R0 = mix_radix(N, 0), M0 = N / R0;
@@ -203,18 +258,19 @@ __global__ void __launch_bounds__(512, 1) k_inv_cols_tma(const __grid_constant__
     uint64_t* bar = reinterpret_cast<uint64_t*>(lines + (size_t)TX * line_pitch(N));
     const int tid = threadIdx.x, c = tid % TX, t = tid / TX;
     float2* buf = lines + c * line_pitch(N);
-    const int nk = plan.n_corr;
+    const int nu = units.count;
     if (smem_addr(sa) & 127) {  // a tiled copy's destination must be 128-byte aligned
         if (tid == 0) atomicOr(fault, 2u);
         return;
     }
-    auto issue = [&](int item) {
-        const int k = item % nk, col0 = (item / nk) * TX;
-        mbar_expect_tx(bar, (uint32_t)SH::stage_bytes);
+    // copies of column tile col0: side A's plane pa into sa and side B's pb into sb; a negative
+    // plane leaves that side's tile as it is
+    auto issue = [&](int col0, int pa, int pb) {
+        mbar_expect_tx(bar, (uint32_t)(((pa >= 0) + (pb >= 0)) * SH::tile_bytes));
 #pragma unroll 1
         for (int i = 0; i < N / kBoxRows; ++i) {
-            tma_load_3d(sa + (size_t)i * kBoxRows * TX, &map_a, 2 * col0, i * kBoxRows, plan.ca[k], bar);
-            tma_load_3d(sb + (size_t)i * kBoxRows * TX, &map_b, 2 * col0, i * kBoxRows, plan.cb[k], bar);
+            if (pa >= 0) tma_load_3d(sa + (size_t)i * kBoxRows * TX, &map_a, 2 * col0, i * kBoxRows, pa, bar);
+            if (pb >= 0) tma_load_3d(sb + (size_t)i * kBoxRows * TX, &map_b, 2 * col0, i * kBoxRows, pb, bar);
         }
     };
     float2 w[rt_total(N, TL)];
@@ -224,42 +280,59 @@ __global__ void __launch_bounds__(512, 1) k_inv_cols_tma(const __grid_constant__
         mbar_init_fence();
     }
     __syncthreads();
-    int item = blockIdx.x;
-    if (tid == 0 && item < nitems) issue(item);
+    int wk = blockIdx.x;
+    if (tid == 0 && wk < nwork) {
+        const int k0 = units.k[wk % nu][0];
+        issue((wk / nu) * TX, plan.ca[k0], plan.cb[k0]);
+    }
     uint32_t phase = 0;
-    for (; item < nitems; item += gridDim.x) {
-        const bool ok = mbar_wait(bar, phase);
-        if (__syncthreads_or(!ok)) {
-            // a copy did not land: report it, give the copies in flight one more bounded wait, stop
-            if (tid == 0) {
-                atomicOr(fault, 1u);
-                mbar_wait(bar, phase);
-            }
-            return;
-        }
-        phase ^= 1u;
-        const int k = item % nk, col = (item / nk) * TX + c;
+    for (; wk < nwork; wk += gridDim.x) {
+        const int un = wk % nu, col0 = (wk / nu) * TX, len = units.n[un];
+        const bool keep_a = units.side[un] == 0;
+        const int col = col0 + c;
         const bool okc = col < ncols;
-        float2* O = Q + (size_t)k * pstride + (okc ? col : 0);
-        float2 v[R0];
+#pragma unroll 1
+        for (int i = 0; i < len; ++i) {
+            const bool ok = mbar_wait(bar, phase);
+            if (__syncthreads_or(!ok)) {
+                // a copy did not land: report it, give the copies in flight one more bounded wait, stop
+                if (tid == 0) {
+                    atomicOr(fault, 1u);
+                    mbar_wait(bar, phase);
+                }
+                return;
+            }
+            phase ^= 1u;
+            const int k = units.k[un][i];
+            float2* O = Q + (size_t)k * pstride + (okc ? col : 0);
+            float2 v[R0];
 #pragma unroll
-        for (int r = 0; r < R0; ++r) {
-            const int y = t + r * M0;
-            v[r] = cmulc(sa[y * TX + c], sb[y * TX + c]);
-        }
-        dft<R0, true>(v);
+            for (int r = 0; r < R0; ++r) {
+                const int y = t + r * M0;
+                v[r] = cmulc(sa[y * TX + c], sb[y * TX + c]);
+            }
+            dft<R0, true>(v);
 #pragma unroll
-        for (int r = 0; r < R0; ++r) buf[first_slot<R0>(t, r)] = v[r];
-        __syncthreads();  // the staging buffer is read: the next item's copies may land in it
-        if (tid == 0 && item + (int)gridDim.x < nitems) {
-            fence_proxy_async();
-            issue(item + gridDim.x);
+            for (int r = 0; r < R0; ++r) buf[first_slot<R0>(t, r)] = v[r];
+            __syncthreads();  // both tiles are read: the next copies may land in them
+            if (tid == 0) {
+                if (i + 1 < len) {
+                    // the run's next correlation: only the streamed side's plane changes
+                    const int kn = units.k[un][i + 1];
+                    fence_proxy_async();
+                    issue(col0, keep_a ? -1 : plan.ca[kn], keep_a ? plan.cb[kn] : -1);
+                } else if (wk + (int)gridDim.x < nwork) {
+                    const int wn = wk + gridDim.x, kn = units.k[wn % nu][0];
+                    fence_proxy_async();
+                    issue((wn / nu) * TX, plan.ca[kn], plan.cb[kn]);
+                }
+            }
+            rt_mid<N, TL, true, 1>(buf, w, t);
+            rt_last<N, TL, true>(buf, w, t, [&](int y, float2 val) {
+                if (okc) O[(size_t)y * WP] = val;
+            });
+            __syncthreads();  // the line buffers are refilled by the next item
         }
-        rt_mid<N, TL, true, 1>(buf, w, t);
-        rt_last<N, TL, true>(buf, w, t, [&](int y, float2 val) {
-            if (okc) O[(size_t)y * WP] = val;
-        });
-        __syncthreads();  // the line buffers are refilled by the next item
     }
 }
 
@@ -297,14 +370,16 @@ cudaError_t launch_tma(const float2* ha, const float2* hb, const MapGeom& g, con
         return cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
     if (!fault && (e = fault_word(&fault)) != cudaSuccess) return e;
-    const int nitems = plan.n_corr * ((ncols + SH::TX - 1) / SH::TX);
+    InvUnits units;
+    if (!make_units(plan, units)) return cudaErrorInvalidValue;
+    const int nitems = units.count * ((ncols + SH::TX - 1) / SH::TX);
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     auto k = k_inv_cols_tma<N>;
     if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::smem)) != cudaSuccess)
         return e;
-    k<<<std::min(nitems, sms), 512, SH::smem, st>>>(ma, mb, plan, tw, ncols, Q, pstride, g.WP, nitems, fault);
+    k<<<std::min(nitems, sms), 512, SH::smem, st>>>(ma, mb, plan, units, tw, ncols, Q, pstride, g.WP, nitems, fault);
     return cudaGetLastError();
 }
 
