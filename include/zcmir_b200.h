@@ -136,6 +136,26 @@ int32_t zcb_prop_grad(const float* params, size_t np, const float* x, const int3
 int32_t zcb_prop_train(float* params, size_t np, const float* x, const int32_t* labels, uint32_t n, uint32_t batch,
                        uint32_t epochs, float lr, uint32_t seed, float* epoch_loss);
 
+/* The 2-D convolutional pose proposal on the tensor cores (no counterpart in the reference): input
+ * x [n][128][128][8] BF16 bits (uint16; NHWC: 4 feature planes of each image of a pair), four
+ * 3×3 stride-2 convolutions 8→32→64→64→128 with ReLU, the mean over the 8×8 positions and a
+ * linear layer to logits [n][216] (24 rotation × 9 log-scale bins, index 9·r + s). Weights are
+ * used rounded to BF16, activations stored in BF16, every product summed in FP32 (mma.sync
+ * m16n8k16). params: zcb_cnn_nparams() float32 (W1 [32][3][3][8], b1, W2 [64][3][3][32], b2,
+ * W3 [64][3][3][64], b3, W4 [128][3][3][64], b4, Wfc [216][128], bfc). The calls allocate and
+ * free their own device memory; 0 / −1 with the message from zcb_cnn_error. */
+size_t zcb_cnn_nparams(void);
+size_t zcb_cnn_error(char* buf, size_t cap);
+int32_t zcb_cnn_forward(const float* params, size_t np, const uint16_t* x, uint32_t n, float* logits);
+/* the mean softmax cross-entropy over labels (0..215) of a batch of n ≤ 4096, and its gradient */
+int32_t zcb_cnn_grad(const float* params, size_t np, const uint16_t* x, const int32_t* labels, uint32_t n, float* loss,
+                     float* grad);
+/* Adam (β 0.9 / 0.999) for `steps` minibatches of `batch` ≤ 1024 drawn with replacement (seeded)
+ * from the n samples, all held on the device; params in/out; losses[steps] (nullable) each
+ * step's mean loss; ms_per_step (nullable) the device time per step */
+int32_t zcb_cnn_train(float* params, size_t np, const uint16_t* x, const int32_t* labels, uint32_t n, uint32_t batch,
+                      uint32_t steps, float lr, uint64_t seed, float* losses, float* ms_per_step);
+
 #ifdef __cplusplus
 }
 #endif

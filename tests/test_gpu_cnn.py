@@ -1,0 +1,71 @@
+"""The 2-D convolutional proposal on the tensor cores (zcb_cnn_forward / _grad / _train) against
+the float64 oracle that rounds at the same points to BF16, and its training.
+
+Tolerances: the GPU sums each product in float32 where the oracle sums in float64, so a BF16
+rounding of an activation or a gradient near a rounding boundary can go the other way (one BF16
+step, 2^-8 relative) and carry through the later layers: logits within 1e-2 of the largest,
+the loss within 1e-3 relative, each layer's gradient within 3e-2 of the oracle's in norm."""
+import numpy as np
+import pytest
+
+from oracle import cnn_oracle as C
+from zcmir_b200 import cnn
+
+pytestmark = pytest.mark.gpu
+
+
+def _x(seed, n):
+    rng = np.random.default_rng(seed)
+    return cnn.to_bf16(rng.standard_normal((n, 128, 128, 8)).astype(np.float32))
+
+
+def test_parameter_count_and_bf16_bits_match_the_oracle():
+    assert cnn.nparams() == C.n_params()
+    x = np.random.default_rng(0).standard_normal(1000).astype(np.float32) * 7
+    assert np.array_equal(cnn.to_bf16(x), C.bf16_bits(x))
+
+
+def test_forward_matches_oracle():
+    p = cnn.init_params(3)
+    x = _x(1, 5)
+    z = cnn.forward(p, x)
+    zr, _ = C.forward(p.astype(np.float64), C.from_bits(x))
+    assert z.shape == (5, 216)
+    assert np.abs(z - zr).max() <= 1e-2 * np.abs(zr).max(), np.abs(z - zr).max()
+
+
+def test_gradient_matches_oracle():
+    p = cnn.init_params(4)
+    x = _x(2, 4)
+    y = np.array([0, 17, 108, 215], np.int32)
+    loss, g = cnn.grad(p, x, y)
+    lr, gr = C.loss_grad(p.astype(np.float64), C.from_bits(x), y)
+    assert abs(loss - lr) <= 1e-3 * abs(lr)
+    o = 0
+    for l in range(4):
+        for n in (C.CH[l + 1] * 9 * C.CH[l], C.CH[l + 1]):
+            a, b = g[o:o + n], gr[o:o + n]
+            assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b) + 1e-7, (l, n, np.linalg.norm(a - b), np.linalg.norm(b))
+            o += n
+    a, b = g[o:], gr[o:]
+    assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b)
+
+
+def test_training_fits_a_learnable_map():
+    """Samples whose label sets a constant offset on two channels (channel label mod 8 up, channel
+    (label // 8) mod 8 down, over noise): Adam on the GPU takes the loss from about ln 216 down
+    and ranks the label first on most training samples."""
+    rng = np.random.default_rng(5)
+    n = 1024
+    y = rng.integers(0, 216, n).astype(np.int32)
+    x = rng.standard_normal((n, 128, 128, 8)).astype(np.float32) * 0.5
+    x[np.arange(n), :, :, y % 8] += (1.0 + (y // 64))[:, None, None]
+    x[np.arange(n), :, :, (y // 8) % 8] -= 1.0
+    xb = cnn.to_bf16(x)
+    p0 = cnn.init_params(6)
+    p, losses, ms = cnn.train(p0, xb, y, batch=128, steps=400, lr=2e-3, seed=7)
+    assert losses[:10].mean() > 4.0
+    assert losses[-20:].mean() < 0.5 * losses[:10].mean(), (losses[:10].mean(), losses[-20:].mean())
+    assert ms > 0
+    z = cnn.forward(p, xb[:256])
+    assert np.mean(np.argmax(z, 1) == y[:256]) > 0.3

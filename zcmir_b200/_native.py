@@ -106,6 +106,12 @@ SIGS = {
     "zcb_prop_forward": ([f32p, SZ, f32p, U32, f32p], I32),
     "zcb_prop_grad": ([f32p, SZ, f32p, ctypes.POINTER(ctypes.c_int32), U32, f32p, f32p], I32),
     "zcb_prop_train": ([f32p, SZ, f32p, ctypes.POINTER(ctypes.c_int32), U32, U32, U32, ctypes.c_float, U32, f32p], I32),
+    "zcb_cnn_nparams": ([], SZ),
+    "zcb_cnn_error": ([ctypes.c_char_p, SZ], SZ),
+    "zcb_cnn_forward": ([f32p, SZ, ctypes.POINTER(ctypes.c_uint16), U32, f32p], I32),
+    "zcb_cnn_grad": ([f32p, SZ, ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_int32), U32, f32p, f32p], I32),
+    "zcb_cnn_train": ([f32p, SZ, ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_int32), U32, U32, U32,
+                       ctypes.c_float, ctypes.c_uint64, f32p, f32p], I32),
     "zcb_settings_apply": ([ctypes.c_char_p, SZ, ctypes.c_char_p, SZ, ctypes.POINTER(SZ), ctypes.c_char_p, SZ, ctypes.POINTER(SZ)], I32),
 }
 
