@@ -37,6 +37,15 @@ __host__ __device__ __forceinline__ constexpr int line_pitch(int n) {
     return p + ((4 - (p & 15)) & 15);
 }
 
+// Pitch between the tx lines of a column tile whose threads run column-fastest (line c = thread
+// mod tx): a half-warp then touches min(tx, 16) lines at 16 / min(tx, 16) consecutive points each,
+// and the pitch puts them in distinct bank pairs — ≡ 16/tx (mod 16) for tx = 2, 4, 8, odd for
+// 16 or more lines (or a count that is not a power of two), where each line is touched once.
+__host__ __device__ __forceinline__ constexpr int tile_pitch(int n, int tx) {
+    return (tx >= 16 || (tx & (tx - 1)) != 0) ? (padded_len(n) | 1)
+                                               : padded_len(n) + (((16 / tx) - (padded_len(n) & 15)) & 15);
+}
+
 // Padded slots of the points i0 + r·D (r = 0, 1, ...) from p0 = pad_idx(i0), for a compile-time
 // step D, folded to constant offsets: when D is a multiple of 16 every step adds D + D/16; when
 // all the points lie in one aligned group of 16 (the caller guarantees it) every step adds D.

@@ -46,6 +46,15 @@ inline size_t multi_row_smem(int nx, int n_corr, int tl, int RB) {
     return (size_t)multi_lines(tl) * padded_len(nx) * sizeof(float2) + (size_t)RB * n_corr * nx * sizeof(float);
 }
 
+// Line pitch of a column tile. Lines of 1024 points and more come in tiles of at most 8 lines
+// (512 threads of N/16) and keep line_pitch's ≡ 4 (mod 16), a compile-time constant for
+// compile-time lines; shorter lines come in wide tiles (the sweep's 192-point columns: 33 lines)
+// whose warps touch 32 lines at one point each, which tile_pitch's odd pitch spreads over all
+// bank pairs (≡ 4 put them in 4).
+__host__ __device__ __forceinline__ constexpr int col_pitch(int n, int tx) {
+    return n >= 1024 ? line_pitch(n) : tile_pitch(n, tx);
+}
+
 enum class Pass { FwdRows, FwdCols, InvCols, Rows };
 
 // Everything a pass launch needs; the batch's items sit at the given strides (elements).
@@ -156,7 +165,7 @@ __global__ void __launch_bounds__(512, 2) k_cols(float2* __restrict__ half, size
     extern __shared__ float2 smem[];
     const int x0 = blockIdx.x * tx;
     float2* base = half + (size_t)blockIdx.y * pstride;
-    const int pl = line_pitch(f.n());
+    const int pl = col_pitch(f.n(), tx);
     const int c = threadIdx.x % tx, t = threadIdx.x / tx, col = x0 + c;
     const bool okc = col < ncols;
     float2* p = base + col;
@@ -185,7 +194,7 @@ __global__ void __launch_bounds__(512, 2) k_inv_cols(const float2* __restrict__ 
     const float2* A = ha + item * abs_ + (size_t)plan.ca[k] * pstride + col;
     const float2* B = hb + item * bbs + (size_t)plan.cb[k] * pstride + col;
     float2* O = Q + item * qbs + (size_t)k * pstride + col;
-    const int pl = line_pitch(f.n());
+    const int pl = col_pitch(f.n(), tx);
     f.template run_io<true>(
         smem + c * pl, t, true,
         [&](int y) {
@@ -451,7 +460,7 @@ inline int lines_per_block(int tl, int want_threads) { return std::max(1, want_t
 // shared memory
 inline int col_tile(int n, int tl, int ncols) {
     int tx = std::min(lines_per_block(tl, 512), ncols);
-    while (tx > 1 && (size_t)tx * line_pitch(n) * sizeof(float2) > 110 * 1024) tx >>= 1;
+    while (tx > 1 && (size_t)tx * col_pitch(n, tx) * sizeof(float2) > 110 * 1024) tx >>= 1;
     // the same number of tiles, balanced: no last tile of mostly idle columns
     const int tiles = (ncols + tx - 1) / tx;
     return (ncols + tiles - 1) / tiles;
@@ -513,7 +522,7 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
     } else if constexpr (P == Pass::FwdCols) {
         const int ncols = g.nx / 2 + 1;
         const int tx = col_tile(g.ny, tl, ncols);
-        const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
+        const size_t sm = (size_t)tx * col_pitch(g.ny, tx) * sizeof(float2);
         auto k = 2 * g.ch <= g.ny ? k_cols<F, false, true> : k_cols<F, false, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k<<<dim3((ncols + tx - 1) / tx, plan.n_real * a.batch), tx * tl, sm, st>>>(
@@ -537,7 +546,7 @@ cudaError_t run_pass(F f, const PassArgs& a, cudaStream_t st) {
             }
         }
         const int tx = col_tile(g.ny, tl, ncols);
-        const size_t sm = (size_t)tx * line_pitch(g.ny) * sizeof(float2);
+        const size_t sm = (size_t)tx * col_pitch(g.ny, tx) * sizeof(float2);
         cudaFuncSetAttribute(k_inv_cols<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_inv_cols<F><<<dim3(plan.n_corr, (ncols + tx - 1) / tx, a.batch), tx * tl, sm, st>>>(
             a.half, a.half_b, pstride, g.WP, ncols, plan, f, tx, a.Q, a.half_stride, a.b_stride, a.q_stride);
