@@ -157,8 +157,8 @@ def _pose_pair(seed):
     rng = np.random.default_rng(1_000_003 * (seed + 1))
     deg = float(rng.uniform(0, 360))
     scale = float(np.exp(rng.uniform(np.log(S_MIN), np.log(S_MAX))))
-    m, f, _ = synth.pair_similarity(n=SIDE, seed=seed, deg=deg, scale=scale)
-    return m, f, deg, scale
+    m, f, H = synth.pair_similarity(n=SIDE, seed=seed, deg=deg, scale=scale)
+    return m, f, deg, scale, H
 
 
 def pose_dataset(seeds, workers=None):
@@ -170,15 +170,33 @@ def pose_dataset(seeds, workers=None):
     workers = workers or max(1, min(16, os.cpu_count() or 1))
     with mp.get_context("spawn").Pool(workers) as pool:
         res = pool.map(_pose_pair, list(seeds), chunksize=32)
-    x = pair_stacks([(m, f) for m, f, _, _ in res])
+    x = pair_stacks([(r[0], r[1]) for r in res])
     deg = np.array([r[2] for r in res])
     sc = np.array([r[3] for r in res])
     return x, labels(deg, sc), deg, sc
 
 
-def evaluate_pose(n_train=6000, n_test=500, steps=3000, batch=256, lr=1e-3, seed=0):
+def shipped_params():
+    """The network trained by this build (zcmir_b200/data/cnn_params.npy)."""
+    from pathlib import Path
+
+    return np.load(Path(__file__).resolve().parent / "data" / "cnn_params.npy").astype(np.float32)
+
+
+def pose_scores(p, xt, yt):
+    """Held-out hit rates of params p on stacks xt with labels yt."""
+    z = forward(p, xt)
+    r_pred = np.argmax(z, 1) // SCALE_BINS
+    r_true = yt // SCALE_BINS
+    dr = np.minimum((r_pred - r_true) % ROT_BINS, (r_true - r_pred) % ROT_BINS)
+    return {"test_top1": float(np.mean(np.argmax(z, 1) == yt)), "test_top8": top_k_hits(z, yt, 8),
+            "test_rotation_within_1_bin": float(np.mean(dr <= 1))}
+
+
+def evaluate_pose(n_train=6000, n_test=500, steps=3000, batch=256, lr=1e-3, seed=0, save=None):
     """Train on n_train seeded pairs, report on n_test held-out pairs: the label's top-1 / top-8
-    hit rates, the rotation bin within one bin (either sense), against chance."""
+    hit rates, the rotation bin within one bin (either sense), against chance; save: where to
+    write the trained parameters (.npy)."""
     import time
 
     t0 = time.perf_counter()
@@ -186,6 +204,8 @@ def evaluate_pose(n_train=6000, n_test=500, steps=3000, batch=256, lr=1e-3, seed
     xt, yt, _, _ = pose_dataset(range(10_000_000 + seed, 10_000_000 + seed + n_test))
     t_data = time.perf_counter() - t0
     p, losses, ms = train(init_params(seed), x, y, batch=batch, steps=steps, lr=lr, seed=seed + 1)
+    if save:
+        np.save(save, p)
     z = forward(p, xt)
     zr = forward(p, x[:n_test])
     r_pred = np.argmax(z, 1) // SCALE_BINS
@@ -202,6 +222,72 @@ def evaluate_pose(n_train=6000, n_test=500, steps=3000, batch=256, lr=1e-3, seed
     }
 
 
+def search(reg, params=None, k=8, offsets=(-5.0, 0.0, 5.0), iters=25):
+    """The network's proposal search on the 128² pair loaded in reg: the network reads the pair's
+    feature stacks, its k best bins each give len(offsets) seeds (the bin's centre rotation plus
+    each offset in degrees, the bin's scale, about the moving centre), each seed is placed by one
+    shift map and all are refined together by the batched Gauss–Newton (zcb_refine_poses); the
+    best refined pose becomes the pose when it beats the current one. Returns dict(H, score,
+    maps)."""
+    from . import proposal
+
+    (mw, mh), (fw, fh) = reg.image_size(0), reg.image_size(1)
+    if (mw, mh, fw, fh) != (SIDE, SIDE, SIDE, SIDE):
+        raise ValueError(f"cnn.search: the network reads pairs of {SIDE}² images")
+    p = shipped_params() if params is None else params
+    st = np.concatenate([reg.features(0), reg.features(1)])
+    z = forward(p, to_bf16(np.transpose(st, (1, 2, 0)))[None])[0]
+    cur = reg.score().mean
+    seeds = []
+    for b in np.argsort(-z)[:k]:
+        deg, sc = bin_pose(b)
+        for o in offsets:
+            H = proposal.candidate_pose(reg, deg + o, sc)
+            sm = reg.shift_map(H, want_map=False)
+            seeds.append(np.array([[1, 0, -sm.dx], [0, 1, -sm.dy], [0, 0, 1.0]]) @ H)
+    Hs, scores = reg.refine_poses(np.array(seeds), iters)
+    i = int(np.argmax(scores))
+    best_H, best_s = np.asarray(Hs[i]), float(scores[i])
+    if best_s > cur + max(1e-6 * abs(cur), 1e-12):
+        reg.pose = best_H
+    return dict(H=best_H, score=best_s, maps=len(seeds))
+
+
+def evaluate_search(n_pairs=64, params=None, k=8, seed=30_000_000):
+    """The network's search against the plain search (the full 360 × 9 sweep, its screen and
+    finalists) on n_pairs held-out 128² pairs on the same GPU: per form the mean seconds per
+    search and the share within 0.5 px corner RMS of the planted pose."""
+    import time
+
+    from . import proposal
+    from .engine import Engine
+
+    p = shipped_params() if params is None else params
+    out = {"pairs": n_pairs, "k": k}
+    rows = {"plain": [], "cnn": []}
+    with Engine(half=False, sw_nth=360, sw_ns=9, sw_smin=S_MIN, sw_smax=S_MAX, sw_grid=SIDE) as reg:
+        for j in range(n_pairs):
+            m, f, _, _, Ht = _pose_pair(seed + j)
+            reg.set_images(m / 65535.0, f / 65535.0, preprocess=False)
+            for form in ("plain", "cnn"):
+                reg.pose = np.eye(3)
+                reg.score()
+                t0 = time.perf_counter()
+                if form == "plain":
+                    r = reg.search()
+                    H = np.asarray(r.H)
+                else:
+                    H = search(reg, p, k=k)["H"]
+                dt = time.perf_counter() - t0
+                rows[form].append((dt, proposal.corner_rms(H, Ht, SIDE, SIDE)))
+    for form, r in rows.items():
+        a = np.array(r)
+        out[form] = {"seconds_per_search": float(a[1:, 0].mean()) if len(a) > 1 else float(a[0, 0]),
+                     "within_0_5_px": float(np.mean(a[:, 1] <= 0.5)),
+                     "median_corner_rms_px": float(np.median(a[:, 1]))}
+    return out
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -212,5 +298,10 @@ if __name__ == "__main__":
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--save", default=None)
+    ap.add_argument("--search", type=int, default=0, help="compare the searches on this many held-out pairs")
     a = ap.parse_args()
-    print(json.dumps(evaluate_pose(a.train, a.test, a.steps, a.batch, a.lr)))
+    if a.search:
+        print(json.dumps(evaluate_search(a.search)))
+    else:
+        print(json.dumps(evaluate_pose(a.train, a.test, a.steps, a.batch, a.lr, save=a.save)))
