@@ -204,6 +204,27 @@ def survey_bytes(p):
     return 2 * 5 * p["canvas_w"] * p["canvas_h"] * 4 + 2 * (2 * P * nx * (ny // 2 + 1) * 8) + nx * ny * 4
 
 
+def survey_flops(p):
+    """The whole map's FP32 flops by the survey's counting rule: both sides' forward FFTs over the
+    canvas rows and all columns (packed complex lines), the inverse 2-D FFTs of the packed
+    correlations, the conjugate products and about 300 flops of scoring per shift."""
+    nx, ny, ch, P, C = p["nx"], p["ny"], p["ch"], p["n_real"], p["n_corr"]
+    lx, ly = np.log2(nx), np.log2(ny)
+    fwd = 2 * ((P + 1) // 2) * 5 * (nx * lx * ch + ny * ly * nx)
+    inv = ((C + 1) // 2) * 5 * nx * ny * np.log2(nx * ny)
+    return float(fwd + inv + 10 * C * nx * ny + 300 * nx * ny)
+
+
+def fp32_peak_tflops():
+    """The device's FMA rate measured now by zcb_fp32_peak (TFLOP/s), or None."""
+    import ctypes
+
+    from zcmir_b200 import _native
+
+    t = ctypes.c_double(0.0)
+    return t.value if _native.load().zcb_fp32_peak(ctypes.byref(t)) == 0 else None
+
+
 def cpu_map_seconds(m, f):
     """One map of the pair by the CPU restatement (float64; scipy FFTs on every host core)."""
     import scipy.fft as sf
@@ -553,6 +574,7 @@ def run_gpu(args, rank, ws, local):
         tf = ROOT / "profiles" / "traffic.json"
         if tf.exists():
             traffic = json.loads(tf.read_text()).get(top)
+        fp32 = fp32_peak_tflops()
         line = {
             "metric": METRIC, "value": ws * 1000.0 / ms, "unit": "maps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -571,7 +593,11 @@ def run_gpu(args, rank, ws, local):
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": b_launch, "launch_ms": t_launch,
                          "map_algorithmic_bytes": survey_bytes(r),
-                         "map_frac": survey_bytes(r) / (ms * 1e-3) / 1e9 / hbm},
+                         "map_frac": survey_bytes(r) / (ms * 1e-3) / 1e9 / hbm,
+                         "map_fp32": {"flops_per_map": survey_flops(r),
+                                      "tflops": survey_flops(r) / (ms * 1e-3) / 1e12,
+                                      "peak_tflops": fp32, "peak_source": "measured in this run (zcb_fp32_peak)",
+                                      "frac": (survey_flops(r) / (ms * 1e-3) / 1e12 / fp32) if fp32 else None}},
             "e2e": {"value": ws / e2e_s, "unit": "maps/s", "h2d_bytes_per_step": int(pm.nbytes + pf.nbytes),
                     "d2h_bytes_per_step": int(2048 * 2048 * 4 + 88)},
             "gpu_launches": int(launches),

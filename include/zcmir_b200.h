@@ -156,6 +156,10 @@ int32_t zcb_cnn_grad(const float* params, size_t np, const uint16_t* x, const in
 int32_t zcb_cnn_train(float* params, size_t np, const uint16_t* x, const int32_t* labels, uint32_t n, uint32_t batch,
                       uint32_t steps, float lr, uint64_t seed, float* losses, float* ms_per_step);
 
+/* The device's measured FP32 rate (TFLOP/s, fused multiply-adds counted as two), the
+ * denominator of the maps' FP32 roofline fraction (no counterpart in the reference). 0 / −1. */
+int32_t zcb_fp32_peak(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

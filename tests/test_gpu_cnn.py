@@ -80,3 +80,27 @@ def test_shipped_network_places_held_out_pairs():
     s = cnn.pose_scores(cnn.shipped_params(), x, y)
     assert s["test_top8"] >= 5 * 8 / 216, s
     assert s["test_rotation_within_1_bin"] >= 3 * 3 / 24, s
+
+
+def test_network_search_finds_the_plain_search_pose():
+    """On 10 held-out 128² pairs the network's search (its 8 best bins, three rotations each,
+    placed by shift maps, the 4 best refined by the batched Gauss–Newton) reaches the plain
+    search's pose (within 0.5 px corner RMS) on at least 2 — 56 % in the 32-pair evaluation —
+    and never ends below the score it started from."""
+    from zcmir_b200 import proposal
+    from zcmir_b200.engine import Engine
+
+    p = cnn.shipped_params()
+    same = 0
+    with Engine(half=False, sw_nth=360, sw_ns=9, sw_smin=0.8, sw_smax=1.25, sw_grid=128) as reg:
+        for j in range(10):
+            m, f, _, _, _ = cnn._pose_pair(40_000_000 + j)
+            reg.set_images(m / 65535.0, f / 65535.0, preprocess=False)
+            reg.pose = np.eye(3)
+            Hp = np.asarray(reg.search().H)
+            reg.pose = np.eye(3)
+            s0 = reg.score().mean
+            r = cnn.search(reg, p, k=8, keep=4)
+            assert r["maps"] == 24 and reg.score().mean >= s0 - 1e-6 * abs(s0)
+            same += proposal.corner_rms(r["H"], Hp, 128, 128) <= 0.5
+    assert same >= 2, same

@@ -112,6 +112,7 @@ SIGS = {
     "zcb_cnn_grad": ([f32p, SZ, ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_int32), U32, f32p, f32p], I32),
     "zcb_cnn_train": ([f32p, SZ, ctypes.POINTER(ctypes.c_uint16), ctypes.POINTER(ctypes.c_int32), U32, U32, U32,
                        ctypes.c_float, ctypes.c_uint64, f32p, f32p], I32),
+    "zcb_fp32_peak": ([f64p], I32),
     "zcb_settings_apply": ([ctypes.c_char_p, SZ, ctypes.c_char_p, SZ, ctypes.POINTER(SZ), ctypes.c_char_p, SZ, ctypes.POINTER(SZ)], I32),
 }
 

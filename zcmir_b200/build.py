@@ -20,7 +20,7 @@ ROOT = HERE.parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libzcmir.so"
-SOURCES = ["features.cu", "preprocess.cu", "shiftmap.cu", "lines_a.cu", "lines_b.cu", "lines_c.cu", "rows_tmem.cu", "inv_cols_tma.cu", "pose.cu", "sweep.cu", "rs.cu", "ncc.cu", "score_static.cu", "gn_device.cu", "dft_tc.cu", "proposal.cu", "cnn.cu", "engine.cpp", "engine_pose.cpp", "engine_sweep.cpp", "engine_stack.cpp", "engine_rs.cpp", "engine_ncc.cpp", "engine_ffd.cpp", "settings.cpp", "exports.cpp"]
+SOURCES = ["features.cu", "preprocess.cu", "shiftmap.cu", "lines_a.cu", "lines_b.cu", "lines_c.cu", "rows_tmem.cu", "inv_cols_tma.cu", "pose.cu", "sweep.cu", "rs.cu", "ncc.cu", "score_static.cu", "gn_device.cu", "dft_tc.cu", "proposal.cu", "cnn.cu", "peak.cu", "engine.cpp", "engine_pose.cpp", "engine_sweep.cpp", "engine_stack.cpp", "engine_rs.cpp", "engine_ncc.cpp", "engine_ffd.cpp", "settings.cpp", "exports.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # the device refine restates the host's float64 pose algebra operation for operation: no fused
 # multiply-adds, so both give the same poses bit for bit
