@@ -333,7 +333,7 @@ def _eval_main(a):
                     H, maps = _with(reg, fine_settings(), reg.search).H, FINE_NTH * FINE_NS
                     fb = False
                 else:
-                    out = search(reg, net, k=a.k, with_network=name == "proposal")
+                    out = search(reg, net, k=a.k, with_network=name == "proposal", iters=a.iters)
                     H, maps, fb = out["H"], out["maps"], out["fallback"]
                 r[name] = dict(err=corner_rms(H, Ht, mw, mh), s=time.perf_counter() - t0, maps=maps, fallback=fb)
             rows.append(r)
@@ -344,7 +344,7 @@ def _eval_main(a):
                           s_per_search=float(np.mean([r[name]["s"] for r in rows])),
                           maps_mean=float(np.mean([r[name]["maps"] for r in rows])),
                           fallbacks=int(sum(r[name]["fallback"] for r in rows)))
-    print(json.dumps({"pairs": a.pairs, "first_seed": a.first, "k": a.k, "summary": summ,
+    print(json.dumps({"pairs": a.pairs, "first_seed": a.first, "n": a.n, "k": a.k, "iters": a.iters, "summary": summ,
                       "errors": {n: [round(r[n]["err"], 3) for r in rows] for n in ("plain", "coarse", "proposal")}}))
 
 
@@ -366,6 +366,7 @@ def main():
     e.add_argument("--first", type=int, default=100_000)
     e.add_argument("--n", type=int, default=256)
     e.add_argument("--k", type=int, default=4)
+    e.add_argument("--iters", type=int, default=25, help="Gauss–Newton steps of the proposal's refine")
     e.add_argument("--params", type=Path, default=PARAMS_PATH)
     a = ap.parse_args()
     if a.cmd == "train":
