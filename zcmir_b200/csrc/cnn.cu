@@ -59,8 +59,33 @@ __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], 
 
 // Block: 4 warps over a 64 × 64 tile of C, warp w rows 16w..16w+15 × all 64 columns (8 n-tiles).
 // K in steps of 32 from blockIdx.z · kspan (split K: each z adds its part through epi).
-// AKF / BKF: consecutive threads walk k (true) or m / n (false) when staging, whichever the
-// gather reads contiguously.
+// Operands are staged 8 BF16 values (16 bytes) at a time from the gather's run8(row, k): 8
+// consecutive k (AKF / BKF true: the row's channels of one tap, contiguous in NHWC) or 8
+// consecutive rows (false: the output channels of one pixel). So K and kspan are multiples of 8
+// when the run is along k, M (or N) a multiple of 8 when it is along the rows.
+__device__ __forceinline__ uint4 zero8() { return make_uint4(0u, 0u, 0u, 0u); }
+
+template <bool KF, int R, class L>
+__device__ __forceinline__ void stage(bf16 (&S)[R][BKP], const L& l, int r0, int nr, int k0, int ke, int tid) {
+    if constexpr (KF) {
+#pragma unroll
+        for (int i = tid; i < R * BK / 8; i += kThreads) {
+            const int r = i / (BK / 8), cg = i % (BK / 8);
+            const int row = r0 + r, k = k0 + cg * 8;
+            *reinterpret_cast<uint4*>(&S[r][cg * 8]) = (row < nr && k < ke) ? l.run8(row, k) : zero8();
+        }
+    } else {
+#pragma unroll
+        for (int i = tid; i < R * BK / 8; i += kThreads) {
+            const int c = i / (R / 8), rg = i % (R / 8);
+            const int row = r0 + rg * 8, k = k0 + c;
+            const uint4 v = (row < nr && k < ke) ? l.run8(row, k) : zero8();
+            const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) S[rg * 8 + j][c] = e[j];
+        }
+    }
+}
 template <bool AKF, bool BKF, class LA, class LB, class EPI>
 __global__ void __launch_bounds__(kThreads) k_gemm(int M, int N, int K, int kspan, LA la, LB lb, EPI epi) {
     __shared__ __align__(16) bf16 As[BM][BKP];
@@ -71,18 +96,8 @@ __global__ void __launch_bounds__(kThreads) k_gemm(int M, int N, int K, int kspa
     float acc[8][4] = {};
     const int g = lane >> 2, q = lane & 3;
     for (int k0 = kb; k0 < ke; k0 += BK) {
-#pragma unroll 4
-        for (int i = tid; i < BM * BK; i += kThreads) {
-            const int r = AKF ? i / BK : i % BM, c = AKF ? i % BK : i / BM;
-            const int m = m0 + r, k = k0 + c;
-            As[r][c] = (m < M && k < ke) ? la(m, k) : __float2bfloat16_rn(0.f);
-        }
-#pragma unroll 4
-        for (int i = tid; i < BN * BK; i += kThreads) {
-            const int r = BKF ? i / BK : i % BN, c = BKF ? i % BK : i / BN;
-            const int n = n0 + r, k = k0 + c;
-            Bs[r][c] = (n < N && k < ke) ? lb(n, k) : __float2bfloat16_rn(0.f);
-        }
+        stage<AKF>(As, la, m0, M, k0, ke, tid);
+        stage<BKF>(Bs, lb, n0, N, k0, ke, tid);
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 16) {
@@ -119,21 +134,24 @@ struct ConvShape {
 };
 
 // patch element (output pixel m, column k = tap·Ci + ci) of a stride-2, pad-1 3×3 convolution
+// (8 consecutive k from a multiple of 8: 8 channels of one tap, Ci a multiple of 8)
 struct Patch {
     const bf16* x;
     ConvShape s;
-    __device__ __forceinline__ bf16 operator()(int m, int k) const {
+    __device__ __forceinline__ uint4 run8(int m, int k) const {
         const int ohw = s.OH() * s.OW(), b = m / ohw, p = m - b * ohw, oy = p / s.OW(), ox = p - oy * s.OW();
         const int tap = k / s.Ci, ci = k - tap * s.Ci, ky = tap / 3, kx = tap - ky * 3;
         const int iy = 2 * oy + ky - 1, ix = 2 * ox + kx - 1;
-        if (iy < 0 || iy >= s.H || ix < 0 || ix >= s.W) return __float2bfloat16_rn(0.f);
-        return x[(((size_t)b * s.H + iy) * s.W + ix) * s.Ci + ci];
+        if (iy < 0 || iy >= s.H || ix < 0 || ix >= s.W) return zero8();
+        return *reinterpret_cast<const uint4*>(x + (((size_t)b * s.H + iy) * s.W + ix) * s.Ci + ci);
     }
 };
-struct RowMajor {  // a[r · ld + k]
+struct RowMajor {  // a[r · ld + k .. + 7], ld a multiple of 8
     const bf16* a;
     int ld;
-    __device__ __forceinline__ bf16 operator()(int r, int k) const { return a[(size_t)r * ld + k]; }
+    __device__ __forceinline__ uint4 run8(int r, int k) const {
+        return *reinterpret_cast<const uint4*>(a + (size_t)r * ld + k);
+    }
 };
 // forward epilogue: bias, ReLU, BF16 store
 struct FwdEpi {
@@ -149,14 +167,14 @@ struct FwdEpi {
 struct DataGather {
     const bf16* dz;
     ConvShape s;
-    __device__ __forceinline__ bf16 operator()(int m, int k) const {
+    __device__ __forceinline__ uint4 run8(int m, int k) const {
         const int hw = s.H * s.W, b = m / hw, p = m - b * hw, iy = p / s.W, ix = p - iy * s.W;
         const int tap = k / s.Co, co = k - tap * s.Co, ky = tap / 3, kx = tap - ky * 3;
         const int ty = iy + 1 - ky, tx = ix + 1 - kx;
-        if (ty < 0 || tx < 0 || (ty & 1) || (tx & 1)) return __float2bfloat16_rn(0.f);
+        if (ty < 0 || tx < 0 || (ty & 1) || (tx & 1)) return zero8();
         const int oy = ty >> 1, ox = tx >> 1;
-        if (oy >= s.OH() || ox >= s.OW()) return __float2bfloat16_rn(0.f);
-        return dz[(((size_t)b * s.OH() + oy) * s.OW() + ox) * s.Co + co];
+        if (oy >= s.OH() || ox >= s.OW()) return zero8();
+        return *reinterpret_cast<const uint4*>(dz + (((size_t)b * s.OH() + oy) * s.OW() + ox) * s.Co + co);
     }
 };
 // input-gradient epilogue: through the ReLU that produced the input (mask: input > 0), BF16
@@ -169,15 +187,18 @@ struct DataEpi {
         dzp[i] = __float2bfloat16_rn(__bfloat162float(x[i]) > 0.f ? v : 0.f);
     }
 };
-// weight-gradient operands: A(co, pixel) = dz[pixel][co]; B(tap·Ci + ci, pixel) = the patch
+// weight-gradient operands, 8 consecutive rows of one pixel: A(co .. co + 7, pixel) =
+// dz[pixel][co ..]; B(tap·Ci + ci .. + 7, pixel) = the patch's 8 channels
 struct DzT {
     const bf16* dz;
     int Co;
-    __device__ __forceinline__ bf16 operator()(int co, int px) const { return dz[(size_t)px * Co + co]; }
+    __device__ __forceinline__ uint4 run8(int co, int px) const {
+        return *reinterpret_cast<const uint4*>(dz + (size_t)px * Co + co);
+    }
 };
 struct PatchT {
     Patch p;
-    __device__ __forceinline__ bf16 operator()(int n, int px) const { return p(px, n); }
+    __device__ __forceinline__ uint4 run8(int n, int px) const { return p.run8(px, n); }
 };
 struct AtomicEpi {
     float* dw;
